@@ -1,0 +1,366 @@
+"""Benchmark of the B200 RK12 step: body-steps/s on the full-shape synthetic solar system.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload config2]
+
+Workload: the 504-body full-physics synthetic system (ephemeris_b200.synth.make_config2, seed 2002:
+geopotentials on 9 bodies, time-lagged tides, a ring, soft masses, radiation pressure), fixed step of
+0.05 day. One bench "step" is one call of the integrator over `--rk-steps` RK12 steps (default 100) of
+the whole system, i.e. rk_steps * 504 body-steps. The state (double-double position/velocity, full
+auxiliaries) is resident in HBM when the timed region starts (`value`); `e2e` repeats the measurement
+through the public C-ABI with the system planes uploaded from pinned host memory and downloaded back
+every step.
+
+Multi-GPU: a single system does not shard (one system per GPU is replicated; "replicas only"), so
+N ranks integrate N independent replicas; value = all ranks' body-steps / max-over-ranks device time.
+
+--impl reference times the reference's own CPU integrator (oracle/_ref, built from the reference
+sources, with its thread pool) on the same workload; without it, the oracle restatement is timed.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "body-steps/s vs plain FP64 at <=1e-12 pos err; small-body p50/p99 latency"
+UNIT = "body-steps/s"
+
+# Algorithmic flop convention per ordered pair and stage evaluation ("Roofline"):
+FLOP_PASS_A = 20            # potential + Newtonian acceleration
+FLOP_PASS_A_TIDE = 120      # time-lagged tidal matrix, extra over the Newtonian part
+FLOP_1PN = 80
+FLOP_DEFORM = 90            # tidal/rotational deformation force of i and j
+FLOP_LT = 80
+FLOP_RAD = 10
+FLOP_GP = 250               # per (body, geopotential host), Nz=6/Nt=4
+FLOP_RING_DISK = 60         # per (body, ring host, disk)
+FLOP_RK = 3900              # RK12 combination + update per body-step
+
+
+def algorithmic_flops_per_step(planes, models):
+    """FLOPs of one RK12 step (25 stage evaluations) of the whole system, by the convention above."""
+    n = planes.shape[1]
+    k2, td = planes[46], planes[48]
+    delayed = int(((k2 != 0) & (td != 0)).sum())
+    per_stage = (n * (n - 1) * (FLOP_PASS_A + FLOP_1PN + FLOP_DEFORM + FLOP_LT + FLOP_RAD)
+                 + delayed * (n - 1) * FLOP_PASS_A_TIDE)
+    per_stage += len(models.gp_nz) * (n - 1) * FLOP_GP
+    per_stage += int(np.sum(models.ring_ndisk)) * (n - 1) * FLOP_RING_DISK
+    return 25 * per_stage + n * FLOP_RK
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.idx = device_index
+        self.proc = None
+        self.out = None
+
+    def start(self):
+        try:
+            self.out = tempfile.TemporaryFile(mode="w+")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.out, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.out.seek(0)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.out.read().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def load_workload(workload: str, tmpdir: str):
+    from ephemeris_b200 import synth
+    return synth.write_workload(workload, os.path.join(tmpdir, workload))
+
+
+def dist_setup(n_gpus):
+    """Rank / world size from torchrun's environment; NCCL process group when N > 1."""
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        backend = os.environ.get("EPH_BENCH_BACKEND", "nccl")
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    return rank, world, local, pg
+
+
+def reduce_max(pg, value: float, device=None) -> float:
+    """Maximum of a per-rank float over all ranks (identity without a process group)."""
+    if pg is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg, device=None):
+    if pg is None:
+        return
+    import torch
+    t = torch.zeros(1, device=device)
+    pg.all_reduce(t)
+
+
+def cpu_baseline(cfg, n_steps: int):
+    """The reference's own CPU integrator (thread pool) on a bounded sample; else the oracle port."""
+    from oracle.pyoracle import Oracle, RefSystem, ref_available
+    cores = os.cpu_count() or 1
+    if ref_available():
+        ref = RefSystem(cfg)
+        RefSystem.thread_pool(True)
+        dt = ref.lib().ref_delta_t(ref.h)
+        ref.integrate(dt, 1)                       # warm the pool
+        t0 = time.perf_counter()
+        ref.integrate(dt, n_steps)
+        el = time.perf_counter() - t0
+        RefSystem.thread_pool(False)
+        return {"value": ref.n * n_steps / el, "unit": UNIT, "cores": min(16, cores), "kind": "reference",
+                "sample": f"{n_steps} RK12 steps of the {ref.n}-body system, msystem::integrate(dt,n,0) with "
+                          f"ThreadPool (min(16, {cores}) workers), {el:.1f} s"}
+    from ephemeris_b200 import MSystem  # noqa: F401  (product loader provides the state)
+    raise RuntimeError("oracle/_ref missing")
+
+
+def run_reference(args):
+    """--impl reference: the reference CPU integrator, rank 0 only."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle.pyoracle import Oracle, RefSystem, ref_available
+    with tempfile.TemporaryDirectory() as td:
+        cfg = load_workload(args.workload, td)
+        cores = os.cpu_count() or 1
+        per_step = args.ref_rk_steps
+        if ref_available():
+            ref = RefSystem(cfg)
+            RefSystem.thread_pool(True)
+            dt = ref.lib().ref_delta_t(ref.h)
+            n = ref.n
+            for _ in range(args.warmup):
+                ref.integrate(dt, per_step)
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                ref.integrate(dt, per_step)
+            el = time.perf_counter() - t0
+            kind, used = "reference", min(16, cores)
+            sample = (f"{args.steps} x {per_step} RK12 steps of the {n}-body system, reference "
+                      f"msystem::integrate(dt,n,0) with its ThreadPool ({used} workers)")
+        else:
+            from ephemeris_b200 import MSystem
+            ms = MSystem(0)
+            assert ms.load(cfg)
+            pl, md = ms.planes(), ms.models()
+            orc = Oracle()
+            from oracle.pyoracle import Models as OM
+            om = OM(md.gp_nz, md.gp_nt, md.gp_coef, md.ring_ndisk, md.ring_param, md.ring_disk)
+            dt, n = ms.delta_t, pl.shape[1]
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                pl, _, _ = orc.integrate(pl, om, dt, per_step)
+            el = time.perf_counter() - t0
+            kind, used = "port", 1
+            sample = f"{args.steps} x {per_step} RK12 steps, C restatement, 1 thread"
+        value = n * per_step * args.steps / el
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64 (double-double state)", "data": "synthetic",
+                "impl": "reference",
+                "config": {"workload": f"{args.workload}: {n}-body full-physics synthetic system, dt=0.05 day",
+                           "rk_steps_per_step": per_step},
+                "cpu_baseline": {"value": value, "unit": UNIT, "cores": used, "kind": kind, "sample": sample},
+                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+
+
+def run_b200(args):
+    import torch
+    from ephemeris_b200 import Context, MSystem
+    rank, world, local, pg = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    with tempfile.TemporaryDirectory() as td:
+        cfg = load_workload(args.workload, td)
+        ms = MSystem(local)
+        if not ms.load(cfg):
+            raise RuntimeError("workload failed to load")
+        planes0 = ms.planes()
+        models = ms.models()
+        n = planes0.shape[1]
+        dt = ms.delta_t
+        rk = args.rk_steps
+        ctx = Context(local)
+        ctx.upload(planes0, models)
+        if args.grid or args.per_cta:
+            ctx.set_launch(args.grid, args.per_cta)
+        stream = torch.cuda.current_stream(dev)
+        ctx.set_stream(stream.cuda_stream)
+        flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)   # > 126 MB L2
+
+        # ---- device-resident throughput: CUDA events on the launching stream, L2 flushed between steps
+        t = (0.0, 0.0)
+        for _ in range(args.warmup):
+            t = ctx.integrate(dt, rk, t)
+        barrier(pg, dev)
+        torch.cuda.synchronize(dev)
+        clocks = ClockSampler(local)
+        clocks.start()
+        launches0 = ctx.launches()
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            starts[k].record(stream)
+            t = ctx.integrate(dt, rk, t)
+            ends[k].record(stream)
+        torch.cuda.synchronize(dev)
+        clk = clocks.stop()
+        launches = ctx.launches() - launches0
+        dev_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+        barrier(pg, dev)
+        dev_ms_max = reduce_max(pg, dev_ms, dev)
+        value = world * n * rk * args.steps / (dev_ms_max / 1e3)
+        kern_ms = dev_ms / args.steps
+
+        # ---- end to end through the public C ABI with host buffers (pinned)
+        host_in = torch.from_numpy(planes0.copy()).pin_memory()
+        host_out = torch.empty_like(host_in).pin_memory()
+        pin_in, pin_out = host_in.numpy(), host_out.numpy()
+        for _ in range(max(1, args.warmup // 2)):
+            ctx.upload(pin_in, models)
+            ctx.integrate(dt, rk)
+            ctx.download(pin_out)
+        barrier(pg, dev)
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            ctx.upload(pin_in, models)
+            ctx.integrate(dt, rk)
+            ctx.download(pin_out)
+        torch.cuda.synchronize(dev)
+        e2e_s = reduce_max(pg, time.perf_counter() - t0, dev)
+        e2e = world * n * rk * args.steps / e2e_s
+
+        flops_step = algorithmic_flops_per_step(planes0, models)
+        achieved = flops_step * rk / (kern_ms / 1e3) / 1e12
+        peak, peak_src = fp64_peak(dev)
+        cpu = None
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            try:
+                cpu = cpu_baseline(cfg, args.cpu_rk_steps)
+            except Exception as exc:   # the baseline is reported, not required
+                cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "unavailable", "sample": str(exc)}
+        if rank == 0:
+            grid, per = ctx.launch_shape()
+            line = {
+                "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64 (double-double state)", "data": "synthetic",
+                "config": {"workload": f"{args.workload}: {n}-body full-physics synthetic system (seeded), "
+                                       f"dt=0.05 day", "rk_steps_per_step": rk, "bodies": n,
+                           "parallelism": f"replicas x{world}" if world > 1 else "single system, 1 GPU",
+                           "l2": "flushed between timed steps (256 MB write)", "grid": grid, "bodies_per_cta": per},
+                "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(planes0.nbytes),
+                        "d2h_bytes_per_step": int(planes0.nbytes)},
+                "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                             "frac": achieved / peak if peak else None, "traffic": None,
+                             "peak_source": peak_src, "flops_per_launch": flops_step * rk},
+                "gpu_launches": launches,
+                "clocks": clk,
+            }
+            if cpu is not None:
+                line["cpu_baseline"] = cpu
+            print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+def fp64_peak(dev):
+    """Measured FP64 peak: cuBLAS DGEMM 8192^3 (best of 5, CUDA events)."""
+    import torch
+    try:
+        a = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
+        b = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
+        torch.matmul(a, b)
+        torch.cuda.synchronize(dev)
+        best = None
+        for _ in range(5):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            torch.matmul(a, b)
+            e.record()
+            e.synchronize()
+            ms = s.elapsed_time(e)
+            best = ms if best is None else min(best, ms)
+        del a, b
+        return 2 * 8192 ** 3 / (best / 1e3) / 1e12, "cuBLAS DGEMM 8192^3, measured in bench.py (best of 5)"
+    except Exception as exc:
+        return None, f"unavailable: {exc}"
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="config2")
+    ap.add_argument("--rk-steps", type=int, default=100, help="RK12 steps per bench step")
+    ap.add_argument("--ref-rk-steps", type=int, default=2, help="RK12 steps per reference bench step")
+    ap.add_argument("--cpu-rk-steps", type=int, default=20, help="RK12 steps of the CPU baseline sample")
+    ap.add_argument("--grid", type=int, default=0)
+    ap.add_argument("--per-cta", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

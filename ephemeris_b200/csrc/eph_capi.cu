@@ -1,0 +1,402 @@
+// eph_capi.cu - context management and the extern "C" entry points of include/eph_b200.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <numeric>
+#include <vector>
+
+#include "eph_system.cuh"
+#include "../../include/eph_b200.h"
+
+namespace eph {
+size_t step_smem_bytes();
+cudaError_t upload_constants(int device);
+cudaError_t launch_step(const SysDev &S, const StepParams &P, int grid, cudaStream_t stream);
+int max_coresident_ctas(int device, int *out);
+}  // namespace eph
+
+using namespace eph;
+
+struct eph_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;       // work stream (own_stream unless eph_set_stream chose another)
+    cudaStream_t own_stream = nullptr;
+    std::mutex mu;
+    char err[512] = {0};
+    // system
+    int n = 0, n_gp = 0, n_ring = 0, n_ext = 0;
+    size_t cap_n = 0;
+    int cap_gp = 0, cap_ring = 0;
+    double *d_planes = nullptr, *d_pub = nullptr, *d_aux = nullptr, *d_cst = nullptr;
+    int *d_ext = nullptr, *d_own = nullptr, *d_status = nullptr;
+    unsigned *d_bar = nullptr;
+    int *d_gp_nz = nullptr, *d_gp_nt = nullptr, *d_ring_nd = nullptr;
+    double *d_gp_coef = nullptr, *d_ring_param = nullptr, *d_ring_disk = nullptr;
+    std::vector<double> h_cost;          // per-body work estimate for the ownership split
+    int grid = 0, per_cta = 0;           // current launch shape
+    int req_grid = 0, req_per_cta = 0;   // requested by eph_set_launch (0 = automatic)
+    int64_t launches = 0;
+};
+
+static int fail(eph_ctx *c, int code, const char *what, cudaError_t e = cudaSuccess) {
+    if (c) {
+        if (e != cudaSuccess)
+            snprintf(c->err, sizeof(c->err), "%s: %s", what, cudaGetErrorString(e));
+        else
+            snprintf(c->err, sizeof(c->err), "%s", what);
+    }
+    return code;
+}
+#define CK(call, what)                                                                 \
+    do {                                                                               \
+        cudaError_t e_ = (call);                                                       \
+        if (e_ != cudaSuccess)                                                         \
+            return fail(ctx, e_ == cudaErrorMemoryAllocation ? EPH_ERR_OOM : EPH_ERR_CUDA, what, e_); \
+    } while (0)
+
+static void free_system(eph_ctx *ctx) {
+    void *ptrs[] = {ctx->d_planes, ctx->d_pub, ctx->d_aux, ctx->d_cst, ctx->d_ext, ctx->d_own,
+                    ctx->d_gp_nz, ctx->d_gp_nt, ctx->d_ring_nd, ctx->d_gp_coef, ctx->d_ring_param,
+                    ctx->d_ring_disk};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    ctx->d_planes = ctx->d_pub = ctx->d_aux = ctx->d_cst = nullptr;
+    ctx->d_ext = ctx->d_own = nullptr;
+    ctx->d_gp_nz = ctx->d_gp_nt = ctx->d_ring_nd = nullptr;
+    ctx->d_gp_coef = ctx->d_ring_param = ctx->d_ring_disk = nullptr;
+    ctx->cap_n = 0;
+    ctx->cap_gp = ctx->cap_ring = 0;
+    ctx->n = 0;
+    ctx->grid = 0;
+}
+
+extern "C" {
+
+int eph_ctx_create(int device, eph_ctx **out) {
+    if (!out) return EPH_ERR_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) return EPH_ERR_ARG;
+    eph_ctx *ctx = new eph_ctx();
+    ctx->device = device;
+    CK(cudaSetDevice(device), "cudaSetDevice");
+    CK(cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    ctx->stream = ctx->own_stream;
+    CK(cudaMalloc(&ctx->d_bar, 2 * sizeof(unsigned)), "cudaMalloc(barrier)");
+    CK(cudaMalloc(&ctx->d_status, sizeof(int)), "cudaMalloc(status)");
+    CK(upload_constants(device), "upload RK12 constants");
+    *out = ctx;
+    return EPH_OK;
+}
+
+int eph_ctx_destroy(eph_ctx *ctx) {
+    if (!ctx) return EPH_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    free_system(ctx);
+    if (ctx->d_bar) cudaFree(ctx->d_bar);
+    if (ctx->d_status) cudaFree(ctx->d_status);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+    return EPH_OK;
+}
+
+const char *eph_last_error(const eph_ctx *ctx) { return ctx ? ctx->err : "null context"; }
+
+}  // extern "C"
+
+// Split bodies over CTAs: longest-processing-time-first into `grid` bins of at most `cap` bodies.
+static void plan_ownership(const std::vector<double> &cost, int grid, int cap, std::vector<int> &own) {
+    const int n = (int)cost.size();
+    std::vector<int> order(n);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+    std::vector<double> load(grid, 0.0);
+    std::vector<int> cnt(grid, 0);
+    own.assign((size_t)grid * kOwnMax, -1);
+    for (int i : order) {
+        int best = -1;
+        for (int g = 0; g < grid; ++g) {
+            if (cnt[g] >= cap) continue;
+            if (best < 0 || load[g] < load[best]) best = g;
+        }
+        own[(size_t)best * kOwnMax + cnt[best]++] = i;
+        load[best] += cost[i];
+    }
+    // bodies of a CTA in index order, so every CTA's list is deterministic and monotone
+    for (int g = 0; g < grid; ++g) std::sort(own.begin() + (size_t)g * kOwnMax, own.begin() + (size_t)g * kOwnMax + cnt[g]);
+}
+
+static int choose_shape(eph_ctx *ctx) {
+    int maxc = 0;
+    if (max_coresident_ctas(ctx->device, &maxc) != 0 || maxc <= 0) return fail(ctx, EPH_ERR_CUDA, "occupancy query failed");
+    const int n = ctx->n;
+    int per = ctx->req_per_cta, grid = ctx->req_grid;
+    if (per <= 0 && grid <= 0) {
+        grid = std::min(maxc, n);
+        per = (n + grid - 1) / grid;
+        grid = (n + per - 1) / per;
+        if (n > 64 && grid < maxc) grid = std::min(maxc, n);   // spread work when every SM can take some
+    } else if (per <= 0) {
+        per = (n + grid - 1) / grid;
+    } else if (grid <= 0) {
+        grid = (n + per - 1) / per;
+    }
+    per = std::max(1, std::min(per, (int)kOwnMax));
+    grid = std::max(grid, (n + per - 1) / per);
+    if (grid > maxc) return fail(ctx, EPH_ERR_ARG, "launch shape exceeds co-resident CTAs (bodies_per_cta too small)");
+    std::vector<int> own;
+    plan_ownership(ctx->h_cost, grid, per, own);
+    cudaError_t e = cudaMemcpy(ctx->d_own, own.data(), own.size() * sizeof(int), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return fail(ctx, EPH_ERR_CUDA, "upload ownership", e);
+    ctx->grid = grid;
+    ctx->per_cta = per;
+    return EPH_OK;
+}
+
+static int prepare_constants(eph_ctx *ctx, const double *h_planes) {
+    const int n = ctx->n;
+    std::vector<double> cst((size_t)CST_NPLANES * n);
+    std::vector<int> ext;
+    ctx->h_cost.assign(n, 0.0);
+    for (int i = 0; i < n; ++i) {
+        auto P = [&](int p) { return h_planes[(size_t)p * n + i]; };
+        cst[CST_SR2 * n + i] = P(EPH_P_SR2);
+        cst[CST_TDF * n + i] = P(EPH_P_TIDE_DELAY_FACTOR);
+        cst[CST_R2 * n + i] = P(EPH_P_R2);
+        cst[CST_LUM * n + i] = P(EPH_P_LUM);
+        cst[CST_R * n + i] = P(EPH_P_RADIUS);
+        cst[CST_GP * n + i] = P(EPH_P_GP_INDEX);
+        cst[CST_RING * n + i] = P(EPH_P_RING_INDEX);
+        const bool gp = P(EPH_P_GP_INDEX) >= 0, ring = P(EPH_P_RING_INDEX) >= 0;
+        if (gp || ring) ext.push_back(i);
+        const bool delayed = P(EPH_P_K2) != 0 && P(EPH_P_TIDE_DELAY) != 0;
+        // relative work: pass A (three sweeps for a delayed tide), pass B, extended-body models
+        ctx->h_cost[i] = (delayed ? 3.0 * 2.0 : 1.0) + 3.0 + (gp ? 4.0 : 0.0) + (ring ? 8.0 : 0.0);
+    }
+    if ((int)ext.size() > kMaxExt) return fail(ctx, EPH_ERR_ARG, "too many bodies with geopotential or ring models");
+    ctx->n_ext = (int)ext.size();
+    cudaError_t e = cudaMemcpy(ctx->d_cst, cst.data(), cst.size() * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !ext.empty())
+        e = cudaMemcpy(ctx->d_ext, ext.data(), ext.size() * sizeof(int), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return fail(ctx, EPH_ERR_CUDA, "upload constants", e);
+    return EPH_OK;
+}
+
+extern "C" {
+
+int eph_upload_system(eph_ctx *ctx, int64_t n64, const double *planes, const eph_models *models) {
+    if (!ctx || !planes || n64 <= 0 || n64 > (1 << 20)) return fail(ctx, EPH_ERR_ARG, "eph_upload_system: bad arguments");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    const int n = (int)n64;
+    const int n_gp = models ? models->n_gp : 0, n_ring = models ? models->n_ring : 0;
+    if (n_gp < 0 || n_ring < 0 || (n_gp && (!models->gp_nz || !models->gp_nt || !models->gp_coef)) ||
+        (n_ring && (!models->ring_ndisk || !models->ring_param || !models->ring_disk)))
+        return fail(ctx, EPH_ERR_ARG, "eph_upload_system: bad model tables");
+    for (int k = 0; k < n_ring; ++k)
+        if (models->ring_ndisk[k] < 0 || models->ring_ndisk[k] > EPH_RING_MAX_DISKS)
+            return fail(ctx, EPH_ERR_ARG, "eph_upload_system: ring disk count out of range");
+    for (int k = 0; k < n_gp; ++k)
+        if (models->gp_nz[k] < 0 || models->gp_nz[k] > EPH_GP_MAX_DEGREE || models->gp_nt[k] > models->gp_nz[k])
+            return fail(ctx, EPH_ERR_ARG, "eph_upload_system: geopotential degree out of range");
+    for (int i = 0; i < n; ++i) {
+        const double g = planes[(size_t)EPH_P_GP_INDEX * n + i], r = planes[(size_t)EPH_P_RING_INDEX * n + i];
+        if (!(g >= -1 && g < n_gp) || !(r >= -1 && r < n_ring))
+            return fail(ctx, EPH_ERR_ARG, "eph_upload_system: model index out of range");
+    }
+    if ((size_t)n > ctx->cap_n) {
+        free_system(ctx);
+        CK(cudaMalloc(&ctx->d_planes, (size_t)EPH_NPLANES * n * sizeof(double)), "cudaMalloc(planes)");
+        CK(cudaMalloc(&ctx->d_pub, (size_t)2 * PUB_NPLANES * n * sizeof(double)), "cudaMalloc(public state)");
+        CK(cudaMalloc(&ctx->d_aux, (size_t)AUX_NPLANES * n * sizeof(double)), "cudaMalloc(aux)");
+        CK(cudaMalloc(&ctx->d_cst, (size_t)CST_NPLANES * n * sizeof(double)), "cudaMalloc(constants)");
+        CK(cudaMalloc(&ctx->d_ext, (size_t)kMaxExt * sizeof(int)), "cudaMalloc(ext)");
+        CK(cudaMalloc(&ctx->d_own, (size_t)n * kOwnMax * sizeof(int)), "cudaMalloc(ownership)");
+        CK(cudaMemset(ctx->d_pub, 0, (size_t)2 * PUB_NPLANES * n * sizeof(double)), "cudaMemset");
+        ctx->cap_n = n;
+    }
+    // model tables: reallocated only when a larger table set arrives
+    if (!ctx->d_gp_nz || n_gp > ctx->cap_gp) {
+        for (int **p : {&ctx->d_gp_nz, &ctx->d_gp_nt}) { if (*p) cudaFree(*p); *p = nullptr; }
+        if (ctx->d_gp_coef) cudaFree(ctx->d_gp_coef);
+        ctx->d_gp_coef = nullptr;
+        ctx->cap_gp = std::max(n_gp, 1);
+        CK(cudaMalloc(&ctx->d_gp_nz, ctx->cap_gp * sizeof(int)), "cudaMalloc(gp)");
+        CK(cudaMalloc(&ctx->d_gp_nt, ctx->cap_gp * sizeof(int)), "cudaMalloc(gp)");
+        CK(cudaMalloc(&ctx->d_gp_coef, ctx->cap_gp * EPH_GP_TABLE_SIZE * sizeof(double)), "cudaMalloc(gp)");
+    }
+    if (!ctx->d_ring_nd || n_ring > ctx->cap_ring) {
+        if (ctx->d_ring_nd) cudaFree(ctx->d_ring_nd);
+        for (double **p : {&ctx->d_ring_param, &ctx->d_ring_disk}) { if (*p) cudaFree(*p); *p = nullptr; }
+        ctx->d_ring_nd = nullptr;
+        ctx->cap_ring = std::max(n_ring, 1);
+        CK(cudaMalloc(&ctx->d_ring_nd, ctx->cap_ring * sizeof(int)), "cudaMalloc(ring)");
+        CK(cudaMalloc(&ctx->d_ring_param, ctx->cap_ring * 4 * sizeof(double)), "cudaMalloc(ring)");
+        CK(cudaMalloc(&ctx->d_ring_disk, ctx->cap_ring * EPH_RING_MAX_DISKS * 3 * sizeof(double)), "cudaMalloc(ring)");
+    }
+    const bool same_n = (ctx->n == n);
+    ctx->n = n;
+    ctx->n_gp = n_gp;
+    ctx->n_ring = n_ring;
+    if (n_gp) {
+        CK(cudaMemcpy(ctx->d_gp_nz, models->gp_nz, n_gp * sizeof(int), cudaMemcpyHostToDevice), "upload gp");
+        CK(cudaMemcpy(ctx->d_gp_nt, models->gp_nt, n_gp * sizeof(int), cudaMemcpyHostToDevice), "upload gp");
+        CK(cudaMemcpy(ctx->d_gp_coef, models->gp_coef, (size_t)n_gp * EPH_GP_TABLE_SIZE * sizeof(double),
+                      cudaMemcpyHostToDevice), "upload gp");
+    }
+    if (n_ring) {
+        CK(cudaMemcpy(ctx->d_ring_nd, models->ring_ndisk, n_ring * sizeof(int), cudaMemcpyHostToDevice), "upload ring");
+        CK(cudaMemcpy(ctx->d_ring_param, models->ring_param, (size_t)n_ring * 4 * sizeof(double),
+                      cudaMemcpyHostToDevice), "upload ring");
+        CK(cudaMemcpy(ctx->d_ring_disk, models->ring_disk, (size_t)n_ring * EPH_RING_MAX_DISKS * 3 * sizeof(double),
+                      cudaMemcpyHostToDevice), "upload ring");
+    }
+    CK(cudaMemcpy(ctx->d_planes, planes, (size_t)EPH_NPLANES * n * sizeof(double), cudaMemcpyHostToDevice),
+       "upload planes");
+    std::vector<double> old_cost = ctx->h_cost;
+    int rc = prepare_constants(ctx, planes);
+    if (rc) return rc;
+    if (same_n && ctx->grid > 0 && old_cost == ctx->h_cost) return EPH_OK;   // same ownership plan
+    return choose_shape(ctx);
+}
+
+int eph_upload_planes_device(eph_ctx *ctx, const double *d_planes) {
+    if (!ctx || !d_planes) return fail(ctx, EPH_ERR_ARG, "eph_upload_planes_device: bad arguments");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    if (!ctx->n) return fail(ctx, EPH_ERR_STATE, "no system uploaded");
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    CK(cudaMemcpyAsync(ctx->d_planes, d_planes, (size_t)EPH_NPLANES * ctx->n * sizeof(double),
+                       cudaMemcpyDeviceToDevice, ctx->stream), "device planes copy");
+    CK(cudaStreamSynchronize(ctx->stream), "sync");
+    return EPH_OK;
+}
+
+int eph_download_system(eph_ctx *ctx, double *planes) {
+    if (!ctx || !planes) return fail(ctx, EPH_ERR_ARG, "eph_download_system: bad arguments");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    if (!ctx->n) return fail(ctx, EPH_ERR_STATE, "no system uploaded");
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    CK(cudaMemcpy(planes, ctx->d_planes, (size_t)EPH_NPLANES * ctx->n * sizeof(double), cudaMemcpyDeviceToHost),
+       "download planes");
+    return EPH_OK;
+}
+
+int eph_device_planes(eph_ctx *ctx, double **d_planes) {
+    if (!ctx || !d_planes) return fail(ctx, EPH_ERR_ARG, "eph_device_planes: bad arguments");
+    if (!ctx->n) return fail(ctx, EPH_ERR_STATE, "no system uploaded");
+    *d_planes = ctx->d_planes;
+    return EPH_OK;
+}
+
+}  // extern "C"
+
+static int run(eph_ctx *ctx, const StepParams &P) {
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    if (!ctx->n) return fail(ctx, EPH_ERR_STATE, "no system uploaded");
+    SysDev S;
+    S.n = ctx->n;
+    S.n_ext = ctx->n_ext;
+    S.pub = ctx->d_pub;
+    S.aux = ctx->d_aux;
+    S.cst = ctx->d_cst;
+    S.planes = ctx->d_planes;
+    S.ext_body = ctx->d_ext;
+    S.gp_nz = ctx->d_gp_nz;
+    S.gp_nt = ctx->d_gp_nt;
+    S.gp_coef = ctx->d_gp_coef;
+    S.ring_nd = ctx->d_ring_nd;
+    S.ring_param = ctx->d_ring_param;
+    S.ring_disk = ctx->d_ring_disk;
+    S.own_list = ctx->d_own;
+    S.bar = ctx->d_bar;
+    S.status = ctx->d_status;
+    CK(cudaMemsetAsync(ctx->d_bar, 0, 2 * sizeof(unsigned), ctx->stream), "reset barrier");
+    CK(cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream), "reset status");
+    CK(launch_step(S, P, ctx->grid, ctx->stream), "launch RK12 kernel");
+    ctx->launches++;
+    int status = 0;
+    CK(cudaMemcpyAsync(&status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream), "read status");
+    CK(cudaStreamSynchronize(ctx->stream), "RK12 kernel");
+    if (status == ST_BARRIER_TIMEOUT) return fail(ctx, EPH_ERR_TIMEOUT, "grid barrier wait timed out");
+    return EPH_OK;
+}
+
+extern "C" {
+
+int eph_rk12(eph_ctx *ctx, double dt, int64_t n_step, double t_eph_hi, double t_eph_lo) {
+    if (!ctx) return EPH_ERR_ARG;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    if (n_step <= 0) return EPH_OK;   // RungeKutta.cu:392
+    StepParams P{MODE_INTEGRATE, 0, 0, (long long)n_step, dt, t_eph_hi + t_eph_lo};
+    return run(ctx, P);
+}
+
+int eph_integrate(eph_ctx *ctx, double dt, int64_t n_step, double *t_eph_hi, double *t_eph_lo) {
+    if (!ctx || !t_eph_hi || !t_eph_lo) return fail(ctx, EPH_ERR_ARG, "eph_integrate: bad arguments");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    if (n_step == 0) return EPH_OK;   // mass.cpp:400
+    if (n_step < 0) {                 // mass.cpp:401-404
+        n_step = -n_step;
+        dt = -dt;
+    }
+    StepParams P{MODE_INTEGRATE, 1, 1, (long long)n_step, dt, *t_eph_hi + *t_eph_lo};
+    int rc = run(ctx, P);
+    if (rc) return rc;
+    // t_eph += dt*n_step in double-double (mass.cpp:441, dfloat_t.h:49-55)
+    double a = *t_eph_hi, b = dt * (double)n_step;
+    double s = a + b, t = s - a;
+    double e = (a - (s - t)) + (b - t);
+    e = e + (*t_eph_lo + 0.0);
+    double hi = s + e;
+    double lo = e - (hi - s);
+    *t_eph_hi = hi;
+    *t_eph_lo = lo;
+    return EPH_OK;
+}
+
+int eph_accel(eph_ctx *ctx) {
+    if (!ctx) return EPH_ERR_ARG;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    StepParams P{MODE_ACCEL, 0, 0, 0, 0.0, 0.0};
+    return run(ctx, P);
+}
+
+int eph_deform(eph_ctx *ctx) {
+    if (!ctx) return EPH_ERR_ARG;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    StepParams P{MODE_DEFORM, 0, 0, 0, 0.0, 0.0};
+    return run(ctx, P);
+}
+
+int eph_set_stream(eph_ctx *ctx, void *stream) {
+    if (!ctx) return EPH_ERR_ARG;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+    return EPH_OK;
+}
+
+int eph_set_launch(eph_ctx *ctx, int grid, int bodies_per_cta) {
+    if (!ctx || grid < 0 || bodies_per_cta < 0 || bodies_per_cta > kOwnMax)
+        return fail(ctx, EPH_ERR_ARG, "eph_set_launch: bad arguments");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    ctx->req_grid = grid;
+    ctx->req_per_cta = bodies_per_cta;
+    if (!ctx->n) return EPH_OK;
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    return choose_shape(ctx);
+}
+
+int eph_get_launch(const eph_ctx *ctx, int *grid, int *bodies_per_cta) {
+    if (!ctx || !grid || !bodies_per_cta) return EPH_ERR_ARG;
+    *grid = ctx->grid;
+    *bodies_per_cta = ctx->per_cta;
+    return EPH_OK;
+}
+
+int64_t eph_launch_count(const eph_ctx *ctx) { return ctx ? ctx->launches : -1; }
+
+}  // extern "C"

@@ -1,0 +1,202 @@
+// eph_models.cuh - device evaluation of the extended-body force models.
+//
+//   gp_sum   : spherical-harmonic field of degree 3..8 (zonal up to Nz, tesseral up to Nt) in the
+//              body frame, per unit GM of the extended body. Same recursion and coefficient packing
+//              as geopotential::sum (src/physics/geopotential.impl:18-106).
+//   ring_sum : field of a cylindrical annulus built from signed uniform disks, per unit GM of the
+//              host, in the ring frame. Same Pade series, angle formula and fp32 bicubic correction
+//              table as ring::sum (src/physics/ring.impl:2070-2195).
+#pragma once
+#include "eph_math.cuh"
+#include "../../include/eph_planes.h"
+#include "../../include/eph_ring_table.h"
+
+namespace eph {
+
+__device__ __forceinline__ v3 gp_sum(const double *__restrict__ c_table, int Nz, int Nt, double R, v3 r) {
+    double rho2 = r.x * r.x + r.y * r.y;
+    double rr2 = 1.0 / (rho2 + r.z * r.z);
+    double rho1 = sqrt(rho2);
+    double rr1 = sqrt(rr2);
+    double rb1 = R * rr1;
+    double rbn = rb1;
+    double cphi = rho1 * rr1;
+    double sphi = r.z * rr1;
+    double cm, sm;
+    if (rho2 < 2.2250738585072014e-308) { cm = 1; sm = 0; }
+    else { cm = r.x / rho1; sm = r.y / rho1; }
+    double pnm[EPH_GP_MAX_DEGREE], pn1m[EPH_GP_MAX_DEGREE];
+#pragma unroll
+    for (int q = 0; q < EPH_GP_MAX_DEGREE; ++q) { pnm[q] = 0; pn1m[q] = 0; }
+    pn1m[0] = 1;
+    double ppn = 1, pn = 1, pn1 = sphi;
+    double zx = 0, zz = 0;
+    v3 t = mk(0, 0, 0);
+#pragma unroll
+    for (int n = 2; n <= EPH_GP_MAX_DEGREE; ++n) {
+        if (n > Nz) break;
+        rbn *= rb1;
+        const double *JCSn = c_table + (n * n - 4);
+        pn = ((double)(2 * n - 1) * sphi * pn1 - (double)(n - 1) * pn) / (double)n;
+        ppn = sphi * ppn + (double)n * pn1;
+        double z1 = __ldg(JCSn) * rbn;
+        zx += (double)(n + 1) * z1 * pn;
+        zz -= z1 * ppn;
+        { double sw = pn; pn = pn1; pn1 = sw; }
+        if (n > Nt) continue;
+        v3 f = mk(0, 0, 0);
+        double m1 = (double)(2 * n - 1) * sphi;
+        double m2 = (double)(-n) * sphi;
+        double smm = 0, cmm = 0, smm1 = 0, cmm1 = 0;
+#pragma unroll
+        for (int m = 1; m <= n; ++m) {
+            if (m == n) {
+                pn1m[m - 1] = 0;
+                pnm[m - 1] = (double)(2 * n - 1) * cphi * pnm[m >= 2 ? m - 2 : 0];
+            } else {
+                pnm[m - 1] = (m1 * pn1m[m - 1] - (double)(n + m - 1) * pnm[m - 1]) / (double)(n - m);
+            }
+            if (m == 1) { smm = sm; cmm = cm; smm1 = 0; cmm1 = 1; }
+            else {
+                smm = 2 * cm * smm1 - smm;
+                cmm = 2 * cm * cmm1 - cmm;
+            }
+            double S = __ldg(JCSn + 2 * m), C = __ldg(JCSn + 2 * m - 1);
+            double t1 = S * smm + C * cmm;
+            double t2 = S * cmm - C * smm;
+            double ppnm = m2 * pnm[m - 1] + (double)(n + m) * pn1m[m - 1];
+            f.x += t1 * pnm[m - 1];
+            f.y += (double)m * t2 * pnm[m - 1];
+            f.z += t1 * ppnm;
+            { double sw = cmm; cmm = cmm1; cmm1 = sw; }
+            { double sw = smm; smm = smm1; smm1 = sw; }
+            { double sw = pnm[m - 1]; pnm[m - 1] = pn1m[m - 1]; pn1m[m - 1] = sw; }
+        }
+        f.x *= (double)(n + 1);
+        t += rbn * f;
+    }
+    t.x = zx - cphi * t.x;
+    t.z += zz * cphi;
+    t = rr2 * t;
+    double g1 = t.x * cphi - t.z * sphi;
+    return mk(g1 * cm - t.y * sm, g1 * sm + t.y * cm, cphi * t.z + sphi * t.x);
+}
+
+__device__ __forceinline__ float ring_fzcorr(float x, float y, int kh) {
+    const int N = 32;
+    x *= (float)N;
+    y *= (float)N;
+    int i = (int)floorf(x), j = (int)floorf(y);
+    j -= kh * N;
+    if (i < 0) i = 0;
+    if (j < 0) j = 0;
+    if (i >= N) i = N - 1;
+    if (j >= N) j = N - 1;
+    j += kh * N;
+    x = __fsub_rn(x, (float)i);
+    y = __fsub_rn(y, (float)j);
+    const float *p = reinterpret_cast<const float *>(EPH_RING_TABLE_BITS) + 16 * (2 * N * i + j);
+    float c[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) c[q] = __ldg(p + q);
+    // evaluated without contraction, in the reference's association order
+    auto h = [&](int a) {   // c[a] + x*(c[a+4] + x*(c[a+8] + x*c[a+12]))
+        return __fadd_rn(c[a], __fmul_rn(x, __fadd_rn(c[a + 4], __fmul_rn(x, __fadd_rn(c[a + 8], __fmul_rn(x, c[a + 12]))))));
+    };
+    float h3 = h(3), h2 = h(2), h1 = h(1), h0 = h(0);
+    return __fadd_rn(h0, __fmul_rn(y, __fadd_rn(h1, __fmul_rn(y, __fadd_rn(h2, __fmul_rn(y, h3))))));
+}
+
+template <int NC>
+__device__ __forceinline__ double padesum(double x, const double (&coef)[NC][2]) {
+    double resn = 0, resd = 0;
+#pragma unroll
+    for (int n = NC - 1; n >= 0; --n) {
+        resn = x * resn + coef[n][0];
+        resd = x * resd + coef[n][1];
+    }
+    return resn / resd;
+}
+
+// Pade coefficients of the disk field (src/physics/ring.impl:2101-2107)
+__device__ __constant__ const double RING_XSERKK[5][2] = {{-4228.1846570321674587, 6387.9414439779279738}, {-13276.372802884782407, 16984.953742612298093}, {-11316.549465243054011, 8997.7319379726254196}, {-3242.2867356286923985, 403.15182320396046619}, {-704.60633921130372399, -5.7789477668119521439}};
+__device__ __constant__ const double RING_XSERKM[5][2] = {{-2530.8255093002657219, 7950.8733392382639504}, {-5471.7803365810451727, 17189.101860053144376}, {-1624.0389725420726306, 7100.5562444641275465}, {1164.6058458813108946, 532.54915854738706820}, {270.03897254207263065, -5.0806023029229406554}};
+__device__ __constant__ const double RING_XSER0[6][2] = {{3216.9908772759482762, 32768.000000000000000}, {-6727.1375380948220662, -93098.060290997395032}, {4534.8257724052420971, 96814.901233532309690}, {-1004.5251977686921953, -43973.540867249017404}, {17.915064837735955511, 7754.0323173314244943}, {-0.039157108395559676838, -224.00490789882410101}};
+__device__ __constant__ const double RING_KSERKK[5][2] = {{-2373.3522804139070577, 1124.9866194216978637}, {-8300.7524798211745830, 17215.217000406477760}, {15279.068333441193395, 26590.060415743810476}, {-4354.4701057632348105, -9776.5071563707548874}, {-250.49346744287694398, -2385.7568792012312128}};
+__device__ __constant__ const double RING_KSERKM[5][2] = {{-523.02599873176918199, 290.10526315789473684}, {-5485.2200380469245403, 5336.9790741915028535}, {-8338.1052631578947368, 15206.361445783132530}, {-2017.9378566899175650, 10515.743817374762207}, {-19.710843373493975904, 1418.8103994927076728}};
+__device__ __constant__ const double RING_KSER0[6][2] = {{51471.854036415172419, 32768.000000000000000}, {-119621.18573838632696, -84345.212035111671234}, {96754.491735189724987, 78074.125512775430927}, {-31810.735585315211544, -31108.829182924968396}, {3678.1383813624327949, 4926.4461273804873303}, {-74.040670509817904983, -206.66608791871105442}};
+
+__device__ __forceinline__ v3 ring_sum(const double *__restrict__ disks, int ndisk, double host_R, v3 r) {
+    const double pi = 3.1415926535897932;
+    bool psign = r.z < 0;
+    if (psign) r.z = -r.z;
+    const double re2 = r.x * r.x + r.y * r.y;
+    const double re = sqrt(re2);
+    const double rz2 = r.z * r.z;
+    const double r2 = re2 + rz2;
+    const double rz = r.z;
+    v3 ret = mk(0, 0, 0);
+    for (int i = 0; i < ndisk; ++i) {
+        const double GsR2 = __ldg(disks + 3 * i), R_R = __ldg(disks + 3 * i + 1), H_R = __ldg(disks + 3 * i + 2);
+        double R = R_R * host_R;
+        double H = H_R * host_R;
+        double reR = re * R;
+        double R2 = R * R, H2, fzh = 1;
+        double k2dre = 4.0 / (r2 + R2 + 2 * reR);
+        if (H > 0) {
+            H2 = H * H;
+            k2dre -= H2 * (k2dre * k2dre) * (1 - k2dre * rz2) / 48;
+            fzh = (re > R ? re - R : 0);
+            fzh = 4 * (rz2 + fzh * fzh);
+            fzh = sqrt(fzh / (fzh + H2));
+        }
+        double k2 = reR * k2dre;
+        k2dre *= R2 * sqrt(k2dre);
+        double phi = atan2(rz, re - R);
+        double kk = 0, lk = 0, fx;
+        bool lkh = k2 >= 0.45;
+        if (lkh) {
+            kk = sqrt(k2);
+            lk = log((1 - k2) / (8 * (1 + kk)));
+            fx = (padesum(kk, RING_XSERKK) + lk * padesum(kk, RING_XSERKM)) / (k2 * k2);
+        } else {
+            fx = padesum(k2, RING_XSER0);
+        }
+        fx *= k2dre;
+        double fz;
+        double s, c;
+        sincos(phi, &s, &c);
+        int kh = k2 >= .5;
+        bool exphi;
+        if (kh) {
+            const double phimax = (pi / 2);
+            exphi = c > 0;
+            double ck = 1 - k2, lk2 = log(ck / 16), sk = sqrt(ck);
+            double cc = exphi ? -c : c;
+            double cphi = exphi ? pi - phi : phi;
+            fz = cphi - (s / 8) * ((lk2 * (k2 - 5) - 2 * ck) * sk + 2 * cc * (1 + lk2) * ck);
+            fz *= (double)ring_fzcorr((float)((exphi ? phi : pi - phi) * (1 / phimax)), (float)(k2 * 2), kh);
+        } else {
+            const double phimax = (809. / 512);
+            exphi = phi > phimax;
+            double cr2 = exphi ? R2 + rz2 : r2;
+            double cRdr2 = (exphi ? re2 : R2) / cr2;
+            fz = (pi / 8) * (4 - 3 * cRdr2) * (rz / sqrt(cr2) * cRdr2);
+            fz *= (double)ring_fzcorr((float)((exphi ? pi - phi : phi) * (1 / phimax)), (float)(k2 * 2), kh);
+        }
+        if (exphi) {
+            double ek;
+            if (lkh) ek = padesum(kk, RING_KSERKK) + lk * padesum(kk, RING_KSERKM);
+            else ek = padesum(k2, RING_KSER0);
+            fz = pi - 2 * sqrt(1 - k2) * ek * s - fz;
+        }
+        double Gs = GsR2 / (host_R * host_R);
+        fx *= Gs;
+        fz *= Gs;
+        ret += mk(-4 * fx * r.x, -4 * fx * r.y, -2 * fz * fzh);
+    }
+    if (psign) ret.z = -ret.z;
+    return ret;
+}
+
+}  // namespace eph

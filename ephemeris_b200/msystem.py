@@ -1,0 +1,226 @@
+"""Python mirror of the reference's msystem entry points for the RK12 path.
+
+    ms = MSystem()
+    ms.load("Config.txt")            # msystem::load           (src/modules/mass_loader.cpp:67-294)
+    ms.integrate(dt, n_step, 1)      # msystem::integrate      (src/physics/mass.cpp:399-442)
+    ms.accel(1)                      # msystem::accel(1)       (src/physics/mass.cpp:216-221)
+    ms[i]                            # msystem::operator[]     (src/physics/mass.h:343,353) as a field dict
+
+Every call goes through libeph_b200.so; the body state stays on the GPU between calls.
+
+``Context`` is the lower-level C ABI (include/eph_b200.h): upload a plane array, integrate, download.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from ._lib import NPLANES, EphModels, check, load_library
+
+# plane offsets (include/eph_planes.h)
+P = dict(R_HI=0, R_LO=3, V_HI=6, V_LO=9, GL_HI=12, GL_LO=15, S_HI=18, S_LO=27, W=36, GM=39, EXJ2=40, GM0=41,
+         DGM=42, DJ2=43, RADIUS=44, INERTIA=45, K2=46, K2R=47, TIDE_DELAY=48, TIDE_DELAY_FACTOR=49, LUM=50,
+         RECPT=51, A=52, R2=53, SR2=54, RR2G_4C=55, C_STATIC=56, PHI=65, BETA2=66, NACCEL=67, DACCEL=70,
+         DTORQUE=73, GACCEL=76, BETA=79, GI=82, C_POTENTIAL=91, MIN_DISTANCE=100, MAX_INFLUENCE=101,
+         GP_INDEX=102, RING_INDEX=103)
+VEC3 = {"R_HI", "R_LO", "V_HI", "V_LO", "GL_HI", "GL_LO", "W", "NACCEL", "DACCEL", "DTORQUE", "GACCEL", "BETA"}
+MAT9 = {"S_HI", "S_LO", "C_STATIC", "GI", "C_POTENTIAL"}
+
+CPU_RK12, GPU_RK12, COMBINED_RK12 = 0, 1, 2
+
+
+def _dptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class Models:
+    """Owned copies of the model tables plus the ctypes struct pointing at them."""
+
+    def __init__(self, gp_nz, gp_nt, gp_coef, ring_ndisk, ring_param, ring_disk):
+        self.gp_nz = np.ascontiguousarray(gp_nz, np.int32)
+        self.gp_nt = np.ascontiguousarray(gp_nt, np.int32)
+        self.gp_coef = np.ascontiguousarray(gp_coef, np.float64).reshape(len(self.gp_nz), 77)
+        self.ring_ndisk = np.ascontiguousarray(ring_ndisk, np.int32)
+        self.ring_param = np.ascontiguousarray(ring_param, np.float64).reshape(len(self.ring_ndisk), 4)
+        self.ring_disk = np.ascontiguousarray(ring_disk, np.float64).reshape(len(self.ring_ndisk), 64, 3)
+
+    @staticmethod
+    def empty():
+        return Models(np.zeros(0), np.zeros(0), np.zeros((0, 77)), np.zeros(0), np.zeros((0, 4)), np.zeros((0, 64, 3)))
+
+    def struct(self) -> EphModels:
+        i32 = ctypes.POINTER(ctypes.c_int32)
+        return EphModels(len(self.gp_nz), self.gp_nz.ctypes.data_as(i32), self.gp_nt.ctypes.data_as(i32),
+                         _dptr(self.gp_coef), len(self.ring_ndisk), self.ring_ndisk.ctypes.data_as(i32),
+                         _dptr(self.ring_param), _dptr(self.ring_disk))
+
+
+class Context:
+    """One device context holding one system (include/eph_b200.h)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load_library()
+        h = ctypes.c_void_p()
+        check(self.lib.eph_ctx_create(device, ctypes.byref(h)), None, "eph_ctx_create")
+        self.h = h
+        self.n = 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.eph_ctx_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def upload(self, planes: np.ndarray, models: Models | None = None):
+        pl = np.ascontiguousarray(planes, np.float64)
+        assert pl.shape[0] == NPLANES
+        self._models = models or Models.empty()
+        st = self._models.struct()
+        check(self.lib.eph_upload_system(self.h, pl.shape[1], _dptr(pl), ctypes.byref(st)), self.h, "upload")
+        self.n = pl.shape[1]
+
+    def upload_device(self, d_ptr: int):
+        check(self.lib.eph_upload_planes_device(self.h, ctypes.c_void_p(d_ptr)), self.h, "upload_device")
+
+    def device_planes_ptr(self) -> int:
+        p = ctypes.c_void_p()
+        check(self.lib.eph_device_planes(self.h, ctypes.byref(p)), self.h, "device_planes")
+        return p.value
+
+    def download(self, out: np.ndarray | None = None) -> np.ndarray:
+        out = np.empty((NPLANES, self.n)) if out is None else out
+        check(self.lib.eph_download_system(self.h, _dptr(out)), self.h, "download")
+        return out
+
+    def rk12(self, dt: float, n_step: int, t_eph=(0.0, 0.0)):
+        check(self.lib.eph_rk12(self.h, dt, n_step, t_eph[0], t_eph[1]), self.h, "rk12")
+
+    def integrate(self, dt: float, n_step: int, t_eph=(0.0, 0.0)):
+        hi, lo = ctypes.c_double(t_eph[0]), ctypes.c_double(t_eph[1])
+        check(self.lib.eph_integrate(self.h, dt, n_step, ctypes.byref(hi), ctypes.byref(lo)), self.h, "integrate")
+        return hi.value, lo.value
+
+    def accel(self):
+        check(self.lib.eph_accel(self.h), self.h, "accel")
+
+    def deform(self):
+        check(self.lib.eph_deform(self.h), self.h, "deform")
+
+    def set_stream(self, stream_handle: int | None):
+        check(self.lib.eph_set_stream(self.h, ctypes.c_void_p(stream_handle or 0)), self.h, "set_stream")
+
+    def set_launch(self, grid: int = 0, bodies_per_cta: int = 0):
+        check(self.lib.eph_set_launch(self.h, grid, bodies_per_cta), self.h, "set_launch")
+
+    def launch_shape(self):
+        g, b = ctypes.c_int(), ctypes.c_int()
+        check(self.lib.eph_get_launch(self.h, ctypes.byref(g), ctypes.byref(b)), self.h, "get_launch")
+        return g.value, b.value
+
+    def launches(self) -> int:
+        return int(self.lib.eph_launch_count(self.h))
+
+
+class MSystem:
+    """A system of bodies loaded from the reference's initials files and integrated on the GPU."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load_library()
+        self.device = device
+        self.h = None
+
+    def load(self, fconfig: str) -> bool:
+        self.close()
+        h = ctypes.c_void_p()
+        rc = self.lib.eph_msystem_load(fconfig.encode(), self.device, ctypes.byref(h))
+        if rc != 0:
+            return False
+        self.h = h
+        return True
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.eph_msystem_free(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def _need(self):
+        if not self.h:
+            raise RuntimeError("no system loaded")
+
+    def size(self) -> int:
+        self._need()
+        return int(self.lib.eph_msystem_size(self.h))
+
+    __len__ = size
+
+    def integrate(self, dt: float, n_step: int, USE_GPU: int = GPU_RK12):
+        self._need()
+        rc = self.lib.eph_msystem_integrate(self.h, dt, n_step, USE_GPU)
+        check(rc, None, (self.lib.eph_msystem_error(self.h) or b"").decode())
+
+    def accel(self, parallel_option: int = 1):
+        self._need()
+        rc = self.lib.eph_msystem_accel(self.h, parallel_option)
+        check(rc, None, (self.lib.eph_msystem_error(self.h) or b"").decode())
+
+    @property
+    def t_eph(self):
+        hi, lo = ctypes.c_double(), ctypes.c_double()
+        self.lib.eph_msystem_t_eph(self.h, ctypes.byref(hi), ctypes.byref(lo))
+        return hi.value, lo.value
+
+    def ephemeris_time(self) -> int:
+        hi, lo = self.t_eph
+        return int(np.floor(hi + lo))
+
+    @property
+    def delta_t(self) -> float:
+        return float(self.lib.eph_msystem_delta_t(self.h))
+
+    @property
+    def integrator(self) -> int:
+        return int(self.lib.eph_msystem_integrator(self.h))
+
+    def planes(self) -> np.ndarray:
+        self._need()
+        out = np.empty((NPLANES, self.size()))
+        check(self.lib.eph_msystem_get_planes(self.h, _dptr(out)), None, "get_planes")
+        return out
+
+    def set_planes(self, planes: np.ndarray):
+        self._need()
+        pl = np.ascontiguousarray(planes, np.float64)
+        check(self.lib.eph_msystem_set_planes(self.h, _dptr(pl)), None, "set_planes")
+
+    def models(self) -> Models:
+        st = EphModels()
+        check(self.lib.eph_msystem_models(self.h, ctypes.byref(st)), None, "models")
+        ng, nr = st.n_gp, st.n_ring
+        take = lambda p, n, dt: np.ctypeslib.as_array(p, (n,)).astype(dt).copy() if n else np.zeros(0, dt)
+        return Models(take(st.gp_nz, ng, np.int32), take(st.gp_nt, ng, np.int32), take(st.gp_coef, ng * 77, np.float64),
+                      take(st.ring_ndisk, nr, np.int32), take(st.ring_param, nr * 4, np.float64),
+                      take(st.ring_disk, nr * 64 * 3, np.float64))
+
+    def sids(self):
+        out = np.zeros(self.size(), np.uint64)
+        self.lib.eph_msystem_sids(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)))
+        return [int(s).to_bytes(8, "little").rstrip(b"\0").decode() for s in out]
+
+    def __getitem__(self, i: int) -> dict:
+        pl = self.planes()
+        out = {}
+        for name, p in P.items():
+            w = 3 if name in VEC3 else 9 if name in MAT9 else 1
+            out[name.lower()] = pl[p:p + w, i].copy() if w > 1 else float(pl[p, i])
+        return out
+
+    def context(self) -> ctypes.c_void_p:
+        return self.lib.eph_msystem_ctx(self.h)
+
+
+def set_log_level(level: int):
+    load_library().eph_set_log_level(level)

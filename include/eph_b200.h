@@ -1,0 +1,98 @@
+/*
+ * eph_b200.h - C ABI of the B200 RK12 library (libeph_b200.so).
+ *
+ * Drop-in boundary for the reference's GPU integrator path. The reference reaches its GPU code through
+ * two private msystem members defined in their own translation unit:
+ *   void msystem::Cuda_RungeKutta12(fast_real dt, int_t n_step)   src/physics/mass.h:268, src/integrators/RungeKutta.cu:391-412
+ *   void msystem::Cuda_accel()                                    src/physics/mass.h:270, src/integrators/RungeKutta.cu:418-438
+ * called from msystem::integrate(dt, n_step, USE_GPU=1) (src/physics/mass.cpp:408-409) and
+ * msystem::accel(parallel_option>0) (src/physics/mass.cpp:218-220). A replacement translation unit
+ * marshals the `mass` list into the plane layout of eph_planes.h and calls the functions below
+ * (see INTEGRATION.md). All functions return an eph_status; none throws, exits or traps.
+ *
+ * Threading: one context per system; calls on one context are serialised by the context (the
+ * reference serialises all GPU work on a global mutex, RungeKutta.cu:25,396,410). Different contexts
+ * may be used from different host threads.
+ */
+#ifndef EPH_B200_H
+#define EPH_B200_H
+#include <stddef.h>
+#include <stdint.h>
+#include "eph_planes.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum eph_status {
+    EPH_OK = 0,
+    EPH_ERR_ARG = 1,          /* bad argument (null pointer, size out of range, unknown option) */
+    EPH_ERR_CUDA = 2,         /* a CUDA runtime call failed; eph_last_error() has the text */
+    EPH_ERR_OOM = 3,          /* device allocation failed */
+    EPH_ERR_TIMEOUT = 4,      /* a bounded device-side wait gave up; the context stays usable */
+    EPH_ERR_STATE = 5,        /* no system uploaded */
+    EPH_ERR_LOAD = 6,         /* a config / initials file was missing or malformed */
+    EPH_ERR_UNSUPPORTED = 7   /* requested path is not provided by this library (e.g. a CPU integrator) */
+} eph_status;
+
+/* Geopotential and ring tables of a system (layouts in eph_planes.h). Model k of each kind belongs to
+ * the body whose EPH_P_GP_INDEX / EPH_P_RING_INDEX plane holds k. */
+typedef struct eph_models {
+    int32_t n_gp;
+    const int32_t *gp_nz;     /* [n_gp] maximum zonal degree (geopotential.h:7) */
+    const int32_t *gp_nt;     /* [n_gp] maximum tesseral degree */
+    const double *gp_coef;    /* [n_gp][EPH_GP_TABLE_SIZE] packed J/C/S coefficients (geopotential.impl:21-24) */
+    int32_t n_ring;
+    const int32_t *ring_ndisk;   /* [n_ring] number of signed disks (ring.h:8) */
+    const double *ring_param;    /* [n_ring][4] GM_ratio, A, J2, GL_R2 (ring.h:12) */
+    const double *ring_disk;     /* [n_ring][EPH_RING_MAX_DISKS][3] GsR2, R_R, H_R (ring.h:14-19) */
+} eph_models;
+
+typedef struct eph_ctx eph_ctx;
+
+/* Create a context on CUDA device `device`. Replaces the reference's static device-memory cache
+ * (RungeKutta.cu:38-47): buffers are allocated at upload and kept until the next larger upload. */
+int eph_ctx_create(int device, eph_ctx **out);
+int eph_ctx_destroy(eph_ctx *ctx);
+/* Text of the last error on this context (never NULL). */
+const char *eph_last_error(const eph_ctx *ctx);
+
+/* Copy a system (planes [EPH_NPLANES][n] in host memory) and its models to the device
+ * (cuda_rungekutta_kernel_config::load, RungeKutta.cu:77-122). */
+int eph_upload_system(eph_ctx *ctx, int64_t n, const double *planes, const eph_models *models);
+/* Same, with `planes` already in device memory of this context's device. */
+int eph_upload_planes_device(eph_ctx *ctx, const double *d_planes);
+/* Copy the whole body state back (cuda_rungekutta_kernel_config::save, RungeKutta.cu:124-133). */
+int eph_download_system(eph_ctx *ctx, double *planes);
+/* Device copy of the planes [EPH_NPLANES][n] (valid until the next upload of a larger system). */
+int eph_device_planes(eph_ctx *ctx, double **d_planes);
+
+/* msystem::Cuda_RungeKutta12(dt, n_step) (RungeKutta.cu:391-412): n_step Feagin RK12 steps of dt
+ * starting at ephemeris time t_eph = t_eph_hi + t_eph_lo (double-double). Per-pair maxima
+ * accumulate into min_distance (of 1/r) and max_influence; they are neither reset nor inverted. */
+int eph_rk12(eph_ctx *ctx, double dt, int64_t n_step, double t_eph_hi, double t_eph_lo);
+/* msystem::integrate(dt, n_step, USE_GPU=1) without the log lines (mass.cpp:399-442): a negative n_step
+ * integrates backwards, the maxima are reset before and min_distance inverted after, and the
+ * double-double t_eph advances by dt*n_step. */
+int eph_integrate(eph_ctx *ctx, double dt, int64_t n_step, double *t_eph_hi, double *t_eph_lo);
+/* msystem::Cuda_accel() (RungeKutta.cu:418-438): one acceleration evaluation of the uploaded state. */
+int eph_accel(eph_ctx *ctx);
+/* msystem::deform() (mass.cpp:104-110): tidal / rotational deformation of every body at the uploaded
+ * state (potential, Newtonian acceleration, C_potential, GI), as used by the loader. */
+int eph_deform(eph_ctx *ctx);
+
+/* Issue this context's device work on `stream` (a cudaStream_t of the context's device; NULL restores
+ * the context's own stream). Calls still return only after their work has finished. */
+int eph_set_stream(eph_ctx *ctx, void *stream);
+
+/* Launch shape: grid = CTAs (0: automatic), bodies_per_cta (0: automatic). Used by the autotuner. */
+int eph_set_launch(eph_ctx *ctx, int grid, int bodies_per_cta);
+/* Current launch shape. */
+int eph_get_launch(const eph_ctx *ctx, int *grid, int *bodies_per_cta);
+/* Kernel launches issued on this context so far. */
+int64_t eph_launch_count(const eph_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -709,7 +709,8 @@ static dd rk_coef(int64_t idx) {
     return c;
 }
 
-static void rk12(int64_t n, body *x, const orc_models *md, double dt, int64_t n_step, dd t_eph, double *stage_acc) {
+static void rk12(int64_t n, body *x, const orc_models *md, double dt, int64_t n_step, dd t_eph, double *stage_acc,
+                 double *stage_in, double *stage_out) {
     stage_state *x0 = (stage_state *)malloc(sizeof(stage_state) * (size_t)(n ? n : 1));
     stage_state *f = (stage_state *)malloc(sizeof(stage_state) * (size_t)(25 * (n ? n : 1)));
     int64_t n_rec = 0;
@@ -785,34 +786,45 @@ static void rk12(int64_t n, body *x, const orc_models *md, double dt, int64_t n_
                 xi->GM = xi->GM0 + xi->dGM * t;
                 xi->exJ2 = xi->dJ2 * t;
             }
+            if (stage_in) store_bodies(n, stage_in + n_rec * (int64_t)EPH_NPLANES * n, x);
             accel_serial(n, x, md);
+            if (stage_out) store_bodies(n, stage_out + n_rec * (int64_t)EPH_NPLANES * n, x);
             if (stage_acc) {
                 double *o = stage_acc + n_rec * 3 * n;
                 for (int64_t i = 0; i < n; ++i) {
                     v3 a = v3_add(v3_add(x[i].gaccel, x[i].daccel), x[i].naccel);
                     o[i] = a.x; o[n + i] = a.y; o[2 * n + i] = a.z;
                 }
-                ++n_rec;
             }
+            ++n_rec;
         }
     }
     free(x0);
     free(f);
 }
 
-void orc_integrate(int64_t n, double *planes, const orc_models *models, double dt, int64_t n_step,
-                   double *t_eph_hi, double *t_eph_lo, double *stage_acc) {
+static void integrate_impl(int64_t n, double *planes, const orc_models *models, double dt, int64_t n_step,
+                           double *t_eph_hi, double *t_eph_lo, double *stage_acc, double *stage_in, double *stage_out) {
     if (n_step == 0) return;   /* mass.cpp:400-404 */
     if (n_step < 0) { n_step = -n_step; dt = -dt; }
     body *b = (body *)malloc(sizeof(body) * (size_t)(n ? n : 1));
     load_bodies(n, planes, b);
     for (int64_t i = 0; i < n; ++i) b[i].max_influence = b[i].min_distance = 0;   /* mass.cpp:406 */
     dd t_eph = {*t_eph_hi, *t_eph_lo};
-    rk12(n, b, models, dt, n_step, t_eph, stage_acc);
+    rk12(n, b, models, dt, n_step, t_eph, stage_acc, stage_in, stage_out);
     for (int64_t i = 0; i < n; ++i) b[i].min_distance = 1 / b[i].min_distance;   /* mass.cpp:416 */
     t_eph = dd_add(t_eph, dd_make(dt * (double)n_step));   /* mass.cpp:441 */
     *t_eph_hi = t_eph.hi;
     *t_eph_lo = t_eph.lo;
     store_bodies(n, planes, b);
     free(b);
+}
+
+void orc_integrate(int64_t n, double *planes, const orc_models *models, double dt, int64_t n_step,
+                   double *t_eph_hi, double *t_eph_lo, double *stage_acc) {
+    integrate_impl(n, planes, models, dt, n_step, t_eph_hi, t_eph_lo, stage_acc, NULL, NULL);
+}
+void orc_integrate_stages(int64_t n, double *planes, const orc_models *models, double dt, int64_t n_step,
+                          double *t_eph_hi, double *t_eph_lo, double *stage_in, double *stage_out) {
+    integrate_impl(n, planes, models, dt, n_step, t_eph_hi, t_eph_lo, NULL, stage_in, stage_out);
 }

@@ -47,6 +47,11 @@ void orc_deform(int64_t n, double *planes, const orc_models *models);
 void orc_integrate(int64_t n, double *planes, const orc_models *models, double dt, int64_t n_step,
                    double *t_eph_hi, double *t_eph_lo, double *stage_acc);
 
+/* As orc_integrate, also capturing the full body planes right before (stage_in) and right after
+ * (stage_out) each of the 25*n_step accel() calls, as [stage][EPH_NPLANES][n]. Either may be NULL. */
+void orc_integrate_stages(int64_t n, double *planes, const orc_models *models, double dt, int64_t n_step,
+                          double *t_eph_hi, double *t_eph_lo, double *stage_in, double *stage_out);
+
 /* Single evaluations of the extended-body models, for tests. */
 void orc_geopotential_sum(const orc_models *models, int32_t k, double R, const double r[3], double out[3]);
 void orc_ring_sum(const orc_models *models, int32_t k, double R, const double r[3], double out[3]);

@@ -74,6 +74,8 @@ class Oracle:
         L.orc_deform.argtypes = [ctypes.c_int64, _c_double_p, ctypes.POINTER(_OrcModels)]
         L.orc_integrate.argtypes = [ctypes.c_int64, _c_double_p, ctypes.POINTER(_OrcModels), ctypes.c_double,
                                     ctypes.c_int64, _c_double_p, _c_double_p, _c_double_p]
+        L.orc_integrate_stages.argtypes = [ctypes.c_int64, _c_double_p, ctypes.POINTER(_OrcModels), ctypes.c_double,
+                                           ctypes.c_int64, _c_double_p, _c_double_p, _c_double_p, _c_double_p]
         L.orc_geopotential_sum.argtypes = [ctypes.POINTER(_OrcModels), ctypes.c_int32, ctypes.c_double,
                                            _c_double_p, _c_double_p]
         L.orc_ring_sum.argtypes = L.orc_geopotential_sum.argtypes
@@ -100,6 +102,20 @@ class Oracle:
         acc = np.zeros((25 * abs(n_step), 3, n)) if stage_acc else None
         self.L.orc_integrate(n, _ptr(p), ctypes.byref(s), dt, n_step, ctypes.byref(th), ctypes.byref(tl), _ptr(acc))
         return p, (th.value, tl.value), acc
+
+    def integrate_stages(self, planes, models, dt, n_step, t_eph=(0.0, 0.0)):
+        """integrate() returning (planes, t_eph, stage_in, stage_out): the body planes right before
+        and right after each of the 25*n_step accel() calls, each [stage][NPLANES][n]."""
+        p = np.ascontiguousarray(planes, dtype=np.float64).copy()
+        n = p.shape[1]
+        s, keep = _orc_models(models)
+        th = ctypes.c_double(t_eph[0])
+        tl = ctypes.c_double(t_eph[1])
+        sin = np.zeros((25 * n_step, NPLANES, n))
+        sout = np.zeros((25 * n_step, NPLANES, n))
+        self.L.orc_integrate_stages(n, _ptr(p), ctypes.byref(s), dt, n_step, ctypes.byref(th), ctypes.byref(tl),
+                                    _ptr(sin), _ptr(sout))
+        return p, (th.value, tl.value), sin, sout
 
     def geopotential_sum(self, models, k, R, r):
         s, keep = _orc_models(models)
