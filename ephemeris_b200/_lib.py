@@ -45,6 +45,9 @@ SIGNATURES = [
     ("eph_set_launch", ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int]),
     ("eph_get_launch", ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     ("eph_launch_count", ctypes.c_int64, [_VP]),
+    ("eph_profile_phases", ctypes.c_int, [_VP, ctypes.c_int]),
+    ("eph_phase_times", ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_int),
+                                       ctypes.POINTER(ctypes.c_int)]),
     ("eph_msystem_load", ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(_VP)]),
     ("eph_msystem_free", ctypes.c_int, [_VP]),
     ("eph_msystem_size", ctypes.c_int64, [_VP]),

@@ -40,6 +40,8 @@ struct eph_ctx {
     int grid = 0, per_cta = 0;           // current launch shape
     int req_grid = 0, req_per_cta = 0;   // requested by eph_set_launch (0 = automatic)
     int64_t launches = 0;
+    unsigned long long *d_timers = nullptr;   // phase timers of the last launch, when profiling
+    int timers_grid = 0;
 };
 
 static int fail(eph_ctx *c, int code, const char *what, cudaError_t e = cudaSuccess) {
@@ -97,6 +99,7 @@ int eph_ctx_destroy(eph_ctx *ctx) {
     if (!ctx) return EPH_ERR_ARG;
     cudaSetDevice(ctx->device);
     free_system(ctx);
+    if (ctx->d_timers) cudaFree(ctx->d_timers);
     if (ctx->d_bar) cudaFree(ctx->d_bar);
     if (ctx->d_status) cudaFree(ctx->d_status);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
@@ -314,6 +317,16 @@ static int run(eph_ctx *ctx, const StepParams &P) {
     S.own_list = ctx->d_own;
     S.bar = ctx->d_bar;
     S.status = ctx->d_status;
+    S.timers = nullptr;
+    if (ctx->d_timers) {
+        if (ctx->timers_grid < ctx->grid) {
+            cudaFree(ctx->d_timers);
+            ctx->d_timers = nullptr;
+            CK(cudaMalloc(&ctx->d_timers, (size_t)ctx->grid * kPhases * sizeof(unsigned long long)), "cudaMalloc(timers)");
+            ctx->timers_grid = ctx->grid;
+        }
+        S.timers = ctx->d_timers;
+    }
     CK(cudaMemsetAsync(ctx->d_bar, 0, 2 * sizeof(unsigned), ctx->stream), "reset barrier");
     CK(cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->stream), "reset status");
     CK(launch_step(S, P, ctx->grid, ctx->stream), "launch RK12 kernel");
@@ -398,5 +411,36 @@ int eph_get_launch(const eph_ctx *ctx, int *grid, int *bodies_per_cta) {
 }
 
 int64_t eph_launch_count(const eph_ctx *ctx) { return ctx ? ctx->launches : -1; }
+
+int eph_profile_phases(eph_ctx *ctx, int enable) {
+    if (!ctx) return EPH_ERR_ARG;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    if (!enable) {
+        if (ctx->d_timers) cudaFree(ctx->d_timers);
+        ctx->d_timers = nullptr;
+        ctx->timers_grid = 0;
+        return EPH_OK;
+    }
+    if (!ctx->d_timers) {
+        const int g = std::max(ctx->grid, 1);
+        CK(cudaMalloc(&ctx->d_timers, (size_t)g * kPhases * sizeof(unsigned long long)), "cudaMalloc(timers)");
+        CK(cudaMemset(ctx->d_timers, 0, (size_t)g * kPhases * sizeof(unsigned long long)), "cudaMemset(timers)");
+        ctx->timers_grid = g;
+    }
+    return EPH_OK;
+}
+
+int eph_phase_times(eph_ctx *ctx, uint64_t *out, int *grid, int *phases) {
+    if (!ctx || !out || !grid || !phases) return EPH_ERR_ARG;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    if (!ctx->d_timers) return fail(ctx, EPH_ERR_STATE, "phase timers are off");
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    CK(cudaMemcpy(out, ctx->d_timers, (size_t)ctx->grid * kPhases * sizeof(unsigned long long), cudaMemcpyDeviceToHost),
+       "read timers");
+    *grid = ctx->grid;
+    *phases = kPhases;
+    return EPH_OK;
+}
 
 }  // extern "C"

@@ -69,8 +69,21 @@ struct Own {
 struct Scratch {
     double red[kThreads / 32][kRegBodies][13];
     double ext[kOwnMax][kMaxExt][3];
+    unsigned long long t_last, t_phase[kPhases];
     int flag;
 };
+
+__device__ __forceinline__ unsigned long long global_ns();
+
+// Optional phase timers: thread 0 charges the time since the previous mark to phase `ph`. Marks sit
+// right after a __syncthreads(), so they bound the whole CTA's work of the phase.
+__device__ __forceinline__ void mark(const SysDev &S, Scratch &sc, int ph) {
+    if (S.timers && threadIdx.x == 0) {
+        unsigned long long t = global_ns();
+        sc.t_phase[ph] += t - sc.t_last;
+        sc.t_last = t;
+    }
+}
 
 // ------------------------------------------------------------------ small helpers
 __device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
@@ -419,6 +432,7 @@ __device__ void pass_a(const SysDev &S, Own *own, int nb, int buf, bool deform_o
             }
             __syncthreads();
         }
+        mark(S, sc, PH_A_SWEEP);
         if (threadIdx.x < nb) {
             Own &o = own[threadIdx.x];
             if (!o.converged) {
@@ -427,6 +441,7 @@ __device__ void pass_a(const SysDev &S, Own *own, int nb, int buf, bool deform_o
             }
         }
         __syncthreads();
+        mark(S, sc, PH_A_UPDATE);
         int all = 1;
         for (int b = 0; b < nb; ++b) all &= own[b].converged;
         if (all) break;
@@ -456,6 +471,7 @@ __device__ void pass_a(const SysDev &S, Own *own, int nb, int buf, bool deform_o
         if (o.gl_fixed) publish_body(S, o, buf);
     }
     __syncthreads();
+    mark(S, sc, PH_A_UPDATE);
 }
 
 // ------------------------------------------------------------------ pass B: main force
@@ -597,6 +613,7 @@ __device__ void pass_b(const SysDev &S, Own *own, int nb, int buf, Scratch &sc, 
         }
         __syncthreads();
     }
+    mark(S, sc, PH_B_SWEEP);
     // forces of the other extended bodies' geopotentials and rings on the owned bodies
     // (the `mj.daccel += mi.GM*an` half of APPLY_NONPOINT_FORCE, mass.impl:127-128)
     const int n_ext = S.n_ext;
@@ -628,6 +645,7 @@ __device__ void pass_b(const SysDev &S, Own *own, int nb, int buf, Scratch &sc, 
         sc.ext[b][e][0] = add3.x; sc.ext[b][e][1] = add3.y; sc.ext[b][e][2] = add3.z;
     }
     __syncthreads();
+    mark(S, sc, PH_B_EXT);
     // finalisation (mass.cpp:389-396): FINALIZE_RELATIVITY and RING_CORRECTION
     const double c2 = kC * kC;
     for (int b = threadIdx.x; b < nb; b += blockDim.x) {
@@ -653,6 +671,7 @@ __device__ void pass_b(const SysDev &S, Own *own, int nb, int buf, Scratch &sc, 
         stv(o.fa, (ga + da) + na);
     }
     __syncthreads();
+    mark(S, sc, PH_B_FINAL);
 }
 
 // ------------------------------------------------------------------ RK12 stage combination and update
@@ -763,6 +782,10 @@ __global__ void __launch_bounds__(kThreads, 1) step_kernel(SysDev S, StepParams 
     Scratch &sc = *reinterpret_cast<Scratch *>(smem_raw + sizeof(Own) * kOwnMax);
     __shared__ double red_out[kRegBodies * 13];
 
+    if (threadIdx.x == 0) {
+        sc.t_last = global_ns();
+        for (int p = 0; p < kPhases; ++p) sc.t_phase[p] = 0;
+    }
     int nb = 0;
     for (int b = 0; b < kOwnMax; ++b) {
         int id = S.own_list[blockIdx.x * kOwnMax + b];
@@ -774,15 +797,28 @@ __global__ void __launch_bounds__(kThreads, 1) step_kernel(SysDev S, StepParams 
     load_own(S, own, nb, P);
     __syncthreads();
     if (threadIdx.x < nb) publish_body(S, own[threadIdx.x], 0);
+    auto sync = [&]() {
+        bool ok = grid_sync(S, sc);
+        mark(S, sc, PH_BARRIER);
+        return ok;
+    };
+    auto finish = [&](bool deform_only) {
+        store_own(S, own, nb, deform_only);
+        __syncthreads();
+        mark(S, sc, PH_IO);
+        if (S.timers && threadIdx.x == 0)
+            for (int p = 0; p < kPhases; ++p) S.timers[blockIdx.x * kPhases + p] = sc.t_phase[p];
+    };
+    mark(S, sc, PH_IO);
 
     if (P.mode == MODE_DEFORM || P.mode == MODE_ACCEL) {
-        if (!grid_sync(S, sc)) return;
+        if (!sync()) return;
         pass_a(S, own, nb, 0, P.mode == MODE_DEFORM, sc, red_out);
         if (P.mode == MODE_ACCEL) {
-            if (!grid_sync(S, sc)) return;
+            if (!sync()) return;
             pass_b(S, own, nb, 0, sc, red_out);
         }
-        store_own(S, own, nb, P.mode == MODE_DEFORM);
+        finish(P.mode == MODE_DEFORM);
         return;
     }
     // MODE_INTEGRATE: the loaded auxiliaries are f_0 of the first step
@@ -795,16 +831,17 @@ __global__ void __launch_bounds__(kThreads, 1) step_kernel(SysDev S, StepParams 
     for (long long step = 0; step < P.n_step; ++step) {
         for (int s = 0; s < kStages; ++s) {
             rk_stage(S, own, nb, s, step, P, buf ^ 1);
+            mark(S, sc, PH_RK);
             buf ^= 1;
-            if (!grid_sync(S, sc)) return;
+            if (!sync()) return;
             pass_a(S, own, nb, buf, false, sc, red_out);
-            if (!grid_sync(S, sc)) return;
+            if (!sync()) return;
             pass_b(S, own, nb, buf, sc, red_out);
         }
     }
     if (P.invert_min && threadIdx.x < nb) own[threadIdx.x].mind = 1 / own[threadIdx.x].mind;
     __syncthreads();
-    store_own(S, own, nb, false);
+    finish(false);
 }
 
 }  // namespace eph

@@ -48,7 +48,12 @@ struct SysDev {
     const int *own_list;      // [grid][kOwnMax], -1 padded
     unsigned int *bar;        // grid barrier words {count, generation}
     int *status;              // device status word (0 = ok)
+    unsigned long long *timers;   // optional [grid][kPhases] nanoseconds per phase (profiling), or null
 };
+
+// phases of a stage evaluation, for the optional per-CTA phase timers
+enum Phase { PH_IO = 0, PH_RK = 1, PH_BARRIER = 2, PH_A_SWEEP = 3, PH_A_UPDATE = 4, PH_B_SWEEP = 5,
+             PH_B_EXT = 6, PH_B_FINAL = 7, kPhases = 8 };
 
 enum Mode { MODE_INTEGRATE = 0, MODE_ACCEL = 1, MODE_DEFORM = 2 };
 

@@ -122,6 +122,20 @@ class Context:
     def launches(self) -> int:
         return int(self.lib.eph_launch_count(self.h))
 
+    PHASES = ("io", "rk", "barrier", "a_sweep", "a_update", "b_sweep", "b_ext", "b_final")
+
+    def profile_phases(self, enable: bool = True):
+        check(self.lib.eph_profile_phases(self.h, 1 if enable else 0), self.h, "profile_phases")
+
+    def phase_times(self) -> np.ndarray:
+        """[grid, 8] nanoseconds per phase of the last launch (profiling must be on)."""
+        g, p = self.launch_shape()
+        out = np.zeros(max(g, 1) * 8, np.uint64)
+        gg, pp = ctypes.c_int(), ctypes.c_int()
+        check(self.lib.eph_phase_times(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)),
+                                       ctypes.byref(gg), ctypes.byref(pp)), self.h, "phase_times")
+        return out[:gg.value * pp.value].reshape(gg.value, pp.value)
+
 
 class MSystem:
     """A system of bodies loaded from the reference's initials files and integrated on the GPU."""

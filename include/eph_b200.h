@@ -92,6 +92,13 @@ int eph_get_launch(const eph_ctx *ctx, int *grid, int *bodies_per_cta);
 /* Kernel launches issued on this context so far. */
 int64_t eph_launch_count(const eph_ctx *ctx);
 
+/* Profiling aid: with enable != 0 every launch records, per CTA, the nanoseconds spent in each phase
+ * of the step (load/store, RK combination, barrier waits, pass-A sweeps, pass-A updates, pass-B sweeps,
+ * extended-body forces, finalisation). eph_phase_times copies the last launch's [grid][phases] table
+ * (out must hold grid*8 values; grid = CTAs of the current launch shape). */
+int eph_profile_phases(eph_ctx *ctx, int enable);
+int eph_phase_times(eph_ctx *ctx, uint64_t *out, int *grid, int *phases);
+
 #ifdef __cplusplus
 }
 #endif

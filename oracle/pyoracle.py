@@ -111,8 +111,9 @@ class Oracle:
         s, keep = _orc_models(models)
         th = ctypes.c_double(t_eph[0])
         tl = ctypes.c_double(t_eph[1])
-        sin = np.zeros((25 * n_step, NPLANES, n))
-        sout = np.zeros((25 * n_step, NPLANES, n))
+        # constants and model links are not rewritten per stage: start every stage from the input planes
+        sin = np.repeat(p[None], 25 * n_step, axis=0)
+        sout = sin.copy()
         self.L.orc_integrate_stages(n, _ptr(p), ctypes.byref(s), dt, n_step, ctypes.byref(th), ctypes.byref(tl),
                                     _ptr(sin), _ptr(sout))
         return p, (th.value, tl.value), sin, sout
@@ -133,59 +134,70 @@ class Oracle:
 
 
 REF_LIB = os.path.join(HERE, "_ref", "libephref.so")
+BRIDGE_LIB = os.path.join(HERE, "_ref", "libephref_b200.so")
+_REF_LIBS = {}
 
 
-def ref_available() -> bool:
-    return os.path.exists(REF_LIB)
+def ref_available(path: str = REF_LIB) -> bool:
+    return os.path.exists(path)
+
+
+def _ref_lib(path):
+    if path not in _REF_LIBS:
+        L = ctypes.CDLL(path)
+        L.ref_load.restype = ctypes.c_void_p
+        L.ref_load.argtypes = [ctypes.c_char_p]
+        L.ref_free.argtypes = [ctypes.c_void_p]
+        L.ref_clone.restype = ctypes.c_void_p
+        L.ref_clone.argtypes = [ctypes.c_void_p]
+        L.ref_size.restype = ctypes.c_int64
+        L.ref_size.argtypes = [ctypes.c_void_p]
+        L.ref_get_t_eph.argtypes = [ctypes.c_void_p, _c_double_p, _c_double_p]
+        L.ref_delta_t.restype = ctypes.c_double
+        L.ref_delta_t.argtypes = [ctypes.c_void_p]
+        L.ref_set_log_level.argtypes = [ctypes.c_int]
+        L.ref_thread_pool.argtypes = [ctypes.c_int]
+        L.ref_integrate.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int64]
+        L.ref_integrate_gpu.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int64]
+        L.ref_accel.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.ref_deform.argtypes = [ctypes.c_void_p]
+        L.ref_get_planes.argtypes = [ctypes.c_void_p, _c_double_p, ctypes.POINTER(ctypes.c_uint64)]
+        L.ref_set_planes.argtypes = [ctypes.c_void_p, _c_double_p]
+        L.ref_get_models.restype = ctypes.c_int64
+        L.ref_get_models.argtypes = [ctypes.c_void_p, _c_int32_p, _c_int32_p, _c_double_p, _c_int32_p,
+                                     _c_double_p, _c_double_p]
+        L.ref_capture.restype = ctypes.c_int64
+        L.ref_capture.argtypes = [ctypes.c_void_p, _c_double_p, ctypes.c_int64]
+        L.ref_set_log_level(40)   # LogLevel::ERROR: keep step-size warnings quiet
+        _REF_LIBS[path] = L
+    return _REF_LIBS[path]
 
 
 class RefSystem:
-    """One reference `msystem`, loaded by the reference's own loader from a config file."""
-    _L = None
+    """One reference `msystem`, loaded by the reference's own loader from a config file.
 
-    @classmethod
-    def lib(cls):
-        if cls._L is None:
-            L = ctypes.CDLL(REF_LIB)
-            L.ref_load.restype = ctypes.c_void_p
-            L.ref_load.argtypes = [ctypes.c_char_p]
-            L.ref_free.argtypes = [ctypes.c_void_p]
-            L.ref_clone.restype = ctypes.c_void_p
-            L.ref_clone.argtypes = [ctypes.c_void_p]
-            L.ref_size.restype = ctypes.c_int64
-            L.ref_size.argtypes = [ctypes.c_void_p]
-            L.ref_get_t_eph.argtypes = [ctypes.c_void_p, _c_double_p, _c_double_p]
-            L.ref_delta_t.restype = ctypes.c_double
-            L.ref_delta_t.argtypes = [ctypes.c_void_p]
-            L.ref_set_log_level.argtypes = [ctypes.c_int]
-            L.ref_thread_pool.argtypes = [ctypes.c_int]
-            L.ref_integrate.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int64]
-            L.ref_accel.argtypes = [ctypes.c_void_p, ctypes.c_int]
-            L.ref_deform.argtypes = [ctypes.c_void_p]
-            L.ref_get_planes.argtypes = [ctypes.c_void_p, _c_double_p, ctypes.POINTER(ctypes.c_uint64)]
-            L.ref_set_planes.argtypes = [ctypes.c_void_p, _c_double_p]
-            L.ref_get_models.restype = ctypes.c_int64
-            L.ref_get_models.argtypes = [ctypes.c_void_p, _c_int32_p, _c_int32_p, _c_double_p, _c_int32_p,
-                                         _c_double_p, _c_double_p]
-            L.ref_capture.restype = ctypes.c_int64
-            L.ref_capture.argtypes = [ctypes.c_void_p, _c_double_p, ctypes.c_int64]
-            L.ref_set_log_level(40)   # LogLevel::ERROR: keep step-size warnings quiet
-            cls._L = L
-        return cls._L
+    lib_path selects the build: libephref.so (CPU only) or libephref_b200.so (the reference with its
+    GPU members served by the B200 bridge)."""
+    _path = REF_LIB
 
-    def __init__(self, config: str | None = None, handle=None):
+    def __init__(self, config: str | None = None, handle=None, lib_path: str | None = None):
+        if lib_path:
+            self._path = lib_path
         L = self.lib()
         self.h = handle if handle is not None else L.ref_load(config.encode())
         if not self.h:
             raise RuntimeError(f"reference loader rejected {config}")
 
+    def lib(self):
+        return _ref_lib(self._path)
+
     def __del__(self):
-        if getattr(self, "h", None) and self._L is not None:
-            self._L.ref_free(self.h)
+        if getattr(self, "h", None):
+            _ref_lib(self._path).ref_free(self.h)
             self.h = None
 
     def clone(self):
-        return RefSystem(handle=self.lib().ref_clone(self.h))
+        return RefSystem(handle=self.lib().ref_clone(self.h), lib_path=self._path)
 
     @property
     def n(self) -> int:
@@ -223,8 +235,11 @@ class RefSystem:
                          _ptr(m.ring_ndisk, _c_int32_p), _ptr(m.ring_param), _ptr(m.ring_disk))
         return m
 
-    def integrate(self, dt: float, n_step: int):
-        self.lib().ref_integrate(self.h, dt, n_step)
+    def integrate(self, dt: float, n_step: int, use_gpu: int = 0):
+        if use_gpu:
+            self.lib().ref_integrate_gpu(self.h, dt, n_step)
+        else:
+            self.lib().ref_integrate(self.h, dt, n_step)
 
     def accel(self, option: int = -1):
         self.lib().ref_accel(self.h, option)
@@ -242,5 +257,5 @@ class RefSystem:
         return buf[:got]
 
     @staticmethod
-    def thread_pool(enable: bool):
-        RefSystem.lib().ref_thread_pool(1 if enable else 0)
+    def thread_pool(enable: bool, lib_path: str = REF_LIB):
+        _ref_lib(lib_path).ref_thread_pool(1 if enable else 0)

@@ -156,6 +156,9 @@ void ref_thread_pool(int enable) {
 }
 
 void ref_integrate(void *h, double dt, int64_t n_step) { ((msystem *)h)->integrate(dt, n_step, 0); }
+/* msystem::integrate(dt, n, USE_GPU=1): the reference's GPU branch, i.e. whatever translation unit
+ * defines msystem::Cuda_RungeKutta12 in this library (the B200 bridge in libephref_b200.so). */
+void ref_integrate_gpu(void *h, double dt, int64_t n_step) { ((msystem *)h)->integrate(dt, n_step, 1); }
 void ref_accel(void *h, int option) { ((msystem *)h)->accel(option); }
 void ref_deform(void *h) { ephemeris_reader::deform(*(msystem *)h); }
 
@@ -238,15 +241,3 @@ int64_t ref_capture_count(void) { return g_rec.count; }
 
 }  // extern "C"
 
-/* The CUDA integrator (src/integrators/RungeKutta.cu) is not part of this CPU build. */
-void msystem::Cuda_RungeKutta12(fast_real, int_t) {
-    LogCritical("reference CUDA path is not built into the CPU oracle library\n");
-    abort();
-}
-void msystem::Cuda_accel() {
-    LogCritical("reference CUDA path is not built into the CPU oracle library\n");
-    abort();
-}
-/* src/modules/ephemeris_generator.cpp:303-304: returns at once unless a combined-integrator
- * subsystem is attached, which never happens through these entry points. */
-void msystem::record_substeps(fast_real, bool) {}

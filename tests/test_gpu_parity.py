@@ -140,8 +140,10 @@ def test_loader_matches_reference(golden):
     # state and constants are parsed and built identically
     for p in list(range(0, 36)) + list(range(39, 56)) + [102, 103]:
         assert np.array_equal(pl[p], ref[p]), p
-    # static harmonics corrected by the device deformation and the initial acceleration
-    assert rel_err(pl[56:65], ref[56:65], floor=1e-9) <= 1e-12
+    # static harmonics corrected by the device deformation, relative to each body's matrix scale
+    scale = np.abs(ref[56:65]).max(0)
+    scale[scale == 0] = 1.0
+    assert (np.abs(pl[56:65] - ref[56:65]) / scale).max() <= 1e-13
     assert accel_error(pl, ref) <= ACC_TOL
 
 
