@@ -241,10 +241,13 @@ def run_b200(args):
         ctx.set_stream(stream.cuda_stream)
         flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)   # > 126 MB L2
 
-        # ---- device-resident throughput: CUDA events on the launching stream, L2 flushed between steps
-        t = (0.0, 0.0)
+        # ---- device-resident throughput: CUDA events on the launching stream, L2 flushed between steps.
+        # Every step integrates the same initial state (restored from an HBM snapshot outside the events),
+        # so each timed step is the same workload.
+        snap = torch.from_numpy(planes0.copy()).to(dev)
         for _ in range(args.warmup):
-            t = ctx.integrate(dt, rk, t)
+            ctx.upload_device(snap.data_ptr())
+            ctx.integrate(dt, rk)
         barrier(pg, dev)
         torch.cuda.synchronize(dev)
         clocks = ClockSampler(local)
@@ -253,9 +256,10 @@ def run_b200(args):
         starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
         ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
         for k in range(args.steps):
+            ctx.upload_device(snap.data_ptr())
             flush.fill_(float(k))
             starts[k].record(stream)
-            t = ctx.integrate(dt, rk, t)
+            ctx.integrate(dt, rk)
             ends[k].record(stream)
         torch.cuda.synchronize(dev)
         clk = clocks.stop()

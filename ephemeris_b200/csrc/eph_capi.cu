@@ -13,10 +13,11 @@
 #include "../../include/eph_b200.h"
 
 namespace eph {
-size_t step_smem_bytes();
+size_t step_smem_bytes(int tile);
+int max_tile();
 cudaError_t upload_constants(int device);
 cudaError_t launch_step(const SysDev &S, const StepParams &P, int grid, cudaStream_t stream);
-int max_coresident_ctas(int device, int *out);
+int max_coresident_ctas(int device, int tile, int *out);
 }  // namespace eph
 
 using namespace eph;
@@ -31,7 +32,10 @@ struct eph_ctx {
     int n = 0, n_gp = 0, n_ring = 0, n_ext = 0;
     size_t cap_n = 0;
     int cap_gp = 0, cap_ring = 0;
-    double *d_planes = nullptr, *d_pub = nullptr, *d_aux = nullptr, *d_cst = nullptr;
+    double *d_planes = nullptr, *d_pub = nullptr, *d_aux = nullptr, *d_cst = nullptr, *d_react = nullptr;
+    int ld = 0, tile = 0;                // plane stride (n rounded up to kPad), bodies per smem tile
+    int n_full = 0;                      // full-class bodies (device order)
+    int *d_orig = nullptr;               // [n] device order -> caller order
     int *d_ext = nullptr, *d_own = nullptr, *d_status = nullptr;
     unsigned *d_bar = nullptr;
     int *d_gp_nz = nullptr, *d_gp_nt = nullptr, *d_ring_nd = nullptr;
@@ -61,13 +65,13 @@ static int fail(eph_ctx *c, int code, const char *what, cudaError_t e = cudaSucc
     } while (0)
 
 static void free_system(eph_ctx *ctx) {
-    void *ptrs[] = {ctx->d_planes, ctx->d_pub, ctx->d_aux, ctx->d_cst, ctx->d_ext, ctx->d_own,
+    void *ptrs[] = {ctx->d_planes, ctx->d_pub, ctx->d_aux, ctx->d_cst, ctx->d_react, ctx->d_ext, ctx->d_own, ctx->d_orig,
                     ctx->d_gp_nz, ctx->d_gp_nt, ctx->d_ring_nd, ctx->d_gp_coef, ctx->d_ring_param,
                     ctx->d_ring_disk};
     for (void *p : ptrs)
         if (p) cudaFree(p);
-    ctx->d_planes = ctx->d_pub = ctx->d_aux = ctx->d_cst = nullptr;
-    ctx->d_ext = ctx->d_own = nullptr;
+    ctx->d_planes = ctx->d_pub = ctx->d_aux = ctx->d_cst = ctx->d_react = nullptr;
+    ctx->d_ext = ctx->d_own = ctx->d_orig = nullptr;
     ctx->d_gp_nz = ctx->d_gp_nt = ctx->d_ring_nd = nullptr;
     ctx->d_gp_coef = ctx->d_ring_param = ctx->d_ring_disk = nullptr;
     ctx->cap_n = 0;
@@ -135,7 +139,8 @@ static void plan_ownership(const std::vector<double> &cost, int grid, int cap, s
 
 static int choose_shape(eph_ctx *ctx) {
     int maxc = 0;
-    if (max_coresident_ctas(ctx->device, &maxc) != 0 || maxc <= 0) return fail(ctx, EPH_ERR_CUDA, "occupancy query failed");
+    ctx->tile = std::min(max_tile(), ctx->ld);
+    if (max_coresident_ctas(ctx->device, ctx->tile, &maxc) != 0 || maxc <= 0) return fail(ctx, EPH_ERR_CUDA, "occupancy query failed");
     const int n = ctx->n;
     int per = ctx->req_per_cta, grid = ctx->req_grid;
     if (per <= 0 && grid <= 0) {
@@ -160,31 +165,56 @@ static int choose_shape(eph_ctx *ctx) {
     return EPH_OK;
 }
 
+// Body class of the device ordering (eph_system.cuh): full if any term beyond point-mass Newtonian + 1PN
+// can be nonzero for the body, as source or as target.
+static bool full_class(const double *h_planes, int n, int i) {
+    auto P = [&](int p) { return h_planes[(size_t)p * n + i]; };
+    if (P(EPH_P_K2) != 0 || P(EPH_P_K2R) != 0 || P(EPH_P_DJ2) != 0 || P(EPH_P_LUM) != 0 || P(EPH_P_RR2G_4C) != 0)
+        return true;
+    if (P(EPH_P_GP_INDEX) >= 0 || P(EPH_P_RING_INDEX) >= 0) return true;
+    for (int q = 0; q < 9; ++q)
+        if (P(EPH_P_C_STATIC + q) != 0) return true;
+    for (int c = 0; c < 3; ++c)
+        if (P(EPH_P_W + c) != 0 || P(EPH_P_GL_HI + c) != 0 || P(EPH_P_GL_LO + c) != 0) return true;
+    return false;
+}
+
 static int prepare_constants(eph_ctx *ctx, const double *h_planes) {
     const int n = ctx->n;
-    std::vector<double> cst((size_t)CST_NPLANES * n);
+    const int ld = ctx->ld;
+    // device order: full-class bodies first, each class in the caller's order
+    std::vector<int> orig;
+    orig.reserve(n);
+    for (int i = 0; i < n; ++i)
+        if (full_class(h_planes, n, i)) orig.push_back(i);
+    ctx->n_full = (int)orig.size();
+    for (int i = 0; i < n; ++i)
+        if (!full_class(h_planes, n, i)) orig.push_back(i);
+    std::vector<double> cst((size_t)CST_NPLANES * ld, 0.0);
     std::vector<int> ext;
     ctx->h_cost.assign(n, 0.0);
-    for (int i = 0; i < n; ++i) {
+    for (int k = 0; k < n; ++k) {
+        const int i = orig[k];
         auto P = [&](int p) { return h_planes[(size_t)p * n + i]; };
-        cst[CST_SR2 * n + i] = P(EPH_P_SR2);
-        cst[CST_TDF * n + i] = P(EPH_P_TIDE_DELAY_FACTOR);
-        cst[CST_R2 * n + i] = P(EPH_P_R2);
-        cst[CST_LUM * n + i] = P(EPH_P_LUM);
-        cst[CST_R * n + i] = P(EPH_P_RADIUS);
-        cst[CST_GP * n + i] = P(EPH_P_GP_INDEX);
-        cst[CST_RING * n + i] = P(EPH_P_RING_INDEX);
+        cst[CST_SR2 * ld + k] = P(EPH_P_SR2);
+        cst[CST_TDF * ld + k] = P(EPH_P_TIDE_DELAY_FACTOR);
+        cst[CST_R2 * ld + k] = P(EPH_P_R2);
+        cst[CST_LUM * ld + k] = P(EPH_P_LUM);
+        cst[CST_R * ld + k] = P(EPH_P_RADIUS);
+        cst[CST_GP * ld + k] = P(EPH_P_GP_INDEX);
+        cst[CST_RING * ld + k] = P(EPH_P_RING_INDEX);
         const bool gp = P(EPH_P_GP_INDEX) >= 0, ring = P(EPH_P_RING_INDEX) >= 0;
-        if (gp || ring) ext.push_back(i);
+        if (gp || ring) ext.push_back(k);
         const bool delayed = P(EPH_P_K2) != 0 && P(EPH_P_TIDE_DELAY) != 0;
-        // relative work: pass A (three sweeps for a delayed tide), pass B, extended-body models
-        ctx->h_cost[i] = (delayed ? 3.0 * 2.0 : 1.0) + 3.0 + (gp ? 4.0 : 0.0) + (ring ? 8.0 : 0.0);
+        // relative work: pass A (three sweeps for a delayed tide), pass B (heavier for the full class)
+        ctx->h_cost[k] = (delayed ? 3.0 * 2.0 : 1.0) + (k < ctx->n_full ? 3.0 : 2.0);
     }
     if ((int)ext.size() > kMaxExt) return fail(ctx, EPH_ERR_ARG, "too many bodies with geopotential or ring models");
     ctx->n_ext = (int)ext.size();
     cudaError_t e = cudaMemcpy(ctx->d_cst, cst.data(), cst.size() * sizeof(double), cudaMemcpyHostToDevice);
     if (e == cudaSuccess && !ext.empty())
         e = cudaMemcpy(ctx->d_ext, ext.data(), ext.size() * sizeof(int), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(ctx->d_orig, orig.data(), orig.size() * sizeof(int), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return fail(ctx, EPH_ERR_CUDA, "upload constants", e);
     return EPH_OK;
 }
@@ -214,12 +244,18 @@ int eph_upload_system(eph_ctx *ctx, int64_t n64, const double *planes, const eph
     if ((size_t)n > ctx->cap_n) {
         free_system(ctx);
         CK(cudaMalloc(&ctx->d_planes, (size_t)EPH_NPLANES * n * sizeof(double)), "cudaMalloc(planes)");
-        CK(cudaMalloc(&ctx->d_pub, (size_t)2 * PUB_NPLANES * n * sizeof(double)), "cudaMalloc(public state)");
-        CK(cudaMalloc(&ctx->d_aux, (size_t)AUX_NPLANES * n * sizeof(double)), "cudaMalloc(aux)");
-        CK(cudaMalloc(&ctx->d_cst, (size_t)CST_NPLANES * n * sizeof(double)), "cudaMalloc(constants)");
+        const int ld = (n + kPad - 1) / kPad * kPad;
+        CK(cudaMalloc(&ctx->d_pub, (size_t)2 * PUB_NPLANES * ld * sizeof(double)), "cudaMalloc(public state)");
+        CK(cudaMalloc(&ctx->d_aux, (size_t)AUX_NPLANES * ld * sizeof(double)), "cudaMalloc(aux)");
+        CK(cudaMalloc(&ctx->d_react, (size_t)kMaxExt * ld * 12 * sizeof(double)), "cudaMalloc(reactions)");
+        CK(cudaMalloc(&ctx->d_cst, (size_t)CST_NPLANES * ld * sizeof(double)), "cudaMalloc(constants)");
+        CK(cudaMemset(ctx->d_aux, 0, (size_t)AUX_NPLANES * ld * sizeof(double)), "cudaMemset");
+        CK(cudaMemset(ctx->d_react, 0, (size_t)kMaxExt * ld * 12 * sizeof(double)), "cudaMemset");
         CK(cudaMalloc(&ctx->d_ext, (size_t)kMaxExt * sizeof(int)), "cudaMalloc(ext)");
         CK(cudaMalloc(&ctx->d_own, (size_t)n * kOwnMax * sizeof(int)), "cudaMalloc(ownership)");
-        CK(cudaMemset(ctx->d_pub, 0, (size_t)2 * PUB_NPLANES * n * sizeof(double)), "cudaMemset");
+        CK(cudaMalloc(&ctx->d_orig, (size_t)n * sizeof(int)), "cudaMalloc(order)");
+        CK(cudaMemset(ctx->d_pub, 0, (size_t)2 * PUB_NPLANES * ld * sizeof(double)), "cudaMemset");
+        ctx->ld = ld;
         ctx->cap_n = n;
     }
     // model tables: reallocated only when a larger table set arrives
@@ -302,6 +338,11 @@ static int run(eph_ctx *ctx, const StepParams &P) {
     if (!ctx->n) return fail(ctx, EPH_ERR_STATE, "no system uploaded");
     SysDev S;
     S.n = ctx->n;
+    S.n_full = ctx->n_full;
+    S.orig = ctx->d_orig;
+    S.ld = ctx->ld;
+    S.tile = ctx->tile;
+    S.react = ctx->d_react;
     S.n_ext = ctx->n_ext;
     S.pub = ctx->d_pub;
     S.aux = ctx->d_aux;

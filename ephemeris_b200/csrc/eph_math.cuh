@@ -81,6 +81,12 @@ __device__ __forceinline__ v3d scale(dd s, v3d a) { return v3d{dd_mul(s, a.x), d
 __device__ __forceinline__ double dd_diff(double ahi, double alo, double bhi, double blo) {
     return dd_val(dd_sub(dd{ahi, alo}, dd{bhi, blo}));
 }
+// The same separation in three operations, for the O(N^2) pair sweeps. When ahi - bhi is exact (any two
+// coordinates within a factor of two of each other, e.g. every close pair), the result equals dd_diff;
+// otherwise it differs by at most about one unit in the last place of the separation.
+__device__ __forceinline__ double sep_diff(double ahi, double alo, double bhi, double blo) {
+    return __dadd_rn(__dsub_rn(ahi, bhi), __dsub_rn(alo, blo));
+}
 
 // ----------------------------------------------------------------- matrices (columns x, y, z)
 __device__ __forceinline__ m3 mident(double a) { return m3{{a, 0, 0}, {0, a, 0}, {0, 0, a}}; }

@@ -126,76 +126,100 @@ __device__ __constant__ const double RING_KSERKK[5][2] = {{-2373.352280413907057
 __device__ __constant__ const double RING_KSERKM[5][2] = {{-523.02599873176918199, 290.10526315789473684}, {-5485.2200380469245403, 5336.9790741915028535}, {-8338.1052631578947368, 15206.361445783132530}, {-2017.9378566899175650, 10515.743817374762207}, {-19.710843373493975904, 1418.8103994927076728}};
 __device__ __constant__ const double RING_KSER0[6][2] = {{51471.854036415172419, 32768.000000000000000}, {-119621.18573838632696, -84345.212035111671234}, {96754.491735189724987, 78074.125512775430927}, {-31810.735585315211544, -31108.829182924968396}, {3678.1383813624327949, 4926.4461273804873303}, {-74.040670509817904983, -206.66608791871105442}};
 
-__device__ __forceinline__ v3 ring_sum(const double *__restrict__ disks, int ndisk, double host_R, v3 r) {
+// Geometry of a field point relative to a ring host, in the ring frame (ring.impl:2112-2118).
+struct RingGeom {
+    double x, y, re, re2, rz, rz2, r2;
+    bool psign;
+};
+__device__ __forceinline__ RingGeom ring_geom(v3 r) {
+    RingGeom g;
+    g.psign = r.z < 0;
+    if (g.psign) r.z = -r.z;
+    g.x = r.x;
+    g.y = r.y;
+    g.re2 = r.x * r.x + r.y * r.y;
+    g.re = sqrt(g.re2);
+    g.rz2 = r.z * r.z;
+    g.r2 = g.re2 + g.rz2;
+    g.rz = r.z;
+    return g;
+}
+
+// Contribution of one signed disk {GsR2, R_R, H_R} (ring.impl:2122-2190). sin and cos of
+// phi = atan2(rz, re - R) are formed from the same two legs instead of from phi.
+__device__ __forceinline__ v3 ring_disk_term(const double *__restrict__ disk, double host_R, const RingGeom &g) {
     const double pi = 3.1415926535897932;
-    bool psign = r.z < 0;
-    if (psign) r.z = -r.z;
-    const double re2 = r.x * r.x + r.y * r.y;
-    const double re = sqrt(re2);
-    const double rz2 = r.z * r.z;
-    const double r2 = re2 + rz2;
-    const double rz = r.z;
-    v3 ret = mk(0, 0, 0);
-    for (int i = 0; i < ndisk; ++i) {
-        const double GsR2 = __ldg(disks + 3 * i), R_R = __ldg(disks + 3 * i + 1), H_R = __ldg(disks + 3 * i + 2);
-        double R = R_R * host_R;
-        double H = H_R * host_R;
-        double reR = re * R;
-        double R2 = R * R, H2, fzh = 1;
-        double k2dre = 4.0 / (r2 + R2 + 2 * reR);
-        if (H > 0) {
-            H2 = H * H;
-            k2dre -= H2 * (k2dre * k2dre) * (1 - k2dre * rz2) / 48;
-            fzh = (re > R ? re - R : 0);
-            fzh = 4 * (rz2 + fzh * fzh);
-            fzh = sqrt(fzh / (fzh + H2));
-        }
-        double k2 = reR * k2dre;
-        k2dre *= R2 * sqrt(k2dre);
-        double phi = atan2(rz, re - R);
-        double kk = 0, lk = 0, fx;
-        bool lkh = k2 >= 0.45;
-        if (lkh) {
-            kk = sqrt(k2);
-            lk = log((1 - k2) / (8 * (1 + kk)));
-            fx = (padesum(kk, RING_XSERKK) + lk * padesum(kk, RING_XSERKM)) / (k2 * k2);
-        } else {
-            fx = padesum(k2, RING_XSER0);
-        }
-        fx *= k2dre;
-        double fz;
-        double s, c;
-        sincos(phi, &s, &c);
-        int kh = k2 >= .5;
-        bool exphi;
-        if (kh) {
-            const double phimax = (pi / 2);
-            exphi = c > 0;
-            double ck = 1 - k2, lk2 = log(ck / 16), sk = sqrt(ck);
-            double cc = exphi ? -c : c;
-            double cphi = exphi ? pi - phi : phi;
-            fz = cphi - (s / 8) * ((lk2 * (k2 - 5) - 2 * ck) * sk + 2 * cc * (1 + lk2) * ck);
-            fz *= (double)ring_fzcorr((float)((exphi ? phi : pi - phi) * (1 / phimax)), (float)(k2 * 2), kh);
-        } else {
-            const double phimax = (809. / 512);
-            exphi = phi > phimax;
-            double cr2 = exphi ? R2 + rz2 : r2;
-            double cRdr2 = (exphi ? re2 : R2) / cr2;
-            fz = (pi / 8) * (4 - 3 * cRdr2) * (rz / sqrt(cr2) * cRdr2);
-            fz *= (double)ring_fzcorr((float)((exphi ? pi - phi : phi) * (1 / phimax)), (float)(k2 * 2), kh);
-        }
-        if (exphi) {
-            double ek;
-            if (lkh) ek = padesum(kk, RING_KSERKK) + lk * padesum(kk, RING_KSERKM);
-            else ek = padesum(k2, RING_KSER0);
-            fz = pi - 2 * sqrt(1 - k2) * ek * s - fz;
-        }
-        double Gs = GsR2 / (host_R * host_R);
-        fx *= Gs;
-        fz *= Gs;
-        ret += mk(-4 * fx * r.x, -4 * fx * r.y, -2 * fz * fzh);
+    const double GsR2 = __ldg(disk), R_R = __ldg(disk + 1), H_R = __ldg(disk + 2);
+    const double re = g.re, re2 = g.re2, rz = g.rz, rz2 = g.rz2, r2 = g.r2;
+    double R = R_R * host_R;
+    double H = H_R * host_R;
+    double reR = re * R;
+    double R2 = R * R, H2, fzh = 1;
+    double k2dre = 4.0 / (r2 + R2 + 2 * reR);
+    if (H > 0) {
+        H2 = H * H;
+        k2dre -= H2 * (k2dre * k2dre) * (1 - k2dre * rz2) / 48;
+        fzh = (re > R ? re - R : 0);
+        fzh = 4 * (rz2 + fzh * fzh);
+        fzh = sqrt(fzh / (fzh + H2));
     }
-    if (psign) ret.z = -ret.z;
+    double k2 = reR * k2dre;
+    k2dre *= R2 * sqrt(k2dre);
+    const double dx = re - R;
+    double phi = atan2(rz, dx);
+    double kk = 0, lk = 0, fx;
+    bool lkh = k2 >= 0.45;
+    if (lkh) {
+        kk = sqrt(k2);
+        lk = log((1 - k2) / (8 * (1 + kk)));
+        fx = (padesum(kk, RING_XSERKK) + lk * padesum(kk, RING_XSERKM)) / (k2 * k2);
+    } else {
+        fx = padesum(k2, RING_XSER0);
+    }
+    fx *= k2dre;
+    double fz;
+    double s, c;
+    {
+        const double h = sqrt(rz2 + dx * dx);
+        if (h > 0) { s = rz / h; c = dx / h; }
+        else { s = 0; c = 1; }   // atan2(0, 0) = 0
+    }
+    int kh = k2 >= .5;
+    bool exphi;
+    if (kh) {
+        const double phimax = (pi / 2);
+        exphi = c > 0;
+        double ck = 1 - k2, lk2 = log(ck / 16), sk = sqrt(ck);
+        double cc = exphi ? -c : c;
+        double cphi = exphi ? pi - phi : phi;
+        fz = cphi - (s / 8) * ((lk2 * (k2 - 5) - 2 * ck) * sk + 2 * cc * (1 + lk2) * ck);
+        fz *= (double)ring_fzcorr((float)((exphi ? phi : pi - phi) * (1 / phimax)), (float)(k2 * 2), kh);
+    } else {
+        const double phimax = (809. / 512);
+        exphi = phi > phimax;
+        double cr2 = exphi ? R2 + rz2 : r2;
+        double cRdr2 = (exphi ? re2 : R2) / cr2;
+        fz = (pi / 8) * (4 - 3 * cRdr2) * (rz / sqrt(cr2) * cRdr2);
+        fz *= (double)ring_fzcorr((float)((exphi ? pi - phi : phi) * (1 / phimax)), (float)(k2 * 2), kh);
+    }
+    if (exphi) {
+        double ek;
+        if (lkh) ek = padesum(kk, RING_KSERKK) + lk * padesum(kk, RING_KSERKM);
+        else ek = padesum(k2, RING_KSER0);
+        fz = pi - 2 * sqrt(1 - k2) * ek * s - fz;
+    }
+    double Gs = GsR2 / (host_R * host_R);
+    fx *= Gs;
+    fz *= Gs;
+    return mk(-4 * fx * g.x, -4 * fx * g.y, -2 * fz * fzh);
+}
+
+// ring::sum: disks added in order, then the sign flip of the mirrored half-space (ring.impl:2109-2195)
+__device__ __forceinline__ v3 ring_sum(const double *__restrict__ disks, int ndisk, double host_R, v3 r) {
+    const RingGeom g = ring_geom(r);
+    v3 ret = mk(0, 0, 0);
+    for (int i = 0; i < ndisk; ++i) ret += ring_disk_term(disks + 3 * i, host_R, g);
+    if (g.psign) ret.z = -ret.z;
     return ret;
 }
 

@@ -7,21 +7,27 @@
 //
 //   * every CTA owns up to kOwnMax bodies for the whole launch and keeps their private state (start of
 //     step, the 25 RK12 stage accumulators, auxiliaries) in shared memory;
-//   * one stage evaluation is two O(N^2) sweeps separated by grid barriers:
-//       pass A  - potential, Newtonian acceleration and tidal matrix of each owned body, summed over all
-//                 bodies j by the CTA's threads (threads stride over j; pair sums stay in registers for
-//                 up to kRegBodies owned bodies so each j is loaded once), reduced with warp shuffles;
-//                 then the harmonics update and the angular-velocity fixed point per body (mass.impl:48-80);
-//       pass B  - 1PN, deformation, Lense-Thirring, radiation and extended-body forces, reduced the same way,
-//                 followed by the finalisation, the RK12 stage combination and the state update of the
-//                 owned bodies (all private, so no barrier is needed between them);
+//   * one stage evaluation is two O(N^2) sweeps separated by grid barriers. Before each sweep the
+//     planes of all bodies j that the pair terms read are staged into a shared-memory tile by the
+//     bulk-copy engine (cp.async.bulk, completion on an mbarrier); the CTA's warps are split into one
+//     group per owned body, each group strides over j in the tile, accumulates that body's pair sums
+//     in registers and reduces them with warp shuffles;
+//       pass A  - potential, Newtonian acceleration and tidal matrix (mass.impl:1-46), then the harmonics
+//                 update and the angular-velocity fixed point per body (mass.impl:48-80); meanwhile the
+//                 other warps evaluate every geopotential / ring host's field at the owned bodies, once
+//                 per (host, body) pair: the force on the body stays in shared memory, the reaction on
+//                 the host goes to a global table its owner sums in pass B (APPLY_NONPOINT_FORCE,
+//                 mass.impl:127-130);
+//       pass B  - 1PN, deformation, Lense-Thirring and radiation (mass.impl:82-125), the hosts' reaction
+//                 sums, finalisation (mass.cpp:389-396), then the RK12 stage combination and the state
+//                 update of the owned bodies;
 //   * the stage state other CTAs read is double-buffered (ping-pong), so pass B of stage k and the state
 //     update for stage k+1 need no barrier between them: 2 barriers per stage, 50 per step;
 //   * the RK12 combination sum_j a_kj f_j is accumulated incrementally: when f_j is known it is added into
 //     the accumulators of every later stage k, in ascending j, which is the reference's summation order.
 //
-// The grid barrier waits are bounded (kBarrierTimeoutNs): on timeout the kernel records
-// ST_BARRIER_TIMEOUT in the status word and returns; it never traps.
+// All waits are bounded (kWaitTimeoutNs): a grid-barrier or copy wait that runs out records a status
+// word and the kernel returns (after waiting, again bounded, for its own copies in flight); it never traps.
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <string.h>
@@ -35,7 +41,7 @@
 namespace eph {
 
 constexpr double kC = 299792458.0;                      // src/math/basic_math.h:10,18
-constexpr unsigned long long kBarrierTimeoutNs = 2000000000ull;
+constexpr unsigned long long kWaitTimeoutNs = 2000000000ull;
 
 __constant__ double c_rk_hi[EPH_RK12_NCOEF];            // a_kj, double-double
 __constant__ double c_rk_lo[EPH_RK12_NCOEF];
@@ -44,7 +50,8 @@ __constant__ double c_dtk[kStages + 1];                 // c_k = sum of nonzero 
 // ------------------------------------------------------------------ owned-body private state (shared memory)
 struct Own {
     int idx, kind, gp, ring;          // kind: 0 point Newtonian (k2 == 0), 1 undelayed tide, 2 delayed tide
-    int converged, swept, pad0, pad1;
+    int converged, ext_slot, gl_fixed, full;   // ext_slot: index in the extended-body list, or -1
+    int orig, pad1, pad2, pad3;               // orig: index in the caller's plane arrays
     double GM0, dGM, dJ2, R, R2, A, k2, k2r, td, sR2, rR2G4c;
     double Cst[9];
     double ring_GM_ratio, ring_GL_R2;
@@ -59,31 +66,24 @@ struct Own {
     double gacc[3], dacc[3], dtq[3], Egrad[3], mind, maxi;
     double sumA[13];
     double fa[3];                     // f_s acceleration of the current stage
-    double gpf[9], rgf[9];            // geopotential frame (rounded s) and ring frame, fixed within a pass
-    int gl_fixed, pad2;
+    double wnew[3], dw[3];            // stage angular velocity and its 2/3 increment (state update)
     // RK12 accumulators of stages k = 1..25 (index k-1)
     dd accv[kStages][3];
     double acca[kStages][3], accw[kStages][3], acct[kStages][3];
 };
 
 struct Scratch {
-    double red[kThreads / 32][kRegBodies][13];
-    double ext[kOwnMax][kMaxExt][3];
+    double part[kWarps][16];          // per-warp partial sums
+    double ext[kOwnMax][kMaxExt][3];  // other hosts' fields on the owned bodies (geopotential, or ring)
+    double ext2[kOwnMax][kMaxExt][3]; // ring half of a host that has both models
+    double react[kOwnMax][6];         // summed reactions of owned hosts
+    double rterm[kOwnMax][kRingPar][kRingDiskPar][3];   // per-disk ring terms before their ordered sum
+    int ring_e[kRingPar], n_ring_e, ring_dmax;
+    double rk_hi[EPH_RK12_NCOEF], rk_lo[EPH_RK12_NCOEF];   // a_kj (lane-divergent reads: shared, not constant, memory)
     unsigned long long t_last, t_phase[kPhases];
-    int flag;
+    unsigned long long mbar;          // mbarrier of the tile copies
+    int flag, pad;
 };
-
-__device__ __forceinline__ unsigned long long global_ns();
-
-// Optional phase timers: thread 0 charges the time since the previous mark to phase `ph`. Marks sit
-// right after a __syncthreads(), so they bound the whole CTA's work of the phase.
-__device__ __forceinline__ void mark(const SysDev &S, Scratch &sc, int ph) {
-    if (S.timers && threadIdx.x == 0) {
-        unsigned long long t = global_ns();
-        sc.t_phase[ph] += t - sc.t_last;
-        sc.t_last = t;
-    }
-}
 
 // ------------------------------------------------------------------ small helpers
 __device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
@@ -95,6 +95,19 @@ __device__ __forceinline__ unsigned long long global_ns() {
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
+}
+__device__ __forceinline__ unsigned smem_addr(const void *p) {
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+
+// Optional phase timers: thread 0 charges the time since the previous mark to phase `ph`. Marks sit
+// right after a __syncthreads(), so they bound the whole CTA's work of the phase.
+__device__ __forceinline__ void mark(const SysDev &S, Scratch &sc, int ph) {
+    if (S.timers && threadIdx.x == 0) {
+        unsigned long long t = global_ns();
+        sc.t_phase[ph] += t - sc.t_last;
+        sc.t_last = t;
+    }
 }
 
 // Barrier over all CTAs of the launch (co-resident by the cooperative launch). Returns false when the
@@ -115,7 +128,7 @@ __device__ bool grid_sync(const SysDev &S, Scratch &sc) {
         } else {
             unsigned long long t0 = global_ns();
             while (ld_acquire(gen) == g) {
-                if (global_ns() - t0 > kBarrierTimeoutNs) {
+                if (global_ns() - t0 > kWaitTimeoutNs) {
                     atomicExch(S.status, (int)ST_BARRIER_TIMEOUT);
                     fail = 1;
                     break;
@@ -128,6 +141,78 @@ __device__ bool grid_sync(const SysDev &S, Scratch &sc) {
     }
     __syncthreads();
     return sc.flag == 0;
+}
+
+// ------------------------------------------------------------------ bulk copies into the staging tile
+struct TileState {
+    unsigned parity;   // phase parity of the mbarrier for the next completion
+};
+
+__device__ __forceinline__ void mbar_init(Scratch &sc) {
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&sc.mbar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+}
+
+// Copy `rows` planes (row r from src[r] + j0, `count` bodies rounded up to kPad) into tile rows of
+// `stride` doubles. Every thread waits for completion (bounded). Returns false on timeout.
+__device__ bool load_tile(const SysDev &S, Scratch &sc, TileState &ts, double *tile, int stride,
+                          const double *const *src, int rows, int j0, int count, int count_tail, int tail_from) {
+    __syncthreads();   // the previous sweep's reads of the tile are done
+    const int cpad = (count + kPad - 1) / kPad * kPad;
+    const int tpad = (count_tail + kPad - 1) / kPad * kPad;
+    const unsigned bytes = (unsigned)cpad * 8u, tbytes = (unsigned)tpad * 8u;
+    const unsigned total = bytes * (unsigned)tail_from + tbytes * (unsigned)(rows - tail_from);
+    const unsigned mb = smem_addr(&sc.mbar);
+    if (threadIdx.x == 0) {
+        // order the generic-proxy accesses (tile reads, other CTAs' global stores) before the copies
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("fence.proxy.async.global;" ::: "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(total) : "memory");
+        for (int r = 0; r < rows; ++r) {
+            const unsigned nbytes = r < tail_from ? bytes : tbytes;
+            if (nbytes == 0) continue;
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                    smem_addr(tile + (size_t)r * stride)),
+                "l"(src[r] + j0), "r"(nbytes), "r"(mb)
+                : "memory");
+        }
+    }
+    const unsigned parity = ts.parity;
+    ts.parity ^= 1u;
+    unsigned long long t0 = 0;
+    for (unsigned it = 0;; ++it) {
+        unsigned done;
+        asm volatile(
+            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+            : "=r"(done)
+            : "r"(mb), "r"(parity)
+            : "memory");
+        if (done) break;
+        if ((it & 63) == 0) {
+            unsigned long long t = global_ns();
+            if (t0 == 0) t0 = t;
+            else if (t - t0 > kWaitTimeoutNs) {
+                if (threadIdx.x == 0) atomicExch(S.status, (int)ST_COPY_TIMEOUT);
+                // give the copies in flight one more bounded wait before the CTA leaves
+                const unsigned long long t1 = global_ns();
+                for (;;) {
+                    asm volatile(
+                        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+                        : "=r"(done)
+                        : "r"(mb), "r"(parity)
+                        : "memory");
+                    if (done || global_ns() - t1 > kWaitTimeoutNs) break;
+                }
+                return false;
+            }
+        }
+    }
+    mark(S, sc, PH_IO);   // tile staging (and load/store) time
+    return true;
 }
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -144,11 +229,11 @@ __device__ __forceinline__ double warp_cmax(double v) {   // NaN-propagating max
     return v;
 }
 
-__device__ __forceinline__ v3 ld3(const double *p, int n, int i) {
-    return mk(__ldcg(p + i), __ldcg(p + n + i), __ldcg(p + 2 * n + i));
+__device__ __forceinline__ v3 ld3(const double *p, int ld, int i) {
+    return mk(__ldcg(p + i), __ldcg(p + ld + i), __ldcg(p + 2 * ld + i));
 }
-__device__ __forceinline__ m3 ld9(const double *p, int n, int i) {
-    return m3{ld3(p, n, i), ld3(p + 3 * n, n, i), ld3(p + 6 * n, n, i)};
+__device__ __forceinline__ m3 ld9(const double *p, int ld, int i) {
+    return m3{ld3(p, ld, i), ld3(p + 3 * ld, ld, i), ld3(p + 6 * ld, ld, i)};
 }
 __device__ __forceinline__ v3 fast3(const dd *a) { return mk(dd_val(a[0]), dd_val(a[1]), dd_val(a[2])); }
 __device__ __forceinline__ m3 fast9(const dd *a) { return m3{fast3(a), fast3(a + 3), fast3(a + 6)}; }
@@ -166,13 +251,61 @@ __device__ __forceinline__ m3 ring_frame(v3 gl) {
     return m3{p, cross(z, p), z};
 }
 
+// Split the CTA's warps into one group per active body: warp w serves active body w % na.
+struct Group {
+    int slot;   // index into the active list
+    int tid;    // thread index inside the group
+    int size;   // threads in the group
+};
+// Groups use the first `nw` warps of the CTA (the others may run different work meanwhile).
+__device__ __forceinline__ Group group_of(int na, int nw) {
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    Group g;
+    g.slot = w % na;
+    const int rank = w / na;
+    const int gw = (nw - 1 - g.slot) / na + 1;
+    g.tid = rank * 32 + lane;
+    g.size = gw * 32;
+    return g;
+}
+
+// Barrier over the first `nthreads` threads (named barrier 1), or the whole CTA.
+__device__ __forceinline__ void part_sync(int nthreads) {
+    if (nthreads == (int)blockDim.x) __syncthreads();
+    else asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory");
+}
+
+// Sum NV per-thread values over each group of the first `nw` warps (warp shuffles, then the group's
+// warps in order) into out[slot][0..NV); entries c >= max_from are NaN-propagating maxima.
+template <int NV>
+__device__ __forceinline__ void group_reduce(const double (&acc)[NV], int na, int nw, Scratch &sc,
+                                             double (*out)[16], int max_from) {
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+    for (int c = 0; c < NV; ++c) {
+        double v = (c >= max_from) ? warp_cmax(acc[c]) : warp_sum(acc[c]);
+        if (lane == 0) sc.part[w][c] = v;
+    }
+    part_sync(nw * 32);
+    for (int idx = threadIdx.x; idx < na * NV; idx += nw * 32) {
+        const int slot = idx / NV, c = idx % NV;
+        double s = sc.part[slot][c];
+        for (int ww = slot + na; ww < nw; ww += na) {
+            if (c >= max_from) checked_maximize(s, sc.part[ww][c]);
+            else s += sc.part[ww][c];
+        }
+        out[slot][c] = s;
+    }
+    part_sync(nw * 32);
+}
+
 // ------------------------------------------------------------------ load / publish / store
 __device__ void load_own(const SysDev &S, Own *own, int nb, const StepParams &P) {
     const int n = S.n;
     const double *pl = S.planes;
     for (int b = threadIdx.x; b < nb; b += blockDim.x) {
         Own &o = own[b];
-        const int i = o.idx;
+        const int i = o.orig;
 #define PLV(p) pl[(size_t)(p) * n + i]
         o.GM0 = PLV(EPH_P_GM0); o.dGM = PLV(EPH_P_DGM); o.dJ2 = PLV(EPH_P_DJ2); o.R = PLV(EPH_P_RADIUS);
         o.R2 = PLV(EPH_P_R2); o.A = PLV(EPH_P_A); o.k2 = PLV(EPH_P_K2); o.k2r = PLV(EPH_P_K2R);
@@ -183,6 +316,9 @@ __device__ void load_own(const SysDev &S, Own *own, int nb, const StepParams &P)
         o.ring = (int)PLV(EPH_P_RING_INDEX);
         o.ring_GM_ratio = o.ring >= 0 ? S.ring_param[o.ring * 4 + 0] : 0.0;
         o.ring_GL_R2 = o.ring >= 0 ? S.ring_param[o.ring * 4 + 3] : 0.0;
+        o.ext_slot = -1;
+        for (int e = 0; e < S.n_ext; ++e)
+            if (S.ext_body[e] == o.idx) o.ext_slot = e;
         for (int c = 0; c < 3; ++c) {
             o.r[c] = dd{PLV(EPH_P_R_HI + c), PLV(EPH_P_R_LO + c)};
             o.v[c] = dd{PLV(EPH_P_V_HI + c), PLV(EPH_P_V_LO + c)};
@@ -214,7 +350,7 @@ __device__ void store_own(const SysDev &S, const Own *own, int nb, bool deform_o
     double *pl = S.planes;
     for (int b = threadIdx.x; b < nb; b += blockDim.x) {
         const Own &o = own[b];
-        const int i = o.idx;
+        const int i = o.orig;
 #define PLV(p) pl[(size_t)(p) * n + i]
         for (int q = 0; q < 9; ++q) {
             PLV(EPH_P_C_POTENTIAL + q) = o.C[q];
@@ -243,43 +379,63 @@ __device__ void store_own(const SysDev &S, const Own *own, int nb, bool deform_o
     }
 }
 
-// publish the stage state of owned body b into public buffer `buf`
+// publish the stage state of owned body o into public buffer `buf` (one thread)
 __device__ void publish_body(const SysDev &S, const Own &o, int buf) {
-    const int n = S.n, i = o.idx;
-    double *pub = S.pub + (size_t)buf * PUB_NPLANES * n;
+    const int ld = S.ld, i = o.idx;
+    double *pub = S.pub + (size_t)buf * PUB_NPLANES * ld;
     for (int c = 0; c < 3; ++c) {
-        pub[(PUB_R_HI + c) * n + i] = o.r[c].hi;
-        pub[(PUB_R_LO + c) * n + i] = o.r[c].lo;
-        pub[(PUB_V_HI + c) * n + i] = o.v[c].hi;
-        pub[(PUB_V_LO + c) * n + i] = o.v[c].lo;
+        pub[(PUB_R_HI + c) * ld + i] = o.r[c].hi;
+        pub[(PUB_R_LO + c) * ld + i] = o.r[c].lo;
+        pub[(PUB_V_HI + c) * ld + i] = o.v[c].hi;
+        pub[(PUB_V_LO + c) * ld + i] = o.v[c].lo;
     }
     v3 gl = fast3(o.GL);
-    pub[(PUB_GL + 0) * n + i] = gl.x;
-    pub[(PUB_GL + 1) * n + i] = gl.y;
-    pub[(PUB_GL + 2) * n + i] = gl.z;
-    pub[PUB_GM * n + i] = o.GM;
+    pub[(PUB_GL + 0) * ld + i] = gl.x;
+    pub[(PUB_GL + 1) * ld + i] = gl.y;
+    pub[(PUB_GL + 2) * ld + i] = gl.z;
+    pub[PUB_GM * ld + i] = o.GM;
     if (o.gp >= 0) {
-        for (int q = 0; q < 9; ++q) pub[(PUB_FRAME + q) * n + i] = dd_val(o.s[q]);
+        for (int q = 0; q < 9; ++q) pub[(PUB_FRAME + q) * ld + i] = dd_val(o.s[q]);
     }
     if (o.ring >= 0) {
-        m3 f = ring_frame(gl);
         double t[9];
-        stm(t, f);
-        for (int q = 0; q < 9; ++q) pub[(PUB_RFRAME + q) * n + i] = t[q];
+        stm(t, ring_frame(gl));
+        for (int q = 0; q < 9; ++q) pub[(PUB_RFRAME + q) * ld + i] = t[q];
     }
 }
 
+// publish_body spread over the lanes of one warp
+__device__ void publish_body_warp(const SysDev &S, const Own &o, int buf, int lane) {
+    const int ld = S.ld, i = o.idx;
+    double *pub = S.pub + (size_t)buf * PUB_NPLANES * ld;
+    if (lane < 3) {
+        const int c = lane;
+        pub[(PUB_R_HI + c) * ld + i] = o.r[c].hi;
+        pub[(PUB_R_LO + c) * ld + i] = o.r[c].lo;
+        pub[(PUB_V_HI + c) * ld + i] = o.v[c].hi;
+        pub[(PUB_V_LO + c) * ld + i] = o.v[c].lo;
+        pub[(PUB_GL + c) * ld + i] = dd_val(o.GL[c]);
+    } else if (lane == 3) {
+        pub[PUB_GM * ld + i] = o.GM;
+    } else if (lane == 4 && o.ring >= 0) {
+        double t[9];
+        stm(t, ring_frame(fast3(o.GL)));
+        for (int q = 0; q < 9; ++q) pub[(PUB_RFRAME + q) * ld + i] = t[q];
+    }
+    if (o.gp >= 0 && lane >= 8 && lane < 17) pub[(PUB_FRAME + lane - 8) * ld + i] = dd_val(o.s[lane - 8]);
+}
+
 // ------------------------------------------------------------------ pass A: deform_by + angular velocity
-// One ordered pair (i = owned body o, j) of DAMPED_TIDAL_DEFORMATION_MATRIX / _NDELAY / _NK2
-// (mass.impl:1-46), accumulated into acc = {phi, naccel[3], C[9]}.
-__device__ __forceinline__ void pair_a(const Own &o, const double rjh[3], const double rjl[3],
-                                       const double vjh[3], const double vjl[3], double GMj, double sR2j,
-                                       double tdfj, double acc[13]) {
-    v3 r = mk(dd_diff(rjh[0], rjl[0], o.r[0].hi, o.r[0].lo), dd_diff(rjh[1], rjl[1], o.r[1].hi, o.r[1].lo),
-              dd_diff(rjh[2], rjl[2], o.r[2].hi, o.r[2].lo));
+// One ordered pair (i = owned body o, j from the tile) of DAMPED_TIDAL_DEFORMATION_MATRIX / _NDELAY /
+// _NK2 (mass.impl:1-46), accumulated into acc = {phi, naccel[3], C[9]}.
+__device__ __forceinline__ void pair_a(const Own &o, const double *T, int ts, int j, double acc[13]) {
+    v3 r = mk(sep_diff(T[(TA_R_HI + 0) * ts + j], T[(TA_R_LO + 0) * ts + j], o.r[0].hi, o.r[0].lo),
+              sep_diff(T[(TA_R_HI + 1) * ts + j], T[(TA_R_LO + 1) * ts + j], o.r[1].hi, o.r[1].lo),
+              sep_diff(T[(TA_R_HI + 2) * ts + j], T[(TA_R_LO + 2) * ts + j], o.r[2].hi, o.r[2].lo));
+    const double GMj = T[TA_GM * ts + j], sR2j = T[TA_SR2 * ts + j];
     double q = dot(r, r), sm = o.sR2 + sR2j;
-    double rr2 = 1.0 / ((q < sm) ? sm : q);
-    double rr = sqrt(rr2);
+    double rr = rsqrt((q < sm) ? sm : q);   // 1/r within 1 ulp; rr2 = rr^2
+    double rr2 = rr * rr;
     double tp_dphi = rr * GMj;
     double tp_dg = rr2 * tp_dphi;
     acc[0] -= tp_dphi;
@@ -288,26 +444,104 @@ __device__ __forceinline__ void pair_a(const Own &o, const double rjh[3], const 
     acc[3] += tp_dg * r.z;
     if (o.kind == 0) return;
     double fk = (-3 * tp_dg) * o.k2;
-    m3 T;
+    m3 M;
     if (o.kind == 2) {
-        v3 v = mk(dd_diff(vjh[0], vjl[0], o.v[0].hi, o.v[0].lo), dd_diff(vjh[1], vjl[1], o.v[1].hi, o.v[1].lo),
-                  dd_diff(vjh[2], vjl[2], o.v[2].hi, o.v[2].lo));
+        v3 v = mk(sep_diff(T[(TA_V_HI + 0) * ts + j], T[(TA_V_LO + 0) * ts + j], o.v[0].hi, o.v[0].lo),
+                  sep_diff(T[(TA_V_HI + 1) * ts + j], T[(TA_V_LO + 1) * ts + j], o.v[1].hi, o.v[1].lo),
+                  sep_diff(T[(TA_V_HI + 2) * ts + j], T[(TA_V_LO + 2) * ts + j], o.v[2].hi, o.v[2].lo));
         v3 w = mk(o.w[0], o.w[1], o.w[2]);
         v3 dw = rr2 * cross(r, cross(w, r) - v);
         double dwt = normalize(dw);
-        dwt *= o.td * tdfj;
+        dwt *= o.td * T[TA_TDF * ts + j];
         double ecwt2 = 1 + 4 * dwt * dwt, secwt2 = sqrt(ecwt2);
         double x0 = sqrt((1 + secwt2) / (2 * ecwt2));
         double y0 = dwt * sqrt(2 / (ecwt2 * (1 + secwt2)));
         double z02 = dwt * dwt * (2 / (ecwt2 + secwt2));
         v3 dr = x0 * r + y0 * cross(dw, r);
-        T = add_diag(outer(rr2 * dr, dr) - outer(z02 * dw, dw), z02 - 1.0 / 3);
+        M = add_diag(outer(rr2 * dr, dr) - outer(z02 * dw, dw), z02 - 1.0 / 3);
     } else {
-        T = add_diag(outer(rr2 * r, r), -(1.0 / 3));
+        M = add_diag(outer(rr2 * r, r), -(1.0 / 3));
     }
-    acc[4] -= fk * T.x.x; acc[5] -= fk * T.x.y; acc[6] -= fk * T.x.z;
-    acc[7] -= fk * T.y.x; acc[8] -= fk * T.y.y; acc[9] -= fk * T.y.z;
-    acc[10] -= fk * T.z.x; acc[11] -= fk * T.z.y; acc[12] -= fk * T.z.z;
+    acc[4] -= fk * M.x.x; acc[5] -= fk * M.x.y; acc[6] -= fk * M.x.z;
+    acc[7] -= fk * M.y.x; acc[8] -= fk * M.y.y; acc[9] -= fk * M.y.z;
+    acc[10] -= fk * M.z.x; acc[11] -= fk * M.z.y; acc[12] -= fk * M.z.z;
+}
+
+// UPDATE_HARMONICS followed by UPDATE_ANGULAR_VELOCITY (mass.impl:48-72) for owned body o on one warp:
+// lane q < 9 owns element q of the 3x3 matrices (column q/3, row q%3). Sets o.converged.
+__device__ void update_warp(Own &o, int lane, bool deform_only) {
+    const unsigned full = 0xffffffffu;
+    const int q = lane < 9 ? lane : 0, col = q / 3, row = q % 3;
+    const v3 w = ldv(o.w);
+    const double *wp = o.w;
+    const m3 f = fast9(o.s);
+    const double *fr = &f.x.x;   // column m at fr[3m]
+    // C = R^3/(2GM) (tidal sums + k2r (w^2/3 - w w^T)) + s (C_static + exJ2 terms) s^T
+    double Cq = o.sumA[4 + q];
+    if (col == row) Cq += dot(w, w) * o.k2r / 3;
+    Cq -= wp[col] * (o.k2r * wp[row]);
+    Cq = (o.R * o.R2 / (2 * o.GM)) * Cq;
+    auto mc0 = [&](int c, int r) {
+        double v = o.Cst[3 * c + r];
+        if (c == r) v += (c < 2) ? o.exJ2 / 2 : -o.exJ2;
+        return v;
+    };
+    // sa = s % mc0: column col, row row
+    const double saq = (fr[0 + row] * mc0(col, 0) + fr[3 + row] * mc0(col, 1)) + fr[6 + row] * mc0(col, 2);
+    const double sa0 = __shfl_sync(full, saq, 0 + row), sa1 = __shfl_sync(full, saq, 3 + row),
+                 sa2 = __shfl_sync(full, saq, 6 + row);
+    // toworld: column col = (s.x[col] sa.x + s.y[col] sa.y) + s.z[col] sa.z
+    const double mcq = (fr[0 + col] * sa0 + fr[3 + col] * sa1) + fr[6 + col] * sa2;
+    Cq = Cq + mcq;
+    const double GIq = ((-2.0) / 3 * o.R2) * (col == row ? Cq - o.A : Cq);
+    if (lane < 9) { o.C[q] = Cq; o.GI[q] = GIq; }
+    if (lane == 0) {
+        o.phi = o.sumA[0];
+        o.nacc[0] = o.sumA[1]; o.nacc[1] = o.sumA[2]; o.nacc[2] = o.sumA[3];
+    }
+    __syncwarp();
+    if (deform_only) {
+        if (lane == 0) o.converged = 1;
+        __syncwarp();
+        return;
+    }
+    bool finite = true;
+    for (int c = 0; c < 3; ++c) finite = finite && dd_finite(o.GL[c]);
+    if (!finite) {   // UPDATE_ANGULAR_VELOCITY's else-branch: GL = GI w
+        if (lane == 0) {
+            v3 gl = mul(ldm(o.GI), w);
+            o.GL[0] = dd_make(gl.x); o.GL[1] = dd_make(gl.y); o.GL[2] = dd_make(gl.z);
+            o.gl_fixed = 1;
+            o.converged = 1;
+        }
+        __syncwarp();
+        return;
+    }
+    // w = GI^-1 GL (vec_t.h:443-454): adjoint element of this lane, determinant from column z of the adjoint
+    const m3 G = ldm(o.GI);
+    const double *g = &G.x.x;
+#define GE(c, r) g[3 * (c) + (r)]
+    auto adj = [&](int c, int r) {   // mat_t::adjoint, element (column c, row r)
+        const int c1 = (c + 1) % 3, c2 = (c + 2) % 3, r1 = (r + 1) % 3, r2 = (r + 2) % 3;
+        // cofactor of element (r, c) of the transpose convention used by mat_t::adjoint
+        return GE(r1, c1) * GE(r2, c2) - GE(r1, c2) * GE(r2, c1);
+    };
+    const double rdet = 1.0 / (adj(0, 2) * GE(2, 0) + adj(1, 2) * GE(2, 1) + adj(2, 2) * GE(2, 2));
+    const double invq = rdet * adj(col, row);
+#undef GE
+    const double i0 = __shfl_sync(full, invq, 0 + row), i1 = __shfl_sync(full, invq, 3 + row),
+                 i2 = __shfl_sync(full, invq, 6 + row);
+    const v3 gl = fast3(o.GL);
+    const double nw = (i0 * gl.x + i1 * gl.y) + i2 * gl.z;   // lanes 0..2: component `row`
+    const double n0 = __shfl_sync(full, nw, 0), n1 = __shfl_sync(full, nw, 1), n2 = __shfl_sync(full, nw, 2);
+    if (lane == 0) {
+        const v3 nv = mk(n0, n1, n2);
+        const v3 d = nv - w;
+        const bool same = nv.x == w.x && nv.y == w.y && nv.z == w.z;
+        stv(o.w, nv);
+        o.converged = (same || dot(d, d) < 1e-18 * dot(w, w)) ? 1 : 0;
+    }
+    __syncwarp();
 }
 
 // UPDATE_HARMONICS (mass.impl:48-61) from the pass-A sums of owned body o
@@ -341,7 +575,11 @@ __device__ bool update_angular_velocity(Own &o) {
         v3 nw = mul(inverse(GI), fast3(o.GL));
         stv(o.w, nw);
         v3 d = nw - w;
-        return dot(d, d) < 1e-18 * dot(w, w);
+        // An iteration that reproduces w exactly is a fixed point: every further iteration of the
+        // reference's loop recomputes the same sums, harmonics and w, so stopping here leaves the
+        // identical state. (Needed for w = 0, where the reference's test 0 < 1e-18*0 never passes.)
+        const bool same = nw.x == w.x && nw.y == w.y && nw.z == w.z;
+        return same || dot(d, d) < 1e-18 * dot(w, w);
     }
     v3 gl = mul(GI, w);
     o.GL[0] = dd_make(gl.x); o.GL[1] = dd_make(gl.y); o.GL[2] = dd_make(gl.z);
@@ -349,105 +587,226 @@ __device__ bool update_angular_velocity(Own &o) {
     return true;
 }
 
-template <int NV>
-__device__ __forceinline__ void block_reduce(double (&acc)[kRegBodies][13], unsigned mask, Scratch &sc,
-                                             double *out /* [kRegBodies][13] */, int max_from) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+// Pair sums of pass A for the owned bodies in `mask` over all bodies j, by the first `nw` warps (tile
+// already staged when the whole system fits in one tile; otherwise tiles are streamed, which needs the
+// whole CTA, nw == kWarps). Results land in own[b].sumA. Two bodies j per iteration keep two
+// independent pair chains in flight per thread.
+__device__ bool sweep_a(const SysDev &S, Own *own, int nb, unsigned mask, int buf, Scratch &sc, TileState &ts,
+                        double *tile, bool staged, int nw) {
+    int act[kOwnMax], na = 0;
+    for (int b = 0; b < nb; ++b)
+        if ((mask >> b) & 1) act[na++] = b;
+    if (na == 0) return true;
+    const int ld = S.ld, n = S.n, T = S.tile;
+    const double *pub = S.pub + (size_t)buf * PUB_NPLANES * ld;
+    const Group g = group_of(na, nw);
+    const Own &o = own[act[g.slot]];
+    double acc[13];
 #pragma unroll
-    for (int bb = 0; bb < kRegBodies; ++bb) {
-        if (!((mask >> bb) & 1)) continue;
-#pragma unroll
-        for (int c = 0; c < NV; ++c) {
-            double v = (c >= max_from) ? warp_cmax(acc[bb][c]) : warp_sum(acc[bb][c]);
-            if (lane == 0) sc.red[warp][bb][c] = v;
+    for (int c = 0; c < 13; ++c) acc[c] = 0;
+    for (int j0 = 0; j0 < n; j0 += T) {
+        const int cnt = min(T, n - j0);
+        if (!staged) {
+            const double *src[TA_ROWS] = {pub + (PUB_R_HI + 0) * ld, pub + (PUB_R_HI + 1) * ld, pub + (PUB_R_HI + 2) * ld,
+                                          pub + (PUB_R_LO + 0) * ld, pub + (PUB_R_LO + 1) * ld, pub + (PUB_R_LO + 2) * ld,
+                                          pub + (PUB_V_HI + 0) * ld, pub + (PUB_V_HI + 1) * ld, pub + (PUB_V_HI + 2) * ld,
+                                          pub + (PUB_V_LO + 0) * ld, pub + (PUB_V_LO + 1) * ld, pub + (PUB_V_LO + 2) * ld,
+                                          pub + PUB_GM * ld, S.cst + CST_SR2 * ld, S.cst + CST_TDF * ld};
+            if (!load_tile(S, sc, ts, tile, T, src, TA_ROWS, j0, cnt, cnt, TA_ROWS)) return false;
         }
-    }
-    __syncthreads();
-    for (int idx = threadIdx.x; idx < kRegBodies * NV; idx += blockDim.x) {
-        int bb = idx / NV, c = idx % NV;
-        if (!((mask >> bb) & 1)) continue;
-        double s = sc.red[0][bb][c];
-        for (int w = 1; w < kThreads / 32; ++w) {
-            if (c >= max_from) checked_maximize(s, sc.red[w][bb][c]);
-            else s += sc.red[w][bb][c];
+        const int self = o.idx - j0;
+        int jj = g.tid;
+        for (; jj + g.size < cnt; jj += 2 * g.size) {
+            if (jj != self) pair_a(o, tile, T, jj, acc);
+            if (jj + g.size != self) pair_a(o, tile, T, jj + g.size, acc);
         }
-        out[bb * 13 + c] = s;
+        if (jj < cnt && jj != self) pair_a(o, tile, T, jj, acc);
     }
-    __syncthreads();
+    __shared__ double red[kOwnMax][16];
+    group_reduce<13>(acc, na, nw, sc, red, 13);
+    for (int idx = threadIdx.x; idx < na * 13; idx += nw * 32) own[act[idx / 13]].sumA[idx % 13] = red[idx / 13][idx % 13];
+    part_sync(nw * 32);
+    return true;
 }
 
-__device__ void pass_a(const SysDev &S, Own *own, int nb, int buf, bool deform_only, Scratch &sc,
-                       double *red_out) {
-    const int n = S.n;
-    const double *pub = S.pub + (size_t)buf * PUB_NPLANES * n;
-    const double *cst = S.cst;
+// Field of every geopotential / ring host at the owned bodies, once per (host, body): the force on the
+// owned body goes to sc.ext, the host's reaction to S.react (APPLY_NONPOINT_FORCE, mass.impl:127-130;
+// r = r_body - r_host as `mj.r - mi.r` with mi the host, mass.cpp:358-371). Runs on warps
+// [first_warp, kWarps): ring items on the last warp, geopotential items on the others, so no warp
+// diverges between the two models.
+__device__ void ext_fields(const SysDev &S, const Own *own, int nb, int buf, Scratch &sc, int first_warp) {
+    const int ld = S.ld, n_ext = S.n_ext;
+    const double *pub = S.pub + (size_t)buf * PUB_NPLANES * ld;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const bool single = first_warp == kWarps - 1;               // one warp runs both halves
+    const bool ring_warp = single || w == kWarps - 1;
+    const bool gp_warp = single || w < kWarps - 1;
+    auto body_sep = [&](const Own &o, int E) {   // r = r_body - r_host (mass.cpp:184,198)
+        return mk(dd_diff(o.r[0].hi, o.r[0].lo, __ldcg(pub + PUB_R_HI * ld + E), __ldcg(pub + PUB_R_LO * ld + E)),
+                  dd_diff(o.r[1].hi, o.r[1].lo, __ldcg(pub + (PUB_R_HI + 1) * ld + E), __ldcg(pub + (PUB_R_LO + 1) * ld + E)),
+                  dd_diff(o.r[2].hi, o.r[2].lo, __ldcg(pub + (PUB_R_HI + 2) * ld + E), __ldcg(pub + (PUB_R_LO + 2) * ld + E)));
+    };
+    // geopotential half: force on the body into sc.ext, reaction on the host into react slot 0
+    auto put = [&](int half, int b, int e, const Own &o, v3 r, v3 an, double GME, bool live) {
+        v3 add3 = mk(0, 0, 0), da = mk(0, 0, 0), dt = mk(0, 0, 0);
+        if (live) {
+            add3 = GME * an;
+            da = -(o.GM * an);
+            dt = -(o.GM * cross(r, an));
+        }
+        double (*dst)[kMaxExt][3] = half ? sc.ext2 : sc.ext;
+        dst[b][e][0] = add3.x; dst[b][e][1] = add3.y; dst[b][e][2] = add3.z;
+        double *rc = S.react + (((size_t)e * ld + o.idx) * 2 + half) * 6;
+        rc[0] = da.x; rc[1] = da.y; rc[2] = da.z; rc[3] = dt.x; rc[4] = dt.y; rc[5] = dt.z;
+    };
+    if (gp_warp) {
+        const int t0 = single ? lane : threadIdx.x - first_warp * 32;
+        const int stride = single ? 32 : (kWarps - 1 - first_warp) * 32;
+        for (int item = t0; item < nb * n_ext; item += stride) {
+            const int b = item / n_ext, e = item % n_ext;
+            const Own &o = own[b];
+            const int E = __ldg(S.ext_body + e);
+            const int gpE = (int)__ldg(S.cst + CST_GP * ld + E);
+            const bool live = gpE >= 0 && E != o.idx;
+            v3 r = mk(0, 0, 0), an = mk(0, 0, 0);
+            double GME = 0;
+            if (live) {
+                r = body_sep(o, E);
+                GME = __ldcg(pub + PUB_GM * ld + E);
+                m3 f = ld9(pub + PUB_FRAME * ld, ld, E);
+                an = toworld(f, gp_sum(S.gp_coef + (size_t)gpE * EPH_GP_TABLE_SIZE, __ldg(S.gp_nz + gpE),
+                                       __ldg(S.gp_nt + gpE), __ldg(S.cst + CST_R * ld + E), tolocal(f, r)));
+            }
+            put(0, b, e, o, r, an, GME, live);
+        }
+    }
+    if (!ring_warp) return;
+    // ring half (react slot 1, sc.ext2). With few hosts and disks each lane takes one (body, host, disk)
+    // term and the terms are added in disk order afterwards (ring.impl:2122-2192); otherwise one lane
+    // per (body, host) runs ring::sum whole.
+    if (lane == 0) {
+        int nr = 0, dmax = 0;
+        for (int e = 0; e < n_ext; ++e) {
+            const int E = S.ext_body[e];
+            const int rg = (int)S.cst[CST_RING * ld + E];
+            if (rg < 0) continue;
+            if (nr < kRingPar) sc.ring_e[nr] = e;
+            ++nr;
+            dmax = max(dmax, S.ring_nd[rg]);
+        }
+        sc.n_ring_e = nr;
+        sc.ring_dmax = dmax;
+    }
+    __syncwarp();
+    const int nr = sc.n_ring_e, dmax = sc.ring_dmax;
+    const bool parallel = nr <= kRingPar && dmax <= kRingDiskPar;
+    for (int item = lane; item < nb * n_ext; item += 32) {   // zero the slots of hosts without a ring
+        const int b = item / n_ext, e = item % n_ext;
+        const int E = __ldg(S.ext_body + e);
+        if ((int)__ldg(S.cst + CST_RING * ld + E) >= 0 && parallel) continue;
+        const Own &o = own[b];
+        const int rg = (int)__ldg(S.cst + CST_RING * ld + E);
+        const bool live = rg >= 0 && E != o.idx;
+        v3 r = mk(0, 0, 0), an = mk(0, 0, 0);
+        double GME = 0;
+        if (live) {   // sequential fallback
+            r = body_sep(o, E);
+            GME = __ldcg(pub + PUB_GM * ld + E);
+            m3 f = ld9(pub + PUB_RFRAME * ld, ld, E);
+            an = toworld(f, ring_sum(S.ring_disk + (size_t)rg * EPH_RING_MAX_DISKS * 3, __ldg(S.ring_nd + rg),
+                                     __ldg(S.cst + CST_R * ld + E), tolocal(f, r)));
+        }
+        put(1, b, e, o, r, an, GME, live);
+    }
+    if (!parallel) return;
+    for (int item = lane; item < nb * nr * dmax; item += 32) {
+        const int b = item / (nr * dmax), h = (item / dmax) % nr, d = item % dmax;
+        const Own &o = own[b];
+        const int e = sc.ring_e[h], E = __ldg(S.ext_body + e);
+        const int rg = (int)__ldg(S.cst + CST_RING * ld + E);
+        v3 t = mk(0, 0, 0);
+        if (E != o.idx && d < __ldg(S.ring_nd + rg)) {
+            m3 f = ld9(pub + PUB_RFRAME * ld, ld, E);
+            const RingGeom g = ring_geom(tolocal(f, body_sep(o, E)));
+            t = ring_disk_term(S.ring_disk + ((size_t)rg * EPH_RING_MAX_DISKS + d) * 3, __ldg(S.cst + CST_R * ld + E), g);
+        }
+        sc.rterm[b][h][d][0] = t.x; sc.rterm[b][h][d][1] = t.y; sc.rterm[b][h][d][2] = t.z;
+    }
+    __syncwarp();
+    for (int item = lane; item < nb * nr; item += 32) {
+        const int b = item / nr, h = item % nr;
+        const Own &o = own[b];
+        const int e = sc.ring_e[h], E = __ldg(S.ext_body + e);
+        const int rg = (int)__ldg(S.cst + CST_RING * ld + E);
+        const bool live = E != o.idx;
+        v3 r = mk(0, 0, 0), an = mk(0, 0, 0);
+        double GME = 0;
+        if (live) {
+            r = body_sep(o, E);
+            GME = __ldcg(pub + PUB_GM * ld + E);
+            m3 f = ld9(pub + PUB_RFRAME * ld, ld, E);
+            const RingGeom g = ring_geom(tolocal(f, r));
+            v3 ret = mk(0, 0, 0);
+            const int nd = __ldg(S.ring_nd + rg);
+            for (int d = 0; d < nd; ++d) ret += mk(sc.rterm[b][h][d][0], sc.rterm[b][h][d][1], sc.rterm[b][h][d][2]);
+            if (g.psign) ret.z = -ret.z;
+            an = toworld(f, ret);
+        }
+        put(1, b, e, o, r, an, GME, live);
+    }
+}
+
+__device__ bool pass_a(const SysDev &S, Own *own, int nb, int buf, bool deform_only, Scratch &sc, TileState &ts,
+                       double *tile) {
+    const int ld = S.ld;
+    const double *pub = S.pub + (size_t)buf * PUB_NPLANES * ld;
     if (threadIdx.x < nb) { own[threadIdx.x].converged = 0; own[threadIdx.x].gl_fixed = 0; }
-    __syncthreads();
+    const bool one_tile = S.n <= S.tile;
+    if (one_tile) {
+        const double *src[TA_ROWS] = {pub + (PUB_R_HI + 0) * ld, pub + (PUB_R_HI + 1) * ld, pub + (PUB_R_HI + 2) * ld,
+                                      pub + (PUB_R_LO + 0) * ld, pub + (PUB_R_LO + 1) * ld, pub + (PUB_R_LO + 2) * ld,
+                                      pub + (PUB_V_HI + 0) * ld, pub + (PUB_V_HI + 1) * ld, pub + (PUB_V_HI + 2) * ld,
+                                      pub + (PUB_V_LO + 0) * ld, pub + (PUB_V_LO + 1) * ld, pub + (PUB_V_LO + 2) * ld,
+                                      pub + PUB_GM * ld, S.cst + CST_SR2 * ld, S.cst + CST_TDF * ld};
+        if (!load_tile(S, sc, ts, tile, S.tile, src, TA_ROWS, 0, S.n, S.n, TA_ROWS)) return false;
+    } else {
+        __syncthreads();
+    }
+    // the extended bodies' fields run on the last kExtWarps warps alongside the first sweep and the
+    // first angular-velocity update (one tile only: streaming tiles needs every warp)
+    const bool ext_overlap = !deform_only && S.n_ext > 0 && one_tile;
     const int max_iter = deform_only ? 1 : 4;   // MAX_ANGULAR_VELOCITY_ITER (mass.impl:74)
     for (int it = 0; it < max_iter; ++it) {
-        for (int c0 = 0; c0 < nb; c0 += kRegBodies) {
+        const int nw = (it == 0 && ext_overlap) ? kWarps - kExtWarps : kWarps;
+        if ((threadIdx.x >> 5) < nw) {
             unsigned mask = 0;
-            bool any_delay = false;
-            for (int bb = 0; bb < kRegBodies && c0 + bb < nb; ++bb) {
-                const Own &o = own[c0 + bb];
+            for (int b = 0; b < nb; ++b) {
                 // the pair sums depend on the angular velocity only for delayed tides
-                bool need = (it == 0) || (!o.converged && o.kind == 2);
-                if (need) { mask |= 1u << bb; any_delay |= (o.kind == 2); }
+                if (it == 0 || (!own[b].converged && own[b].kind == 2)) mask |= 1u << b;
             }
-            if (!mask) continue;
-            double acc[kRegBodies][13];
-#pragma unroll
-            for (int bb = 0; bb < kRegBodies; ++bb)
-#pragma unroll
-                for (int c = 0; c < 13; ++c) acc[bb][c] = 0;
-            for (int j = threadIdx.x; j < n; j += blockDim.x) {
-                double rjh[3], rjl[3], vjh[3] = {0, 0, 0}, vjl[3] = {0, 0, 0};
-#pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    rjh[c] = __ldcg(pub + (PUB_R_HI + c) * n + j);
-                    rjl[c] = __ldcg(pub + (PUB_R_LO + c) * n + j);
-                }
-                if (any_delay) {
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) {
-                        vjh[c] = __ldcg(pub + (PUB_V_HI + c) * n + j);
-                        vjl[c] = __ldcg(pub + (PUB_V_LO + c) * n + j);
-                    }
-                }
-                const double GMj = __ldcg(pub + PUB_GM * n + j);
-                const double sR2j = __ldg(cst + CST_SR2 * n + j);
-                const double tdfj = __ldg(cst + CST_TDF * n + j);
-#pragma unroll
-                for (int bb = 0; bb < kRegBodies; ++bb) {
-                    if (!((mask >> bb) & 1)) continue;
-                    const Own &o = own[c0 + bb];
-                    if (o.idx == j) continue;
-                    pair_a(o, rjh, rjl, vjh, vjl, GMj, sR2j, tdfj, acc[bb]);
-                }
+            if (!sweep_a(S, own, nb, mask, buf, sc, ts, tile, one_tile, nw)) return false;
+            mark(S, sc, PH_A_SWEEP);   // thread 0 sits in a sweep warp
+            // harmonics and angular velocity of the owned bodies: warp b updates body b
+            {
+                const int wb = threadIdx.x >> 5;
+                if (wb < nb && !own[wb].converged) update_warp(own[wb], threadIdx.x & 31, deform_only);
             }
-            block_reduce<13>(acc, mask, sc, red_out, 13);
-            if (threadIdx.x < kRegBodies && ((mask >> threadIdx.x) & 1)) {
-                Own &o = own[c0 + threadIdx.x];
-                for (int c = 0; c < 13; ++c) o.sumA[c] = red_out[threadIdx.x * 13 + c];
-            }
-            __syncthreads();
+            if (nw < kWarps) mark(S, sc, PH_A_UPDATE);
+        } else {
+            ext_fields(S, own, nb, buf, sc, kWarps - kExtWarps);
         }
-        mark(S, sc, PH_A_SWEEP);
-        if (threadIdx.x < nb) {
-            Own &o = own[threadIdx.x];
-            if (!o.converged) {
-                update_harmonics(o);
-                o.converged = deform_only ? 1 : (update_angular_velocity(o) ? 1 : 0);
-            }
+        if (!deform_only && it == 0 && S.n_ext > 0 && !one_tile) {
+            __syncthreads();
+            ext_fields(S, own, nb, buf, sc, 0);
         }
         __syncthreads();
-        mark(S, sc, PH_A_UPDATE);
+        // iteration 0 with the extended-body warps: the wait for them beyond sweep + update
+        mark(S, sc, nw == kWarps ? PH_A_UPDATE : PH_B_EXT);
         int all = 1;
         for (int b = 0; b < nb; ++b) all &= own[b].converged;
         if (all) break;
-        __syncthreads();
     }
-    if (deform_only) return;
+    if (deform_only) return true;
     // PREPARE_RELATIVITY (mass.impl:76-80) and the pass-A outputs other CTAs read in pass B
     const double c2 = kC * kC;
     for (int b = threadIdx.x; b < nb; b += blockDim.x) {
@@ -460,234 +819,247 @@ __device__ void pass_a(const SysDev &S, Own *own, int nb, int buf, bool deform_o
         for (int c = 0; c < 3; ++c) { o.dacc[c] = 0; o.dtq[c] = 0; o.gacc[c] = 0; }
         const int i = o.idx;
         double *aux = S.aux;
-        aux[AUX_PHI * n + i] = o.phi;
+        aux[AUX_PHI * ld + i] = o.phi;
         for (int c = 0; c < 3; ++c) {
-            aux[(AUX_NACC + c) * n + i] = o.nacc[c];
-            aux[(AUX_BETA + c) * n + i] = o.beta[c];
+            aux[(AUX_NACC + c) * ld + i] = o.nacc[c];
+            aux[(AUX_BETA + c) * ld + i] = o.beta[c];
         }
-        aux[AUX_BETA2 * n + i] = o.beta2;
-        for (int q = 0; q < 9; ++q) aux[(AUX_CPOT + q) * n + i] = o.C[q];
+        aux[AUX_BETA2 * ld + i] = o.beta2;
+        for (int q = 0; q < 9; ++q) aux[(AUX_CPOT + q) * ld + i] = o.C[q];
         // a non-finite G*L was replaced by GI*w: republish it for pass B
         if (o.gl_fixed) publish_body(S, o, buf);
     }
     __syncthreads();
     mark(S, sc, PH_A_UPDATE);
+    return true;
 }
 
 // ------------------------------------------------------------------ pass B: main force
-// One ordered pair of RELATIVITY, the per-pair maxima, ROTATIONAL_TIDAL_DEFORMATION_NANTI_FORCE,
-// LENSE_THIRRING and RADIATION_PRESSURE (mass.impl:82-125, mass.cpp:147-155), plus the reaction of
-// owned body o's own geopotential / ring on j (mass.cpp:358-371, APPLY_NONPOINT_FORCE mass.impl:127-130).
-struct JB {
-    double rh[3], rl[3], gl[3], GM, phi, nacc[3], beta[3], beta2, C[9], R2, lum, sR2;
+// Extremal pairs of the per-pair maxima (RungeKutta.cu:229-230; min_distance tracks 1/r, max_influence
+// GM/r^3). The sweep uses a 1-ulp reciprocal square root; the extremes are recomputed afterwards with
+// the reference's own expressions rr2 = 1/m, rr = sqrt(rr2) (mass.impl:84-89) from the tracked pair.
+struct Extremes {
+    double m_min;           // smallest max(r^2, sR2_i + sR2_j): the largest 1/r
+    double tq, tq_m, tq_gm; // largest GM/r^3 seen (approximate), with its m and GM_j
 };
+__device__ __forceinline__ void track(Extremes &x, double m, double tp_dg, double GMj) {
+    if (x.m_min == x.m_min) x.m_min = (m != m || m < x.m_min) ? m : x.m_min;   // NaN sticks
+    if (x.tq == x.tq) {
+        if (tp_dg != tp_dg) x.tq = tp_dg;
+        else if (tp_dg > x.tq) { x.tq = tp_dg; x.tq_m = m; x.tq_gm = GMj; }
+    }
+}
 
-__device__ __forceinline__ void pair_b(const SysDev &S, const Own &o, const JB &J, double acc[13]) {
-    v3 r = mk(dd_diff(J.rh[0], J.rl[0], o.r[0].hi, o.r[0].lo), dd_diff(J.rh[1], J.rl[1], o.r[1].hi, o.r[1].lo),
-              dd_diff(J.rh[2], J.rl[2], o.r[2].hi, o.r[2].lo));
-    double q = dot(r, r), sm = o.sR2 + J.sR2;
-    double rr2 = 1.0 / ((q < sm) ? sm : q);
-    double rr = sqrt(rr2);
-    double rr3 = rr * rr2;
-    double tp_dphi = rr * J.GM;
-    double tp_dg = rr2 * tp_dphi;
-    v3 bj = mk(J.beta[0], J.beta[1], J.beta[2]);
+// One ordered pair of RELATIVITY, ROTATIONAL_TIDAL_DEFORMATION_NANTI_FORCE, LENSE_THIRRING and
+// RADIATION_PRESSURE (mass.impl:82-125, mass.cpp:147-155) into acc = {gaccel[3], daccel[3], dtorque[3]}.
+// IF / JF: body i / body j of the full class. For a point-like body the deformation matrix, G*L,
+// luminosity and receptance are all zero, so the terms they multiply are exactly zero and skipped.
+template <bool IF, bool JF>
+__device__ __forceinline__ void pair_b(const Own &o, const double *T, int ts, int j, double acc[9], Extremes &x) {
+    v3 r = mk(sep_diff(T[(TB_R_HI + 0) * ts + j], T[(TB_R_LO + 0) * ts + j], o.r[0].hi, o.r[0].lo),
+              sep_diff(T[(TB_R_HI + 1) * ts + j], T[(TB_R_LO + 1) * ts + j], o.r[1].hi, o.r[1].lo),
+              sep_diff(T[(TB_R_HI + 2) * ts + j], T[(TB_R_LO + 2) * ts + j], o.r[2].hi, o.r[2].lo));
+    const double GMj = T[TB_GM * ts + j];
+    const double q = dot(r, r), sm = o.sR2 + T[TB_SR2 * ts + j];
+    const double m = (q < sm) ? sm : q;
+    const double rr = rsqrt(m);
+    const double rr2 = rr * rr;
+    const double rr3 = rr * rr2;
+    const double tp_dphi = rr * GMj;
+    const double tp_dg = rr2 * tp_dphi;
+    track(x, m, tp_dg, GMj);
+    v3 bj = mk(T[(TB_BETA + 0) * ts + j], T[(TB_BETA + 1) * ts + j], T[(TB_BETA + 2) * ts + j]);
     v3 bi = ldv(o.beta);
     double rbj = dot(r, bj);
     double tp = rbj * rr;
     tp *= tp;
-    v3 naj = mk(J.nacc[0], J.nacc[1], J.nacc[2]);
-    double delta1 = 4 * o.phi + J.phi + o.beta2 + 2 * J.beta2 - 4 * dot(bi, bj) + (dot(r, naj) - 3 * tp) / 2;
+    v3 naj = mk(T[(TB_NACC + 0) * ts + j], T[(TB_NACC + 1) * ts + j], T[(TB_NACC + 2) * ts + j]);
+    double delta1 = 4 * o.phi + T[TB_PHI * ts + j] + o.beta2 + 2 * T[TB_BETA2 * ts + j] - 4 * dot(bi, bj) +
+                    (dot(r, naj) - 3 * tp) / 2;
     v3 b = bj - bi;
     v3 g = (7 * tp_dphi / 2) * naj + (tp_dg * delta1) * r + (tp_dg * (rbj - dot(r, b) * 4)) * b;
     acc[0] += g.x; acc[1] += g.y; acc[2] += g.z;
-    checked_maximize(acc[9], rr);
-    checked_maximize(acc[10], tp_dg);
-    // deformation of i and of j (no reaction written to j: recomputed by j's owner)
-    m3 Ci = ldm(o.C);
-    v3 Cr = mul(Ci, r);
-    v3 dg = (J.GM * rr3 * rr2 * o.R2) * ((dot(r, Cr) * 5 * rr2) * r - (Cr + Cr));
-    v3 da = dg;
-    v3 dt = cross(r, dg);
-    m3 Cj = m3{mk(J.C[0], J.C[1], J.C[2]), mk(J.C[3], J.C[4], J.C[5]), mk(J.C[6], J.C[7], J.C[8])};
-    v3 Cjr = mul(Cj, r);
-    da += (J.GM * rr3 * rr2 * J.R2) * ((dot(r, Cjr) * 5 * rr2) * r - (Cjr + Cjr));
-    // Lense-Thirring
-    double rcr32 = 2 * J.GM / kC * rr3;
-    v3 GL = fast3(o.GL);
-    v3 GLb = cross(GL, b);
-    da -= rcr32 * (GLb - (3 * dot(GLb, r) * rr2) * r);
-    dt -= rcr32 * cross(GL, cross(r, b));
-    v3 GLj = mk(J.gl[0], J.gl[1], J.gl[2]);
-    da += cross(rcr32 * (GLj - (3 * dot(GLj, r) * rr2) * r), b);
-    // radiation pressure
-    da += (J.lum * o.rR2G4c * rr3 / o.GM) * r;
-    acc[3] += da.x; acc[4] += da.y; acc[5] += da.z;
-    acc[6] += dt.x; acc[7] += dt.y; acc[8] += dt.z;
-}
-
-__device__ __forceinline__ void nonpoint_i(const SysDev &S, const Own &o, const JB &J, double acc[13]) {
-    const m3 gpf = ldm(o.gpf), rgf = ldm(o.rgf);
-    v3 r = mk(dd_diff(J.rh[0], J.rl[0], o.r[0].hi, o.r[0].lo), dd_diff(J.rh[1], J.rl[1], o.r[1].hi, o.r[1].lo),
-              dd_diff(J.rh[2], J.rl[2], o.r[2].hi, o.r[2].lo));
+    if (!IF && !JF) return;
     v3 da = mk(0, 0, 0), dt = mk(0, 0, 0);
-    if (o.gp >= 0) {
-        v3 an = toworld(gpf, gp_sum(S.gp_coef + (size_t)o.gp * EPH_GP_TABLE_SIZE, __ldg(S.gp_nz + o.gp),
-                                    __ldg(S.gp_nt + o.gp), o.R, tolocal(gpf, r)));
-        da -= J.GM * an;
-        dt -= J.GM * cross(r, an);
+    const double rcr32 = 2 * GMj / kC * rr3;
+    if (IF) {
+        // deformation of i, Lense-Thirring of i's spin, radiation received by i
+        m3 Ci = ldm(o.C);
+        v3 Cr = mul(Ci, r);
+        v3 dg = (GMj * rr3 * rr2 * o.R2) * ((dot(r, Cr) * 5 * rr2) * r - (Cr + Cr));
+        da = dg;
+        dt = cross(r, dg);
+        v3 GL = fast3(o.GL);
+        v3 GLb = cross(GL, b);
+        da -= rcr32 * (GLb - (3 * dot(GLb, r) * rr2) * r);
+        dt -= rcr32 * cross(GL, cross(r, b));
     }
-    if (o.ring >= 0) {
-        v3 an = toworld(rgf, ring_sum(S.ring_disk + (size_t)o.ring * EPH_RING_MAX_DISKS * 3,
-                                      __ldg(S.ring_nd + o.ring), o.R, tolocal(rgf, r)));
-        da -= J.GM * an;
-        dt -= J.GM * cross(r, an);
+    if (JF) {
+        // deformation of j (no reaction written to j: recomputed by j's owner), j's spin, j's light
+        const double *Cjp = T + TB_CPOT * ts + j;
+        m3 Cj = m3{mk(Cjp[0], Cjp[ts], Cjp[2 * ts]), mk(Cjp[3 * ts], Cjp[4 * ts], Cjp[5 * ts]),
+                   mk(Cjp[6 * ts], Cjp[7 * ts], Cjp[8 * ts])};
+        v3 Cjr = mul(Cj, r);
+        da += (GMj * rr3 * rr2 * T[TB_R2 * ts + j]) * ((dot(r, Cjr) * 5 * rr2) * r - (Cjr + Cjr));
+        v3 GLj = mk(T[(TB_GL + 0) * ts + j], T[(TB_GL + 1) * ts + j], T[(TB_GL + 2) * ts + j]);
+        da += cross(rcr32 * (GLj - (3 * dot(GLj, r) * rr2) * r), b);
+        if (IF) da += (T[TB_LUM * ts + j] * o.rR2G4c * rr3 / o.GM) * r;
     }
     acc[3] += da.x; acc[4] += da.y; acc[5] += da.z;
     acc[6] += dt.x; acc[7] += dt.y; acc[8] += dt.z;
 }
 
-__device__ void pass_b(const SysDev &S, Own *own, int nb, int buf, Scratch &sc, double *red_out) {
-    const int n = S.n;
-    const double *pub = S.pub + (size_t)buf * PUB_NPLANES * n;
+template <bool IF, bool JF>
+__device__ __forceinline__ void sweep_b_range(const Own &o, const double *tile, int T, int lo, int hi, int self,
+                                              const Group &g, double acc[9], Extremes &x) {
+    int jj = lo + g.tid;
+    for (; jj + g.size < hi; jj += 2 * g.size) {
+        if (jj != self) pair_b<IF, JF>(o, tile, T, jj, acc, x);
+        if (jj + g.size != self) pair_b<IF, JF>(o, tile, T, jj + g.size, acc, x);
+    }
+    if (jj < hi && jj != self) pair_b<IF, JF>(o, tile, T, jj, acc, x);
+}
+
+__device__ bool pass_b(const SysDev &S, Own *own, int nb, int buf, Scratch &sc, TileState &ts, double *tile) {
+    const int ld = S.ld, n = S.n, T = S.tile;
+    const double *pub = S.pub + (size_t)buf * PUB_NPLANES * ld;
     const double *aux = S.aux, *cst = S.cst;
-    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
-        Own &o = own[b];
-        if (o.gp >= 0) stm(o.gpf, fast9(o.s));
-        if (o.ring >= 0) stm(o.rgf, ring_frame(fast3(o.GL)));
+    const Group g = group_of(nb, kWarps);
+    const Own &o = own[g.slot];
+    double acc[9];
+#pragma unroll
+    for (int c = 0; c < 9; ++c) acc[c] = 0;
+    Extremes x{__longlong_as_double(0x7ff0000000000000ll), 0.0, 0.0, 0.0};   // m_min = +inf
+    for (int j0 = 0; j0 < n; j0 += T) {
+        const int cnt = min(T, n - j0);
+        const int cnt_full = max(0, min(cnt, S.n_full - j0));
+        // rows every body needs, then rows only full-class bodies need
+        const double *src[TB_ROWS] = {
+            pub + (PUB_R_HI + 0) * ld, pub + (PUB_R_HI + 1) * ld, pub + (PUB_R_HI + 2) * ld,
+            pub + (PUB_R_LO + 0) * ld, pub + (PUB_R_LO + 1) * ld, pub + (PUB_R_LO + 2) * ld, pub + PUB_GM * ld,
+            aux + AUX_PHI * ld, aux + (AUX_NACC + 0) * ld, aux + (AUX_NACC + 1) * ld, aux + (AUX_NACC + 2) * ld,
+            aux + (AUX_BETA + 0) * ld, aux + (AUX_BETA + 1) * ld, aux + (AUX_BETA + 2) * ld, aux + AUX_BETA2 * ld,
+            cst + CST_SR2 * ld,
+            pub + (PUB_GL + 0) * ld, pub + (PUB_GL + 1) * ld, pub + (PUB_GL + 2) * ld,
+            aux + (AUX_CPOT + 0) * ld, aux + (AUX_CPOT + 1) * ld, aux + (AUX_CPOT + 2) * ld,
+            aux + (AUX_CPOT + 3) * ld, aux + (AUX_CPOT + 4) * ld, aux + (AUX_CPOT + 5) * ld,
+            aux + (AUX_CPOT + 6) * ld, aux + (AUX_CPOT + 7) * ld, aux + (AUX_CPOT + 8) * ld,
+            cst + CST_R2 * ld, cst + CST_LUM * ld};
+        if (!load_tile(S, sc, ts, tile, T, src, TB_ROWS, j0, cnt, cnt_full, kTileBFullRows)) return false;
+        const int self = o.idx - j0;
+        if (o.full) {
+            sweep_b_range<true, true>(o, tile, T, 0, cnt_full, self, g, acc, x);
+            sweep_b_range<true, false>(o, tile, T, cnt_full, cnt, self, g, acc, x);
+        } else {
+            sweep_b_range<false, true>(o, tile, T, 0, cnt_full, self, g, acc, x);
+            sweep_b_range<false, false>(o, tile, T, cnt_full, cnt, self, g, acc, x);
+        }
+    }
+    // exact extremes with the reference's expressions
+    double red_in[11];
+#pragma unroll
+    for (int c = 0; c < 9; ++c) red_in[c] = acc[c];
+    {
+        const double rr2 = 1.0 / x.m_min;
+        red_in[9] = sqrt(rr2);                                // +inf -> 0 when no pair was seen
+        if (x.tq != x.tq) red_in[10] = x.tq;
+        else if (x.tq > 0) {
+            const double r2 = 1.0 / x.tq_m;
+            red_in[10] = r2 * (sqrt(r2) * x.tq_gm);
+        } else red_in[10] = 0.0;
+    }
+    __shared__ double red[kOwnMax][16];
+    group_reduce<11>(red_in, nb, kWarps, sc, red, 9);
+    if (threadIdx.x < nb) {
+        Own &ob = own[threadIdx.x];
+        const double *rr = red[threadIdx.x];
+        for (int c = 0; c < 3; ++c) { ob.gacc[c] = rr[c]; ob.dacc[c] = rr[3 + c]; ob.dtq[c] = rr[6 + c]; }
+        checked_maximize(ob.mind, rr[9]);
+        checked_maximize(ob.maxi, rr[10]);
     }
     __syncthreads();
-    for (int c0 = 0; c0 < nb; c0 += kRegBodies) {
-        unsigned mask = 0;
-        bool any_ext = false;
-        for (int bb = 0; bb < kRegBodies && c0 + bb < nb; ++bb) {
-            mask |= 1u << bb;
-            any_ext |= (own[c0 + bb].gp >= 0 || own[c0 + bb].ring >= 0);
+    mark(S, sc, PH_B_SWEEP);
+    // reactions of the owned extended bodies: sum over all bodies i of the table written in pass A
+    for (int b = 0; b < nb; ++b) {
+        const int e = own[b].ext_slot;
+        if (e < 0) continue;   // uniform over the CTA
+        double part[6] = {0, 0, 0, 0, 0, 0};
+        const double *rc = S.react + (size_t)e * ld * 12;   // [i][geopotential, ring][6]
+        for (int i = threadIdx.x; i < n; i += blockDim.x)
+            for (int c = 0; c < 6; ++c) part[c] += __ldcg(rc + (size_t)i * 12 + c) + __ldcg(rc + (size_t)i * 12 + 6 + c);
+        const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        for (int c = 0; c < 6; ++c) {
+            double v = warp_sum(part[c]);
+            if (lane == 0) sc.part[w][c] = v;
         }
-        double acc[kRegBodies][13];
-#pragma unroll
-        for (int bb = 0; bb < kRegBodies; ++bb)
-#pragma unroll
-            for (int c = 0; c < 13; ++c) acc[bb][c] = 0;
-        for (int j = threadIdx.x; j < n; j += blockDim.x) {
-            JB J;
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                J.rh[c] = __ldcg(pub + (PUB_R_HI + c) * n + j);
-                J.rl[c] = __ldcg(pub + (PUB_R_LO + c) * n + j);
-                J.gl[c] = __ldcg(pub + (PUB_GL + c) * n + j);
-                J.nacc[c] = __ldcg(aux + (AUX_NACC + c) * n + j);
-                J.beta[c] = __ldcg(aux + (AUX_BETA + c) * n + j);
-            }
-            J.GM = __ldcg(pub + PUB_GM * n + j);
-            J.phi = __ldcg(aux + AUX_PHI * n + j);
-            J.beta2 = __ldcg(aux + AUX_BETA2 * n + j);
-#pragma unroll
-            for (int q = 0; q < 9; ++q) J.C[q] = __ldcg(aux + (AUX_CPOT + q) * n + j);
-            J.R2 = __ldg(cst + CST_R2 * n + j);
-            J.lum = __ldg(cst + CST_LUM * n + j);
-            J.sR2 = __ldg(cst + CST_SR2 * n + j);
-#pragma unroll
-            for (int bb = 0; bb < kRegBodies; ++bb) {
-                if (!((mask >> bb) & 1)) continue;
-                const Own &o = own[c0 + bb];
-                if (o.idx == j) continue;
-                pair_b(S, o, J, acc[bb]);
-            }
-            if (any_ext) {
-                for (int bb = 0; bb < kRegBodies; ++bb) {
-                    if (!((mask >> bb) & 1)) continue;
-                    const Own &o = own[c0 + bb];
-                    if (o.idx == j || (o.gp < 0 && o.ring < 0)) continue;
-                    nonpoint_i(S, o, J, acc[bb]);
-                }
-            }
-        }
-        block_reduce<11>(acc, mask, sc, red_out, 9);
-        if (threadIdx.x < kRegBodies && ((mask >> threadIdx.x) & 1)) {
-            Own &o = own[c0 + threadIdx.x];
-            const double *rr = red_out + threadIdx.x * 13;
-            for (int c = 0; c < 3; ++c) { o.gacc[c] = rr[c]; o.dacc[c] = rr[3 + c]; o.dtq[c] = rr[6 + c]; }
-            checked_maximize(o.mind, rr[9]);
-            checked_maximize(o.maxi, rr[10]);
+        __syncthreads();
+        if (threadIdx.x < 6) {
+            double s = 0;
+            for (int ww = 0; ww < kWarps; ++ww) s += sc.part[ww][threadIdx.x];
+            sc.react[b][threadIdx.x] = s;
         }
         __syncthreads();
     }
-    mark(S, sc, PH_B_SWEEP);
-    // forces of the other extended bodies' geopotentials and rings on the owned bodies
-    // (the `mj.daccel += mi.GM*an` half of APPLY_NONPOINT_FORCE, mass.impl:127-128)
-    const int n_ext = S.n_ext;
-    for (int item = threadIdx.x; item < nb * n_ext; item += blockDim.x) {
-        const int b = item / n_ext, e = item % n_ext;
-        const Own &o = own[b];
-        const int E = __ldg(S.ext_body + e);
-        v3 add3 = mk(0, 0, 0);
-        if (E != o.idx) {
-            v3 r = mk(dd_diff(o.r[0].hi, o.r[0].lo, __ldcg(pub + PUB_R_HI * n + E), __ldcg(pub + PUB_R_LO * n + E)),
-                      dd_diff(o.r[1].hi, o.r[1].lo, __ldcg(pub + (PUB_R_HI + 1) * n + E), __ldcg(pub + (PUB_R_LO + 1) * n + E)),
-                      dd_diff(o.r[2].hi, o.r[2].lo, __ldcg(pub + (PUB_R_HI + 2) * n + E), __ldcg(pub + (PUB_R_LO + 2) * n + E)));
-            const double GME = __ldcg(pub + PUB_GM * n + E);
-            const double RE = __ldg(cst + CST_R * n + E);
-            const int gpE = (int)__ldg(cst + CST_GP * n + E), ringE = (int)__ldg(cst + CST_RING * n + E);
-            if (gpE >= 0) {
-                m3 f = ld9(pub + PUB_FRAME * n, n, E);
-                v3 an = toworld(f, gp_sum(S.gp_coef + (size_t)gpE * EPH_GP_TABLE_SIZE, __ldg(S.gp_nz + gpE),
-                                          __ldg(S.gp_nt + gpE), RE, tolocal(f, r)));
-                add3 += GME * an;
-            }
-            if (ringE >= 0) {
-                m3 f = ld9(pub + PUB_RFRAME * n, n, E);
-                v3 an = toworld(f, ring_sum(S.ring_disk + (size_t)ringE * EPH_RING_MAX_DISKS * 3,
-                                            __ldg(S.ring_nd + ringE), RE, tolocal(f, r)));
-                add3 += GME * an;
-            }
-        }
-        sc.ext[b][e][0] = add3.x; sc.ext[b][e][1] = add3.y; sc.ext[b][e][2] = add3.z;
-    }
-    __syncthreads();
-    mark(S, sc, PH_B_EXT);
+    mark(S, sc, PH_B_FINAL);   // host reaction sums
     // finalisation (mass.cpp:389-396): FINALIZE_RELATIVITY and RING_CORRECTION
     const double c2 = kC * kC;
+    const int n_ext = S.n_ext;
     for (int b = threadIdx.x; b < nb; b += blockDim.x) {
-        Own &o = own[b];
-        v3 da = ldv(o.dacc);
-        for (int e = 0; e < n_ext; ++e) da += mk(sc.ext[b][e][0], sc.ext[b][e][1], sc.ext[b][e][2]);
-        o.phi *= c2;
-        v3 na = c2 * ldv(o.nacc);
-        stv(o.nacc, na);
-        v3 ga = ldv(o.gacc);
-        v3 tq = ldv(o.dtq);
-        if (o.ring >= 0) {
-            da = da - o.ring_GM_ratio * ((ga + da) + na);
-            v3 mGL = fast3(o.GL);
+        Own &ob = own[b];
+        v3 da = ldv(ob.dacc);
+        v3 tq = ldv(ob.dtq);
+        for (int e = 0; e < n_ext; ++e) {
+            da += mk(sc.ext[b][e][0], sc.ext[b][e][1], sc.ext[b][e][2]);
+            da += mk(sc.ext2[b][e][0], sc.ext2[b][e][1], sc.ext2[b][e][2]);
+        }
+        if (ob.ext_slot >= 0) {
+            da += mk(sc.react[b][0], sc.react[b][1], sc.react[b][2]);
+            tq += mk(sc.react[b][3], sc.react[b][4], sc.react[b][5]);
+        }
+        ob.phi *= c2;
+        v3 na = c2 * ldv(ob.nacc);
+        stv(ob.nacc, na);
+        v3 ga = ldv(ob.gacc);
+        if (ob.ring >= 0) {
+            da = da - ob.ring_GM_ratio * ((ga + da) + na);
+            v3 mGL = fast3(ob.GL);
             double rmGL = normalize(mGL);
             v3 ptorque = dot(tq, mGL) * mGL;
             v3 dtq = tq - ptorque;
-            dtq = (rmGL / (rmGL + o.ring_GL_R2 * o.R2)) * dtq;
+            dtq = (rmGL / (rmGL + ob.ring_GL_R2 * ob.R2)) * dtq;
             tq = dtq + ptorque;
         }
-        stv(o.dacc, da);
-        stv(o.dtq, tq);
-        stv(o.fa, (ga + da) + na);
+        stv(ob.dacc, da);
+        stv(ob.dtq, tq);
+        stv(ob.fa, (ga + da) + na);
     }
     __syncthreads();
     mark(S, sc, PH_B_FINAL);
+    return true;
 }
 
 // ------------------------------------------------------------------ RK12 stage combination and update
 // Called with f_s known for all owned bodies (s = 0..24). Adds a_{k,s} f_s into the accumulators of
 // stages k = s+1..25 (RungeKutta.impl:148-162 in incremental form), then forms the state of stage s+1
-// (RungeKutta.impl:164-186) and publishes it to buffer `buf_out`.
+// (RungeKutta.impl:164-186) and publishes it to buffer `buf_out`. The state update of body b runs on
+// warp b: lanes 0..2 take the vector components, lanes 0..8 the 3x3 frame elements.
 __device__ void rk_stage(const SysDev &S, Own *own, int nb, int s, long long i_step, const StepParams &P,
-                         int buf_out) {
+                         int buf_out, const Scratch &sc) {
     const double dt = P.dt;
+    if (s == 0) {   // start of a step: x0 = x; Egrad = dtorque (RungeKutta.impl:113-116), 24 items per body
+        for (int item = threadIdx.x; item < nb * 24; item += blockDim.x) {
+            Own &o = own[item / 24];
+            const int f = item % 24;
+            if (f < 3) o.r0[f] = o.r[f];
+            else if (f < 6) o.v0[f - 3] = o.v[f - 3];
+            else if (f < 9) o.GL0[f - 6] = o.GL[f - 6];
+            else if (f < 18) o.s0[f - 9] = o.s[f - 9];
+            else if (f < 21) o.w0[f - 18] = o.w[f - 18];
+            else o.Egrad[f - 21] = o.dtq[f - 21];
+        }
+    }
     if (threadIdx.x < nb) {
         Own &o = own[threadIdx.x];
-        if (s == 0) {   // start of a step: x0 = x; Egrad = dtorque (RungeKutta.impl:113-116)
-            for (int c = 0; c < 3; ++c) { o.r0[c] = o.r[c]; o.v0[c] = o.v[c]; o.GL0[c] = o.GL[c]; o.w0[c] = o.w[c]; }
-            for (int q = 0; q < 9; ++q) o.s0[q] = o.s[q];
-            for (int c = 0; c < 3; ++c) o.Egrad[c] = o.dtq[c];
-        }
         if (s == kStages - 1) {   // rotational end-of-step correction (RungeKutta.impl:129-140)
             m3 GI = ldm(o.GI);
             m3 ir = inverse(GI);
@@ -716,7 +1088,7 @@ __device__ void rk_stage(const SysDev &S, Own *own, int nb, int s, long long i_s
         const int c = rem % 12;
         Own &o = own[b];
         const int ci = k * (k - 1) / 2 + s;
-        const dd a = dd{c_rk_hi[ci], c_rk_lo[ci]};
+        const dd a = dd{sc.rk_hi[ci], sc.rk_lo[ci]};
         const bool nz = a.hi != 0;
         if (c < 3) {
             dd cur = (s == 0) ? dd_make(0) : o.accv[k - 1][c];
@@ -735,62 +1107,98 @@ __device__ void rk_stage(const SysDev &S, Own *own, int nb, int s, long long i_s
         }
     }
     __syncthreads();
-    // state of stage k = s+1
+    // state of stage k = s+1, warp b for body b
     const int k = s + 1;
     const double dt_k = c_dtk[k];
     const double t = P.t_eph + dt * (dt_k + (double)i_step);
-    if (threadIdx.x < nb) {
-        Own &o = own[threadIdx.x];
-        const dd ddt = dd_make(dt);
-        for (int c = 0; c < 3; ++c) {
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (w < nb) {
+        Own &o = own[w];
+        if (lane < 3) {
+            const int c = lane;
+            const dd ddt = dd_make(dt);
             o.r[c] = dd_add(o.r0[c], dd_mul(ddt, o.accv[k - 1][c]));
             o.v[c] = dd_add(o.v0[c], dd_make(dt * o.acca[k - 1][c]));
             o.GL[c] = dd_add(o.GL0[c], dd_make(dt * o.acct[k - 1][c]));
+            const double wc = o.accw[k - 1][c] * (1.0 / dt_k);   // xi.w /= dt_k (vec_t.h:197-203)
+            o.wnew[c] = wc;
+            o.dw[c] = (2.0 / 3) * (wc - o.w0[c]);
         }
-        v3 w = vdiv(ldv(o.accw[k - 1]), dt_k);
-        stv(o.w, w);
-        v3 dw = (2.0 / 3) * (w - ldv(o.w0));
-        for (int q = 0; q < 9; ++q) o.s[q] = o.s0[q];
-        double st[9];
-        m3 R1 = rotation_matrix(w - dw, dt * dt_k / 2);
-        stm(st, mul(R1, fast9(o.s)));
-        for (int q = 0; q < 9; ++q) o.s[q] = dd_add(o.s[q], dd_make(st[q]));
-        m3 R2 = rotation_matrix(w + dw, dt * dt_k / 2);
-        stm(st, mul(R2, fast9(o.s)));
-        for (int q = 0; q < 9; ++q) o.s[q] = dd_add(o.s[q], dd_make(st[q]));
+        __syncwarp();
+        if (lane < 9) o.s[lane] = o.s0[lane];
+        __syncwarp();
+        const v3 wv = ldv(o.wnew), dwv = ldv(o.dw);
+        // s += R % fast(s), element (col, row) = sum_m R[m][row] * s[col][m]
+        for (int pass = 0; pass < (k == kStages ? 3 : 2); ++pass) {
+            m3 R = pass == 0 ? rotation_matrix(wv - dwv, dt * dt_k / 2)
+                 : pass == 1 ? rotation_matrix(wv + dwv, dt * dt_k / 2)
+                             : rotation_matrix(ldv(o.Egrad), 1.0 / 72);
+            double add = 0;
+            if (lane < 9) {
+                const int col = lane / 3, row = lane % 3;
+                const v3 sc = fast3(o.s + 3 * col);
+                const double *Rr = &R.x.x;   // R column m at Rr[3m]
+                add = (Rr[0 + row] * sc.x + Rr[3 + row] * sc.y) + Rr[6 + row] * sc.z;
+            }
+            __syncwarp();
+            if (lane < 9) o.s[lane] = dd_add(o.s[lane], dd_make(add));
+            __syncwarp();
+        }
         if (k == kStages) {
-            m3 R3 = rotation_matrix(ldv(o.Egrad), 1.0 / 72);
-            stm(st, mul(R3, fast9(o.s)));
-            for (int q = 0; q < 9; ++q) o.s[q] = dd_add(o.s[q], dd_make(st[q]));
-            // mass::orthogonalize (mass.h:147-150)
-            m3 fmis = fast9(o.s);
-            m3 one_minus = add_diag((-1.0) * mul(transpose(fmis), fmis), 1.0);
-            stm(st, mul(0.5 * fmis, one_minus));
-            for (int q = 0; q < 9; ++q) o.s[q] = dd_add(o.s[q], dd_make(st[q]));
+            // mass::orthogonalize (mass.h:147-150): s += 0.5 fmis % (1 - fmis^T % fmis)
+            double add = 0;
+            if (lane < 9) {
+                const int col = lane / 3, row = lane % 3;
+                const m3 f = fast9(o.s);
+                // column `col` of (1 - f^T f): entries m = (1 if m == col) - dot(f[m], f[col])
+                const v3 fc = (col == 0) ? f.x : (col == 1) ? f.y : f.z;
+                const double o0 = (col == 0 ? 1.0 : 0.0) - dot(f.x, fc);
+                const double o1 = (col == 1 ? 1.0 : 0.0) - dot(f.y, fc);
+                const double o2 = (col == 2 ? 1.0 : 0.0) - dot(f.z, fc);
+                const double *fr = &f.x.x;
+                add = (0.5 * fr[0 + row] * o0 + 0.5 * fr[3 + row] * o1) + 0.5 * fr[6 + row] * o2;
+            }
+            __syncwarp();
+            if (lane < 9) o.s[lane] = dd_add(o.s[lane], dd_make(add));
+            __syncwarp();
         }
-        o.GM = o.GM0 + o.dGM * t;
-        o.exJ2 = o.dJ2 * t;
-        publish_body(S, o, buf_out);
+        if (lane == 0) {
+            stv(o.w, wv);
+            o.GM = o.GM0 + o.dGM * t;
+            o.exJ2 = o.dJ2 * t;
+        }
+        __syncwarp();
+        publish_body_warp(S, o, buf_out, lane);
     }
     __syncthreads();
 }
 
 // ------------------------------------------------------------------ the kernel
 __global__ void __launch_bounds__(kThreads, 1) step_kernel(SysDev S, StepParams P) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     Own *own = reinterpret_cast<Own *>(smem_raw);
     Scratch &sc = *reinterpret_cast<Scratch *>(smem_raw + sizeof(Own) * kOwnMax);
-    __shared__ double red_out[kRegBodies * 13];
+    double *tile = reinterpret_cast<double *>(smem_raw + ((sizeof(Own) * kOwnMax + sizeof(Scratch) + 127) / 128) * 128);
+    TileState ts{0u};
 
     if (threadIdx.x == 0) {
         sc.t_last = global_ns();
         for (int p = 0; p < kPhases; ++p) sc.t_phase[p] = 0;
     }
+    for (int q = threadIdx.x; q < EPH_RK12_NCOEF; q += blockDim.x) {
+        sc.rk_hi[q] = c_rk_hi[q];
+        sc.rk_lo[q] = c_rk_lo[q];
+    }
+    mbar_init(sc);
     int nb = 0;
     for (int b = 0; b < kOwnMax; ++b) {
         int id = S.own_list[blockIdx.x * kOwnMax + b];
         if (id < 0) break;
-        if (threadIdx.x == 0) own[b].idx = id;
+        if (threadIdx.x == 0) {
+            own[b].idx = id;
+            own[b].orig = S.orig[id];
+            own[b].full = id < S.n_full;
+        }
         ++nb;
     }
     __syncthreads();
@@ -813,10 +1221,10 @@ __global__ void __launch_bounds__(kThreads, 1) step_kernel(SysDev S, StepParams 
 
     if (P.mode == MODE_DEFORM || P.mode == MODE_ACCEL) {
         if (!sync()) return;
-        pass_a(S, own, nb, 0, P.mode == MODE_DEFORM, sc, red_out);
+        if (!pass_a(S, own, nb, 0, P.mode == MODE_DEFORM, sc, ts, tile)) return;
         if (P.mode == MODE_ACCEL) {
             if (!sync()) return;
-            pass_b(S, own, nb, 0, sc, red_out);
+            if (!pass_b(S, own, nb, 0, sc, ts, tile)) return;
         }
         finish(P.mode == MODE_DEFORM);
         return;
@@ -830,13 +1238,13 @@ __global__ void __launch_bounds__(kThreads, 1) step_kernel(SysDev S, StepParams 
     int buf = 0;
     for (long long step = 0; step < P.n_step; ++step) {
         for (int s = 0; s < kStages; ++s) {
-            rk_stage(S, own, nb, s, step, P, buf ^ 1);
+            rk_stage(S, own, nb, s, step, P, buf ^ 1, sc);
             mark(S, sc, PH_RK);
             buf ^= 1;
             if (!sync()) return;
-            pass_a(S, own, nb, buf, false, sc, red_out);
+            if (!pass_a(S, own, nb, buf, false, sc, ts, tile)) return;
             if (!sync()) return;
-            pass_b(S, own, nb, buf, sc, red_out);
+            if (!pass_b(S, own, nb, buf, sc, ts, tile)) return;
         }
     }
     if (P.invert_min && threadIdx.x < nb) own[threadIdx.x].mind = 1 / own[threadIdx.x].mind;
@@ -849,7 +1257,13 @@ __global__ void __launch_bounds__(kThreads, 1) step_kernel(SysDev S, StepParams 
 // ------------------------------------------------------------------ host launcher
 namespace eph {
 
-size_t step_smem_bytes() { return sizeof(Own) * kOwnMax + sizeof(Scratch); }
+size_t step_fixed_smem_bytes() { return ((sizeof(Own) * kOwnMax + sizeof(Scratch) + 127) / 128) * 128; }
+size_t step_smem_bytes(int tile) { return step_fixed_smem_bytes() + (size_t)kTileRows * tile * sizeof(double); }
+// dynamic shared memory limit: the 227 KB per-CTA maximum less room for the kernel's static arrays
+constexpr int kMaxSmem = 227 * 1024 - 4096;
+
+// Largest tile (bodies, multiple of kPad) that fits next to the fixed shared-memory state.
+int max_tile() { return (int)((kMaxSmem - step_fixed_smem_bytes()) / (kTileRows * sizeof(double))) / kPad * kPad; }
 
 static bool g_consts_ready[64];
 
@@ -873,21 +1287,20 @@ cudaError_t upload_constants(int device) {
     cudaError_t e = cudaMemcpyToSymbol(c_rk_hi, hi, sizeof(hi));
     if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_rk_lo, lo, sizeof(lo));
     if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_dtk, dtk, sizeof(dtk));
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                   (int)step_smem_bytes());
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
     if (e == cudaSuccess && device >= 0 && device < 64) g_consts_ready[device] = true;
     return e;
 }
 
 cudaError_t launch_step(const SysDev &S, const StepParams &P, int grid, cudaStream_t stream) {
     void *args[] = {(void *)&S, (void *)&P};
-    return cudaLaunchCooperativeKernel((void *)step_kernel, dim3(grid), dim3(kThreads), args, step_smem_bytes(),
+    return cudaLaunchCooperativeKernel((void *)step_kernel, dim3(grid), dim3(kThreads), args, step_smem_bytes(S.tile),
                                        stream);
 }
 
-int max_coresident_ctas(int device, int *out) {
+int max_coresident_ctas(int device, int tile, int *out) {
     int per_sm = 0, sms = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step_kernel, kThreads, step_smem_bytes());
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, step_kernel, kThreads, step_smem_bytes(tile));
     if (e != cudaSuccess) return (int)e;
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     if (e != cudaSuccess) return (int)e;

@@ -1,25 +1,36 @@
 // eph_system.cuh - device-side layout of one system of bodies and the RK12 step kernel's parameters.
 //
-// HBM layout (all planes structure-of-arrays, plane p of n bodies at base + p*n):
-//   * public stage state, ping-pong buffer [2]: position (double-double, 6 planes), velocity
-//     (double-double, 6 planes), G*L/GM rounded to double (3 planes), GM (1 plane), body frame s
-//     rounded to double (9 planes) and ring frame (9 planes). Written by the owning CTA at the end of
-//     a stage, read by every CTA in the next stage.
-//   * pass-A outputs: phi/c^2, naccel/c^2 (3), beta (3), beta^2, C_potential (9).
-//   * per-body constants: sR2, tide_delay_factor, R2, lum, R, GM0, ... (read-only).
-//   * the planes array [EPH_NPLANES][n] of include/eph_planes.h, used to load and store a whole system.
+// HBM layout. All per-body arrays are structure-of-arrays planes with a padded stride `ld` (n rounded
+// up to a multiple of 32 bodies, so that every plane segment a CTA stages into shared memory starts
+// on a 256-byte boundary and is a multiple of 16 bytes long, as the bulk-copy engine requires):
+//   * public stage state, ping-pong pub[2][PUB_NPLANES][ld]: position (double-double, 6 planes),
+//     velocity (double-double, 6), G*L/GM rounded to double (3), GM (1), body frame s rounded to
+//     double (9, geopotential hosts) and ring frame (9, ring hosts). Written by the owning CTA at the
+//     end of a stage, read by every CTA in the next one.
+//   * pass-A outputs aux[AUX_NPLANES][ld]: phi/c^2, naccel/c^2 (3), beta (3), beta^2, C_potential (9).
+//   * constants cst[CST_NPLANES][ld]: sR2, tide_delay_factor, R^2, luminosity, R, model indices.
+//   * extended-body reactions react[n_ext][ld][2][6]: for host e and body i, -GM_i an and -GM_i (r x an)
+//     of host e's geopotential (slot 0) and ring (slot 1) field at body i (written in pass A by i's
+//     owner, summed by e's owner in pass B).
+//   * planes[EPH_NPLANES][n]: the whole `mass` record (include/eph_planes.h), loaded at kernel start
+//     and stored at kernel end by each body's owner.
 // A CTA keeps the private state of the bodies it owns (start-of-step state, RK12 stage accumulators,
-// auxiliaries) in shared memory for the whole launch.
+// auxiliaries) in shared memory for the whole launch, next to a staging tile that holds, per phase,
+// the planes of every body j the pair sums read.
 #pragma once
 #include <stdint.h>
 
 namespace eph {
 
-constexpr int kThreads = 256;        // threads per CTA
+constexpr int kThreads = 512;        // threads per CTA (16 warps; <= 128 registers per thread)
+constexpr int kWarps = kThreads / 32;
+constexpr int kExtWarps = 4;         // warps computing extended-body fields during the first pass-A sweep
 constexpr int kOwnMax = 8;           // bodies owned by one CTA (private state lives in shared memory)
-constexpr int kRegBodies = 4;        // owned bodies whose pair sums are held in registers at a time
 constexpr int kStages = 25;          // Feagin RK12 stages
 constexpr int kMaxExt = 64;          // extended bodies (geopotential or ring) per system
+constexpr int kPad = 32;             // plane stride granularity (bodies)
+constexpr int kRingPar = 2;          // ring hosts whose disks are evaluated one per lane
+constexpr int kRingDiskPar = 8;      // disks per ring evaluated one per lane
 
 // public ping-pong plane offsets (within one buffer)
 enum PubPlane {
@@ -32,12 +43,30 @@ enum AuxPlane { AUX_PHI = 0, AUX_NACC = 1, AUX_BETA = 4, AUX_BETA2 = 7, AUX_CPOT
 enum ConstPlane { CST_SR2 = 0, CST_TDF = 1, CST_R2 = 2, CST_LUM = 3, CST_R = 4, CST_GP = 5, CST_RING = 6,
                   CST_NPLANES = 7 };
 
+// planes staged into shared memory for the pass-A sweep (tile rows)
+enum TileA { TA_R_HI = 0, TA_R_LO = 3, TA_V_HI = 6, TA_V_LO = 9, TA_GM = 12, TA_SR2 = 13, TA_TDF = 14, TA_ROWS = 15 };
+// planes staged for the pass-B sweep: rows every body needs, then (from kTileBFullRows) rows only
+// bodies of the full class need, staged for the full-class prefix of the tile only
+enum TileB { TB_R_HI = 0, TB_R_LO = 3, TB_GM = 6, TB_PHI = 7, TB_NACC = 8, TB_BETA = 11, TB_BETA2 = 14,
+             TB_SR2 = 15, TB_GL = 16, TB_CPOT = 19, TB_R2 = 28, TB_LUM = 29, TB_ROWS = 30 };
+constexpr int kTileBFullRows = TB_GL;
+constexpr int kTileRows = TB_ROWS;
+
+// Device bodies are ordered by class: the first n_full "full" bodies (any of tidal / rotational
+// deformation, static harmonics, spin, luminosity, radiation receptance, geopotential or ring), then the
+// point-like ones, for which the deformation, Lense-Thirring and radiation terms are exactly zero.
+// Internal index k of a body maps to its position orig[k] in the caller's plane arrays.
 struct SysDev {
     int n;                    // bodies
+    int n_full;               // bodies of the full class (internal indices [0, n_full))
+    int ld;                   // plane stride (n rounded up to kPad)
     int n_ext;                // extended bodies
-    double *pub;              // [2][PUB_NPLANES][n]
-    double *aux;              // [AUX_NPLANES][n]
-    double *cst;              // [CST_NPLANES][n]
+    int tile;                 // bodies per shared-memory tile (multiple of kPad)
+    const int *orig;          // [n] internal index -> index in `planes`
+    double *pub;              // [2][PUB_NPLANES][ld]
+    double *aux;              // [AUX_NPLANES][ld]
+    double *cst;              // [CST_NPLANES][ld]
+    double *react;            // [n_ext][ld][6]
     double *planes;           // [EPH_NPLANES][n]
     const int *ext_body;      // [n_ext] body index of each extended body
     const int *gp_nz, *gp_nt; // geopotential models
@@ -66,6 +95,6 @@ struct StepParams {
     double t_eph;             // double(t_eph) of the reference (hi + lo)
 };
 
-enum Status { ST_OK = 0, ST_BARRIER_TIMEOUT = 1 };
+enum Status { ST_OK = 0, ST_BARRIER_TIMEOUT = 1, ST_COPY_TIMEOUT = 2 };
 
 }  // namespace eph
