@@ -16,7 +16,7 @@ GP_TABLE_SIZE = 77
 RING_MAX_DISKS = 64
 
 STATUS = {0: "EPH_OK", 1: "EPH_ERR_ARG", 2: "EPH_ERR_CUDA", 3: "EPH_ERR_OOM", 4: "EPH_ERR_TIMEOUT",
-          5: "EPH_ERR_STATE", 6: "EPH_ERR_LOAD", 7: "EPH_ERR_UNSUPPORTED"}
+          5: "EPH_ERR_STATE", 6: "EPH_ERR_LOAD", 7: "EPH_ERR_UNSUPPORTED", 8: "EPH_ERR_LIMIT"}
 
 # (name, restype, argtypes) of every exported entry point
 _D = ctypes.POINTER(ctypes.c_double)
@@ -48,6 +48,8 @@ SIGNATURES = [
     ("eph_profile_phases", ctypes.c_int, [_VP, ctypes.c_int]),
     ("eph_phase_times", ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_int),
                                        ctypes.POINTER(ctypes.c_int)]),
+    ("eph_integrate_noalloc", ctypes.c_int, [ctypes.c_int, _VP, ctypes.c_int64, _VP, ctypes.POINTER(EphModels),
+                                             ctypes.c_double, ctypes.c_int64, _D, _D]),
     ("eph_msystem_load", ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(_VP)]),
     ("eph_msystem_free", ctypes.c_int, [_VP]),
     ("eph_msystem_size", ctypes.c_int64, [_VP]),

@@ -32,7 +32,8 @@ typedef enum eph_status {
     EPH_ERR_TIMEOUT = 4,      /* a bounded device-side wait gave up; the context stays usable */
     EPH_ERR_STATE = 5,        /* no system uploaded */
     EPH_ERR_LOAD = 6,         /* a config / initials file was missing or malformed */
-    EPH_ERR_UNSUPPORTED = 7   /* requested path is not provided by this library (e.g. a CPU integrator) */
+    EPH_ERR_UNSUPPORTED = 7,  /* requested path is not provided by this library (e.g. a CPU integrator) */
+    EPH_ERR_LIMIT = 8         /* a size beyond the fixed maximum of eph_integrate_noalloc's scratch */
 } eph_status;
 
 /* Geopotential and ring tables of a system (layouts in eph_planes.h). Model k of each kind belongs to
@@ -98,6 +99,29 @@ int64_t eph_launch_count(const eph_ctx *ctx);
  * (out must hold grid*8 values; grid = CTAs of the current launch shape). */
 int eph_profile_phases(eph_ctx *ctx, int enable);
 int eph_phase_times(eph_ctx *ctx, uint64_t *out, int *grid, int *phases);
+
+/* Limits of eph_integrate_noalloc's fixed scratch (about 2.5 MB of device memory per GPU). */
+#define EPH_NOALLOC_MAX_BODIES 1024
+#define EPH_NOALLOC_MAX_EXT 16     /* bodies with a geopotential or ring model */
+#define EPH_NOALLOC_MAX_GP 16      /* geopotential models */
+#define EPH_NOALLOC_MAX_RING 16    /* ring models */
+
+/* No counterpart in the reference: an added entry point for callers that cannot allocate device memory
+ * (a host program that owns all device memory through its own pool and forbids cudaMalloc, a plug-in with a
+ * fixed per-device budget, or code that must not take cudaMalloc's implicit synchronisation mid-stream).
+ * Same result as eph_upload_system + eph_integrate + eph_download_system on the same system, but the
+ * caller's planes ([EPH_NPLANES][n] doubles) stay in the caller's device memory on `device` and are
+ * integrated in place on `stream` (a cudaStream_t of that device, or NULL for the legacy default stream);
+ * the model tables are read from host memory. The kernel's working memory is one fixed array compiled into
+ * the library, which every GPU that loads the library holds until the process exits; no call allocates
+ * anything, on the device or through any library. Sizes beyond the EPH_NOALLOC_MAX_* limits (or more
+ * co-resident CTAs than the GPU offers) return EPH_ERR_LIMIT before any device work. The first call on a
+ * device sets that device up (looks up the array's device address, uploads the RK12 tables); make that
+ * first call before any stream capture. All calls share the array, and calls that overlapped on the GPU
+ * would race on it: a lock inside the library serialises the calls of one process and each call returns
+ * only after its work has finished. The caller's current device is restored before returning. */
+int eph_integrate_noalloc(int device, void *stream, int64_t n, double *d_planes, const eph_models *models,
+                          double dt, int64_t n_step, double *t_eph_hi, double *t_eph_lo);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,84 @@
+"""eph_integrate_noalloc: the integration entry point that allocates nothing (its working memory is a fixed
+array compiled into the library) against the context path eph_upload_system + eph_integrate.
+
+Tolerances are the parity tests' own: position max_i |dr_i| / |r_i - r_star| <= 1e-12 and acceleration
+max_i |da_i| / sum_j |GM_j/r_ij^2| <= 1e-14 (tests/test_gpu_parity.py).
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from tests.parity import accel_error, position_error
+
+POS_TOL = 1e-12
+ACC_TOL = 1e-14
+MAX_BODIES = 1024          # EPH_NOALLOC_MAX_BODIES
+MAX_GP = 16                # EPH_NOALLOC_MAX_GP
+EPH_ERR_LIMIT = 8
+
+
+def _lib():
+    from ephemeris_b200._lib import load_library
+    return load_library()
+
+
+def _models(g):
+    from ephemeris_b200 import Models
+    m = g.models()
+    return Models(m.gp_nz, m.gp_nt, m.gp_coef, m.ring_ndisk, m.ring_param, m.ring_disk)
+
+
+def _noalloc(lib, d_planes, n, models, dt, n_step, t):
+    hi, lo = ctypes.c_double(t[0]), ctypes.c_double(t[1])
+    st = models.struct()
+    rc = lib.eph_integrate_noalloc(0, None, n, d_planes.data_ptr(), ctypes.byref(st), dt, n_step,
+                                   ctypes.byref(hi), ctypes.byref(lo))
+    return rc, (hi.value, lo.value)
+
+
+def test_sizes_beyond_the_limit_are_rejected():
+    """Checked on the host before any device work (no GPU needed); the planes pointer is never read."""
+    from ephemeris_b200 import Models
+    lib = _lib()
+    hi, lo = ctypes.c_double(0.0), ctypes.c_double(0.0)
+    fake = ctypes.c_void_p(256)
+    st = Models.empty().struct()
+    rc = lib.eph_integrate_noalloc(0, None, MAX_BODIES + 1, fake, ctypes.byref(st), 1.0, 1,
+                                   ctypes.byref(hi), ctypes.byref(lo))
+    assert rc == EPH_ERR_LIMIT
+    nz = np.zeros(MAX_GP + 1, np.int32)
+    coef = np.zeros((MAX_GP + 1, 77))
+    big = Models(nz, nz.copy(), coef, np.zeros(0, np.int32), np.zeros((0, 4)), np.zeros((0, 64, 3)))
+    st = big.struct()
+    rc = lib.eph_integrate_noalloc(0, None, 8, fake, ctypes.byref(st), 1.0, 1, ctypes.byref(hi), ctypes.byref(lo))
+    assert rc == EPH_ERR_LIMIT
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["small_full", "config2"])
+def test_noalloc_matches_context_path_on_two_calls(golden, name):
+    import torch
+    from ephemeris_b200 import Context
+    g = golden(name)
+    lib = _lib()
+    dt = float(g["dt"])
+    n = g["load"].shape[1]
+    models = _models(g)
+
+    ctx = Context(0)
+    ctx.upload(g["load"], models)
+    d = torch.from_numpy(np.ascontiguousarray(g["load"])).to("cuda:0")
+    torch.cuda.synchronize()
+    t_ref = t_na = (0.0, 0.0)
+    for n_step in (3, 2):   # two calls in a row; the second starts from the first's output
+        t_ref = ctx.integrate(dt, n_step, t_ref)
+        want = ctx.download()
+        rc, t_na = _noalloc(lib, d, n, models, dt, n_step, t_na)
+        assert rc == 0, rc
+        got = d.cpu().numpy()
+        assert np.isfinite(got[0:12]).all()
+        assert position_error(got, want) <= POS_TOL
+        assert accel_error(got, want) <= ACC_TOL
+        assert t_na == t_ref
+    ctx.close()
