@@ -9,6 +9,7 @@
 #include <numeric>
 #include <vector>
 
+#include "eph_plan.h"
 #include "eph_system.cuh"
 #include "../../include/eph_b200.h"
 
@@ -115,68 +116,22 @@ const char *eph_last_error(const eph_ctx *ctx) { return ctx ? ctx->err : "null c
 
 }  // extern "C"
 
-// Split bodies over CTAs: longest-processing-time-first into `grid` bins of at most `cap` bodies.
-static void plan_ownership(const std::vector<double> &cost, int grid, int cap, std::vector<int> &own) {
-    const int n = (int)cost.size();
-    std::vector<int> order(n);
-    std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
-    std::vector<double> load(grid, 0.0);
-    std::vector<int> cnt(grid, 0);
-    own.assign((size_t)grid * kOwnMax, -1);
-    for (int i : order) {
-        int best = -1;
-        for (int g = 0; g < grid; ++g) {
-            if (cnt[g] >= cap) continue;
-            if (best < 0 || load[g] < load[best]) best = g;
-        }
-        own[(size_t)best * kOwnMax + cnt[best]++] = i;
-        load[best] += cost[i];
-    }
-    // bodies of a CTA in index order, so every CTA's list is deterministic and monotone
-    for (int g = 0; g < grid; ++g) std::sort(own.begin() + (size_t)g * kOwnMax, own.begin() + (size_t)g * kOwnMax + cnt[g]);
-}
-
 static int choose_shape(eph_ctx *ctx) {
     int maxc = 0;
     ctx->tile = std::min(max_tile(), ctx->ld);
     if (max_coresident_ctas(ctx->device, ctx->tile, &maxc) != 0 || maxc <= 0) return fail(ctx, EPH_ERR_CUDA, "occupancy query failed");
     const int n = ctx->n;
-    int per = ctx->req_per_cta, grid = ctx->req_grid;
-    if (per <= 0 && grid <= 0) {
-        grid = std::min(maxc, n);
-        per = (n + grid - 1) / grid;
-        grid = (n + per - 1) / per;
-        if (n > 64 && grid < maxc) grid = std::min(maxc, n);   // spread work when every SM can take some
-    } else if (per <= 0) {
-        per = (n + grid - 1) / grid;
-    } else if (grid <= 0) {
-        grid = (n + per - 1) / per;
-    }
-    per = std::max(1, std::min(per, (int)kOwnMax));
-    grid = std::max(grid, (n + per - 1) / per);
-    if (grid > maxc) return fail(ctx, EPH_ERR_ARG, "launch shape exceeds co-resident CTAs (bodies_per_cta too small)");
-    std::vector<int> own;
-    plan_ownership(ctx->h_cost, grid, per, own);
+    int grid = 0, per = 0;
+    if (!plan_shape(n, maxc, ctx->req_grid, ctx->req_per_cta, &grid, &per))
+        return fail(ctx, EPH_ERR_ARG, "launch shape exceeds co-resident CTAs (bodies_per_cta too small)");
+    std::vector<int> own((size_t)grid * kOwnMax), order(n), cnt(grid);
+    std::vector<double> load(grid);
+    plan_ownership(ctx->h_cost.data(), n, grid, per, order.data(), load.data(), cnt.data(), own.data());
     cudaError_t e = cudaMemcpy(ctx->d_own, own.data(), own.size() * sizeof(int), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return fail(ctx, EPH_ERR_CUDA, "upload ownership", e);
     ctx->grid = grid;
     ctx->per_cta = per;
     return EPH_OK;
-}
-
-// Body class of the device ordering (eph_system.cuh): full if any term beyond point-mass Newtonian + 1PN
-// can be nonzero for the body, as source or as target.
-static bool full_class(const double *h_planes, int n, int i) {
-    auto P = [&](int p) { return h_planes[(size_t)p * n + i]; };
-    if (P(EPH_P_K2) != 0 || P(EPH_P_K2R) != 0 || P(EPH_P_DJ2) != 0 || P(EPH_P_LUM) != 0 || P(EPH_P_RR2G_4C) != 0)
-        return true;
-    if (P(EPH_P_GP_INDEX) >= 0 || P(EPH_P_RING_INDEX) >= 0) return true;
-    for (int q = 0; q < 9; ++q)
-        if (P(EPH_P_C_STATIC + q) != 0) return true;
-    for (int c = 0; c < 3; ++c)
-        if (P(EPH_P_W + c) != 0 || P(EPH_P_GL_HI + c) != 0 || P(EPH_P_GL_LO + c) != 0) return true;
-    return false;
 }
 
 static int prepare_constants(eph_ctx *ctx, const double *h_planes) {
@@ -186,10 +141,10 @@ static int prepare_constants(eph_ctx *ctx, const double *h_planes) {
     std::vector<int> orig;
     orig.reserve(n);
     for (int i = 0; i < n; ++i)
-        if (full_class(h_planes, n, i)) orig.push_back(i);
+        if (plan_full_class(h_planes, n, i)) orig.push_back(i);
     ctx->n_full = (int)orig.size();
     for (int i = 0; i < n; ++i)
-        if (!full_class(h_planes, n, i)) orig.push_back(i);
+        if (!plan_full_class(h_planes, n, i)) orig.push_back(i);
     std::vector<double> cst((size_t)CST_NPLANES * ld, 0.0);
     std::vector<int> ext;
     ctx->h_cost.assign(n, 0.0);
@@ -205,9 +160,7 @@ static int prepare_constants(eph_ctx *ctx, const double *h_planes) {
         cst[CST_RING * ld + k] = P(EPH_P_RING_INDEX);
         const bool gp = P(EPH_P_GP_INDEX) >= 0, ring = P(EPH_P_RING_INDEX) >= 0;
         if (gp || ring) ext.push_back(k);
-        const bool delayed = P(EPH_P_K2) != 0 && P(EPH_P_TIDE_DELAY) != 0;
-        // relative work: pass A (three sweeps for a delayed tide), pass B (heavier for the full class)
-        ctx->h_cost[k] = (delayed ? 3.0 * 2.0 : 1.0) + (k < ctx->n_full ? 3.0 : 2.0);
+        ctx->h_cost[k] = plan_cost(h_planes, n, i, k < ctx->n_full);
     }
     if ((int)ext.size() > kMaxExt) return fail(ctx, EPH_ERR_ARG, "too many bodies with geopotential or ring models");
     ctx->n_ext = (int)ext.size();

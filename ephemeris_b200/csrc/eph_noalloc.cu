@@ -22,6 +22,7 @@
 #include <cstring>
 #include <mutex>
 
+#include "eph_plan.h"
 #include "eph_system.cuh"
 #include "../../include/eph_b200.h"
 
@@ -90,18 +91,6 @@ cudaError_t noalloc_setup(int device, double **out) {
     return cudaSuccess;
 }
 
-bool full_class_h(const double *pl, int n, int i) {
-    auto P = [&](int p) { return pl[(size_t)p * n + i]; };
-    if (P(EPH_P_K2) != 0 || P(EPH_P_K2R) != 0 || P(EPH_P_DJ2) != 0 || P(EPH_P_LUM) != 0 || P(EPH_P_RR2G_4C) != 0)
-        return true;
-    if (P(EPH_P_GP_INDEX) >= 0 || P(EPH_P_RING_INDEX) >= 0) return true;
-    for (int q = 0; q < 9; ++q)
-        if (P(EPH_P_C_STATIC + q) != 0) return true;
-    for (int c = 0; c < 3; ++c)
-        if (P(EPH_P_W + c) != 0 || P(EPH_P_GL_HI + c) != 0 || P(EPH_P_GL_LO + c) != 0) return true;
-    return false;
-}
-
 struct DeviceGuard {   // restores the caller's current device
     int prev = -1;
     DeviceGuard() { cudaGetDevice(&prev); }
@@ -133,10 +122,10 @@ int body(int device, cudaStream_t stream, int n, double *d_planes, const eph_mod
     // eph_upload_system
     int n_full = 0, k = 0;
     for (int i = 0; i < n; ++i)
-        if (full_class_h(pl, n, i)) g_h_orig[k++] = i;
+        if (plan_full_class(pl, n, i)) g_h_orig[k++] = i;
     n_full = k;
     for (int i = 0; i < n; ++i)
-        if (!full_class_h(pl, n, i)) g_h_orig[k++] = i;
+        if (!plan_full_class(pl, n, i)) g_h_orig[k++] = i;
     std::fill(g_h_cst, g_h_cst + (size_t)CST_NPLANES * ld, 0.0);
     int n_ext = 0;
     for (k = 0; k < n; ++k) {
@@ -153,39 +142,15 @@ int body(int device, cudaStream_t stream, int n, double *d_planes, const eph_mod
             if (n_ext == kNE) return EPH_ERR_LIMIT;
             g_h_ext[n_ext++] = k;
         }
-        const bool delayed = P(EPH_P_K2) != 0 && P(EPH_P_TIDE_DELAY) != 0;
-        g_h_cost[k] = (delayed ? 3.0 * 2.0 : 1.0) + (k < n_full ? 3.0 : 2.0);
+        g_h_cost[k] = plan_cost(pl, n, i, k < n_full);
     }
 
-    // launch shape (the automatic choice of eph_upload_system) and the longest-first ownership split
+    // launch shape and ownership split: the automatic choice of eph_upload_system
     const int tile = std::min(max_tile(), ld);
-    int maxc = 0;
+    int maxc = 0, grid = 0, per = 0;
     if (max_coresident_ctas(device, tile, &maxc) != 0 || maxc <= 0) return EPH_ERR_CUDA;
-    int grid = std::min(maxc, n);
-    int per = (n + grid - 1) / grid;
-    grid = (n + per - 1) / per;
-    if (n > 64 && grid < maxc) grid = std::min(maxc, n);
-    per = std::max(1, std::min(per, (int)kOwnMax));
-    grid = std::max(grid, (n + per - 1) / per);
-    if (grid > maxc) return EPH_ERR_LIMIT;
-    for (int i = 0; i < n; ++i) g_h_order[i] = i;
-    std::sort(g_h_order, g_h_order + n, [](int a, int b) {
-        return g_h_cost[a] > g_h_cost[b] || (g_h_cost[a] == g_h_cost[b] && a < b);
-    });
-    std::fill(g_h_own, g_h_own + (size_t)grid * kOwnMax, -1);
-    std::fill(g_h_load, g_h_load + grid, 0.0);
-    std::fill(g_h_cnt, g_h_cnt + grid, 0);
-    for (int q = 0; q < n; ++q) {
-        const int i = g_h_order[q];
-        int best = -1;
-        for (int g = 0; g < grid; ++g) {
-            if (g_h_cnt[g] >= per) continue;
-            if (best < 0 || g_h_load[g] < g_h_load[best]) best = g;
-        }
-        g_h_own[(size_t)best * kOwnMax + g_h_cnt[best]++] = i;
-        g_h_load[best] += g_h_cost[i];
-    }
-    for (int g = 0; g < grid; ++g) std::sort(g_h_own + (size_t)g * kOwnMax, g_h_own + (size_t)g * kOwnMax + g_h_cnt[g]);
+    if (!plan_shape(n, maxc, 0, 0, &grid, &per)) return EPH_ERR_LIMIT;
+    plan_ownership(g_h_cost, n, grid, per, g_h_order, g_h_load, g_h_cnt, g_h_own);
 
     // scratch contents: the previous call's are stale, so everything the kernel reads before writing is
     // either uploaded here or cleared to zero

@@ -74,6 +74,9 @@ struct Own {
 
 struct Scratch {
     double part[kWarps][16];          // per-warp partial sums
+    int split[kOwnMax + 1];           // warp groups of a pass-A re-sweep (equal split of the active bodies)
+    int split_a0[kOwnMax + 1];        // warp groups of the first pass-A sweep (all owned bodies, weighted)
+    int split_b[kOwnMax + 1];         // warp groups of the pass-B sweep (all owned bodies, weighted)
     double ext[kOwnMax][kMaxExt][3];  // other hosts' fields on the owned bodies (geopotential, or ring)
     double ext2[kOwnMax][kMaxExt][3]; // ring half of a host that has both models
     double react[kOwnMax][6];         // summed reactions of owned hosts
@@ -82,6 +85,7 @@ struct Scratch {
     double rk_hi[EPH_RK12_NCOEF], rk_lo[EPH_RK12_NCOEF];   // a_kj (lane-divergent reads: shared, not constant, memory)
     unsigned long long t_last, t_phase[kPhases];
     unsigned long long mbar;          // mbarrier of the tile copies
+    unsigned long long bar_target;    // grid-barrier arrivals that complete the next barrier
     int flag, pad;
 };
 
@@ -110,32 +114,35 @@ __device__ __forceinline__ void mark(const SysDev &S, Scratch &sc, int ph) {
     }
 }
 
-// Barrier over all CTAs of the launch (co-resident by the cooperative launch). Returns false when the
-// wait timed out here or elsewhere (status word set); the caller then leaves the kernel.
+// Barrier over all CTAs of the launch (co-resident by the cooperative launch). The arrival counter is a
+// 64-bit word zeroed before the launch that only grows: barrier number k of the launch is complete when it
+// reaches k * gridDim.x, so every CTA announces its arrival with one fire-and-forget release add and then
+// polls the counter; no CTA has to reset or flip anything. Returns false when the wait timed out here or
+// elsewhere (status word set); the caller then leaves the kernel.
 __device__ bool grid_sync(const SysDev &S, Scratch &sc) {
     __syncthreads();
     if (gridDim.x == 1) return true;
     if (threadIdx.x == 0) {
-        unsigned *count = S.bar, *gen = S.bar + 1;
-        unsigned g = ld_acquire(gen);
+        unsigned long long *count = reinterpret_cast<unsigned long long *>(S.bar);
+        const unsigned long long target = (sc.bar_target += gridDim.x);
         __threadfence();
-        unsigned prev = atomicAdd(count, 1u);
+        asm volatile("red.release.gpu.global.add.u64 [%0], 1;" ::"l"(count) : "memory");
         int fail = 0;
-        if (prev == gridDim.x - 1) {
-            atomicExch(count, 0u);
-            __threadfence();
-            atomicAdd(gen, 1u);
-        } else {
-            unsigned long long t0 = global_ns();
-            while (ld_acquire(gen) == g) {
-                if (global_ns() - t0 > kWaitTimeoutNs) {
+        unsigned long long t0 = 0;
+        for (unsigned it = 0;; ++it) {
+            unsigned long long v;
+            asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(count) : "memory");
+            if (v >= target) break;
+            if ((it & 15) == 15) {
+                const unsigned long long t = global_ns();
+                if (t0 == 0) t0 = t;
+                else if (t - t0 > kWaitTimeoutNs) {
                     atomicExch(S.status, (int)ST_BARRIER_TIMEOUT);
                     fail = 1;
                     break;
                 }
             }
         }
-        __threadfence();
         if (*(volatile int *)S.status != ST_OK) fail = 1;
         sc.flag = fail;
     }
@@ -251,21 +258,46 @@ __device__ __forceinline__ m3 ring_frame(v3 gl) {
     return m3{p, cross(z, p), z};
 }
 
-// Split the CTA's warps into one group per active body: warp w serves active body w % na.
+// Split the first `nw` warps of the CTA into one group of consecutive warps per active body, in
+// proportion to the bodies' weights (the relative cost of their pair terms), each body at least one warp
+// (na <= nw): the body with the heaviest pair terms gets the most lanes, so the groups finish together.
+// Computed once per launch by one thread: active body a owns warps [first[a], first[a+1]).
+__device__ void split_warps(const int *wt, int na, int nw, int *first) {
+    int cnt[kOwnMax], tot = 0;
+    for (int a = 0; a < na; ++a) tot += wt[a];
+    const int spare = nw - na;
+    int used = 0;
+    for (int a = 0; a < na; ++a) {
+        cnt[a] = 1 + spare * wt[a] / tot;
+        used += cnt[a];
+    }
+    // leftover warps to the heaviest bodies first (ties: lower index), one each
+    for (int lvl_max = 0x7fffffff; used < nw;) {
+        int lvl = -1;
+        for (int a = 0; a < na; ++a)
+            if (wt[a] < lvl_max && wt[a] > lvl) lvl = wt[a];
+        if (lvl < 0) { lvl_max = 0x7fffffff; continue; }
+        for (int a = 0; a < na && used < nw; ++a)
+            if (wt[a] == lvl) { ++cnt[a]; ++used; }
+        lvl_max = lvl;
+    }
+    first[0] = 0;
+    for (int a = 0; a < na; ++a) first[a + 1] = first[a] + cnt[a];
+}
+
 struct Group {
     int slot;   // index into the active list
     int tid;    // thread index inside the group
     int size;   // threads in the group
 };
-// Groups use the first `nw` warps of the CTA (the others may run different work meanwhile).
-__device__ __forceinline__ Group group_of(int na, int nw) {
+__device__ __forceinline__ Group group_of(const int *first, int na) {
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int a = 0;
+    while (a + 1 < na && w >= first[a + 1]) ++a;
     Group g;
-    g.slot = w % na;
-    const int rank = w / na;
-    const int gw = (nw - 1 - g.slot) / na + 1;
-    g.tid = rank * 32 + lane;
-    g.size = gw * 32;
+    g.slot = a;
+    g.tid = (w - first[a]) * 32 + lane;
+    g.size = (first[a + 1] - first[a]) * 32;
     return g;
 }
 
@@ -275,26 +307,72 @@ __device__ __forceinline__ void part_sync(int nthreads) {
     else asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory");
 }
 
-// Sum NV per-thread values over each group of the first `nw` warps (warp shuffles, then the group's
-// warps in order) into out[slot][0..NV); entries c >= max_from are NaN-propagating maxima.
+__device__ __forceinline__ double combine(double a, double b, bool is_max) {
+    if (is_max) {
+        checked_maximize(a, b);
+        return a;
+    }
+    return a + b;
+}
+
+// Reduce-scatter of 16 per-lane values over the warp: afterwards lanes 2c and 2c+1 hold the warp sum of
+// value c. 16 shuffles (8 + 4 + 2 + 1 + 1) instead of 5 per value.
+__device__ __forceinline__ double warp_reduce_scatter16(double (&v)[16], int lane) {
+#pragma unroll
+    for (int h = 8, bit = 16; h >= 1; h >>= 1, bit >>= 1) {
+        const bool up = (lane & bit) != 0;
+#pragma unroll
+        for (int k = 0; k < h; ++k) {
+            const double send = up ? v[k] : v[k + h];
+            const double keep = up ? v[k + h] : v[k];
+            v[k] = keep + __shfl_xor_sync(0xffffffffu, send, bit);
+        }
+    }
+    return v[0] + __shfl_xor_sync(0xffffffffu, v[0], 1);
+}
+
+// Sum NV per-thread values over each group of the first `nw` warps (a warp reduce-scatter, then the
+// group's warps in order, four interleaved partial sums) into out[slot][0..NV); entries c >= max_from are
+// NaN-propagating maxima (reduced across the warp with shuffles of their own).
 template <int NV>
-__device__ __forceinline__ void group_reduce(const double (&acc)[NV], int na, int nw, Scratch &sc,
+__device__ __forceinline__ void group_reduce(const double (&acc)[NV], const int *first, int na, int nw, Scratch &sc,
                                              double (*out)[16], int max_from) {
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    {
+        double v[16];
+#pragma unroll
+        for (int c = 0; c < 16; ++c) v[c] = (c < NV && c < max_from) ? acc[c] : 0.0;
+        const double r = warp_reduce_scatter16(v, lane);
+        if ((lane & 1) == 0 && (lane >> 1) < min(NV, max_from)) sc.part[w][lane >> 1] = r;
+    }
 #pragma unroll
     for (int c = 0; c < NV; ++c) {
-        double v = (c >= max_from) ? warp_cmax(acc[c]) : warp_sum(acc[c]);
+        if (c < max_from) continue;
+        const double v = warp_cmax(acc[c]);
         if (lane == 0) sc.part[w][c] = v;
     }
     part_sync(nw * 32);
     for (int idx = threadIdx.x; idx < na * NV; idx += nw * 32) {
         const int slot = idx / NV, c = idx % NV;
-        double s = sc.part[slot][c];
-        for (int ww = slot + na; ww < nw; ww += na) {
-            if (c >= max_from) checked_maximize(s, sc.part[ww][c]);
-            else s += sc.part[ww][c];
+        const int w0 = first[slot], w1 = first[slot + 1];
+        const bool mx = c >= max_from;
+        // four interleaved partial sums over the group's warps (w0 + 4m + q), then combined in q order
+        double s0 = sc.part[w0][c], s1 = 0, s2 = 0, s3 = 0;
+        const bool h1 = w0 + 1 < w1, h2 = w0 + 2 < w1, h3 = w0 + 3 < w1;
+        if (h1) s1 = sc.part[w0 + 1][c];
+        if (h2) s2 = sc.part[w0 + 2][c];
+        if (h3) s3 = sc.part[w0 + 3][c];
+        for (int ww = w0 + 4; ww < w1; ww += 4) {
+            s0 = combine(s0, sc.part[ww][c], mx);
+            if (ww + 1 < w1) s1 = combine(s1, sc.part[ww + 1][c], mx);
+            if (ww + 2 < w1) s2 = combine(s2, sc.part[ww + 2][c], mx);
+            if (ww + 3 < w1) s3 = combine(s3, sc.part[ww + 3][c], mx);
         }
-        out[slot][c] = s;
+        double r = s0;
+        if (h1) r = combine(r, s1, mx);
+        if (h2) r = combine(r, s2, mx);
+        if (h3) r = combine(r, s3, mx);
+        out[slot][c] = r;
     }
     part_sync(nw * 32);
 }
@@ -451,12 +529,26 @@ __device__ __forceinline__ void pair_a(const Own &o, const double *T, int ts, in
                   sep_diff(T[(TA_V_HI + 2) * ts + j], T[(TA_V_LO + 2) * ts + j], o.v[2].hi, o.v[2].lo));
         v3 w = mk(o.w[0], o.w[1], o.w[2]);
         v3 dw = rr2 * cross(r, cross(w, r) - v);
-        double dwt = normalize(dw);
+        double dwt;
+        const double dw2 = dot(dw, dw);
+        if (dw2 > 0x1p-960 && dw2 < 0x1p960) {   // inside the range where normalize needs no rescaling
+            const double rn = rsqrt(dw2);
+            dwt = dw2 * rn;
+            dw = rn * dw;
+        } else {
+            dwt = normalize(dw);
+        }
         dwt *= o.td * T[TA_TDF * ts + j];
-        double ecwt2 = 1 + 4 * dwt * dwt, secwt2 = sqrt(ecwt2);
-        double x0 = sqrt((1 + secwt2) / (2 * ecwt2));
-        double y0 = dwt * sqrt(2 / (ecwt2 * (1 + secwt2)));
-        double z02 = dwt * dwt * (2 / (ecwt2 + secwt2));
+        // x0, y0, z02 of the damped deformation (mass.impl:16-20) from two reciprocal square roots: with
+        // e = 1 + 4 dwt^2, s = sqrt(e), u = 1 + s, re = 1/s and ru = 1/sqrt(u/2),
+        //   x0 = sqrt(u / (2e)) = (u/2) ru re,  y0 = dwt sqrt(2 / (e u)) = dwt ru re,
+        //   z02 = 2 dwt^2 / (e + s) = dwt^2 re ru^2.
+        const double e = 1 + 4 * dwt * dwt;
+        const double re = rsqrt(e);
+        const double hu = 0.5 * (1 + e * re);
+        const double ru = rsqrt(hu);
+        const double rue = ru * re;
+        const double x0 = hu * rue, y0 = dwt * rue, z02 = (dwt * dwt) * (rue * ru);
         v3 dr = x0 * r + y0 * cross(dw, r);
         M = add_diag(outer(rr2 * dr, dr) - outer(z02 * dw, dw), z02 - 1.0 / 3);
     } else {
@@ -592,14 +684,23 @@ __device__ bool update_angular_velocity(Own &o) {
 // whole CTA, nw == kWarps). Results land in own[b].sumA. Two bodies j per iteration keep two
 // independent pair chains in flight per thread.
 __device__ bool sweep_a(const SysDev &S, Own *own, int nb, unsigned mask, int buf, Scratch &sc, TileState &ts,
-                        double *tile, bool staged, int nw) {
+                        double *tile, bool staged, int nw, const int *first_all) {
     int act[kOwnMax], na = 0;
     for (int b = 0; b < nb; ++b)
         if ((mask >> b) & 1) act[na++] = b;
     if (na == 0) return true;
     const int ld = S.ld, n = S.n, T = S.tile;
     const double *pub = S.pub + (size_t)buf * PUB_NPLANES * ld;
-    const Group g = group_of(na, nw);
+    // the first sweep of a stage covers every owned body (`first_all`, fixed per launch); a re-sweep covers
+    // the unconverged delayed tides, which all cost the same: equal split
+    const int *first = first_all;
+    if (!first) {
+        if (threadIdx.x == 0)
+            for (int a = 0; a <= na; ++a) sc.split[a] = (a * nw + na - 1) / na;
+        part_sync(nw * 32);
+        first = sc.split;
+    }
+    const Group g = group_of(first, na);
     const Own &o = own[act[g.slot]];
     double acc[13];
 #pragma unroll
@@ -623,7 +724,7 @@ __device__ bool sweep_a(const SysDev &S, Own *own, int nb, unsigned mask, int bu
         if (jj < cnt && jj != self) pair_a(o, tile, T, jj, acc);
     }
     __shared__ double red[kOwnMax][16];
-    group_reduce<13>(acc, na, nw, sc, red, 13);
+    group_reduce<13>(acc, first, na, nw, sc, red, 13);
     for (int idx = threadIdx.x; idx < na * 13; idx += nw * 32) own[act[idx / 13]].sumA[idx % 13] = red[idx / 13][idx % 13];
     part_sync(nw * 32);
     return true;
@@ -784,7 +885,7 @@ __device__ bool pass_a(const SysDev &S, Own *own, int nb, int buf, bool deform_o
                 // the pair sums depend on the angular velocity only for delayed tides
                 if (it == 0 || (!own[b].converged && own[b].kind == 2)) mask |= 1u << b;
             }
-            if (!sweep_a(S, own, nb, mask, buf, sc, ts, tile, one_tile, nw)) return false;
+            if (!sweep_a(S, own, nb, mask, buf, sc, ts, tile, one_tile, nw, it == 0 ? sc.split_a0 : nullptr)) return false;
             mark(S, sc, PH_A_SWEEP);   // thread 0 sits in a sweep warp
             // harmonics and angular velocity of the owned bodies: warp b updates body b
             {
@@ -924,7 +1025,7 @@ __device__ bool pass_b(const SysDev &S, Own *own, int nb, int buf, Scratch &sc, 
     const int ld = S.ld, n = S.n, T = S.tile;
     const double *pub = S.pub + (size_t)buf * PUB_NPLANES * ld;
     const double *aux = S.aux, *cst = S.cst;
-    const Group g = group_of(nb, kWarps);
+    const Group g = group_of(sc.split_b, nb);
     const Own &o = own[g.slot];
     double acc[9];
 #pragma unroll
@@ -969,7 +1070,7 @@ __device__ bool pass_b(const SysDev &S, Own *own, int nb, int buf, Scratch &sc, 
         } else red_in[10] = 0.0;
     }
     __shared__ double red[kOwnMax][16];
-    group_reduce<11>(red_in, nb, kWarps, sc, red, 9);
+    group_reduce<11>(red_in, sc.split_b, nb, kWarps, sc, red, 9);
     if (threadIdx.x < nb) {
         Own &ob = own[threadIdx.x];
         const double *rr = red[threadIdx.x];
@@ -1184,6 +1285,7 @@ __global__ void __launch_bounds__(kThreads, 1) step_kernel(SysDev S, StepParams 
     if (threadIdx.x == 0) {
         sc.t_last = global_ns();
         for (int p = 0; p < kPhases; ++p) sc.t_phase[p] = 0;
+        sc.bar_target = 0;
     }
     for (int q = threadIdx.x; q < EPH_RK12_NCOEF; q += blockDim.x) {
         sc.rk_hi[q] = c_rk_hi[q];
@@ -1205,6 +1307,16 @@ __global__ void __launch_bounds__(kThreads, 1) step_kernel(SysDev S, StepParams 
     load_own(S, own, nb, P);
     __syncthreads();
     if (threadIdx.x < nb) publish_body(S, own[threadIdx.x], 0);
+    if (threadIdx.x == 32) {
+        // warp groups of the sweeps over all owned bodies: delayed-tide pass-A pairs cost ~8x a point pair,
+        // full-class pass-B pairs ~2x; the first pass-A sweep leaves kExtWarps warps to the extended bodies
+        int wt[kOwnMax];
+        const bool ext_overlap = P.mode != MODE_DEFORM && S.n_ext > 0 && S.n <= S.tile;
+        for (int b = 0; b < nb; ++b) wt[b] = own[b].kind == 2 ? 8 : 1;
+        split_warps(wt, nb, ext_overlap ? kWarps - kExtWarps : kWarps, sc.split_a0);
+        for (int b = 0; b < nb; ++b) wt[b] = own[b].full ? 2 : 1;
+        split_warps(wt, nb, kWarps, sc.split_b);
+    }
     auto sync = [&]() {
         bool ok = grid_sync(S, sc);
         mark(S, sc, PH_BARRIER);

@@ -75,7 +75,7 @@ struct SysDev {
     const double *ring_param; // [n_ring][4]
     const double *ring_disk;  // [n_ring][EPH_RING_MAX_DISKS][3]
     const int *own_list;      // [grid][kOwnMax], -1 padded
-    unsigned int *bar;        // grid barrier words {count, generation}
+    unsigned int *bar;        // grid barrier: one 64-bit arrival counter (two words, 8-byte aligned), zeroed per launch
     int *status;              // device status word (0 = ok)
     unsigned long long *timers;   // optional [grid][kPhases] nanoseconds per phase (profiling), or null
 };
