@@ -352,6 +352,7 @@ __device__ __forceinline__ void group_reduce(const double (&acc)[NV], const int 
         if (lane == 0) sc.part[w][c] = v;
     }
     part_sync(nw * 32);
+    #pragma unroll 1
     for (int idx = threadIdx.x; idx < na * NV; idx += nw * 32) {
         const int slot = idx / NV, c = idx % NV;
         const int w0 = first[slot], w1 = first[slot + 1];
@@ -381,6 +382,7 @@ __device__ __forceinline__ void group_reduce(const double (&acc)[NV], const int 
 __device__ void load_own(const SysDev &S, Own *own, int nb, const StepParams &P) {
     const int n = S.n;
     const double *pl = S.planes;
+    #pragma unroll 1
     for (int b = threadIdx.x; b < nb; b += blockDim.x) {
         Own &o = own[b];
         const int i = o.orig;
@@ -426,6 +428,7 @@ __device__ void load_own(const SysDev &S, Own *own, int nb, const StepParams &P)
 __device__ void store_own(const SysDev &S, const Own *own, int nb, bool deform_only) {
     const int n = S.n;
     double *pl = S.planes;
+    #pragma unroll 1
     for (int b = threadIdx.x; b < nb; b += blockDim.x) {
         const Own &o = own[b];
         const int i = o.orig;
@@ -705,6 +708,7 @@ __device__ bool sweep_a(const SysDev &S, Own *own, int nb, unsigned mask, int bu
     double acc[13];
 #pragma unroll
     for (int c = 0; c < 13; ++c) acc[c] = 0;
+    #pragma unroll 1
     for (int j0 = 0; j0 < n; j0 += T) {
         const int cnt = min(T, n - j0);
         if (!staged) {
@@ -716,12 +720,9 @@ __device__ bool sweep_a(const SysDev &S, Own *own, int nb, unsigned mask, int bu
             if (!load_tile(S, sc, ts, tile, T, src, TA_ROWS, j0, cnt, cnt, TA_ROWS)) return false;
         }
         const int self = o.idx - j0;
-        int jj = g.tid;
-        for (; jj + g.size < cnt; jj += 2 * g.size) {
+#pragma unroll 1
+        for (int jj = g.tid; jj < cnt; jj += g.size)
             if (jj != self) pair_a(o, tile, T, jj, acc);
-            if (jj + g.size != self) pair_a(o, tile, T, jj + g.size, acc);
-        }
-        if (jj < cnt && jj != self) pair_a(o, tile, T, jj, acc);
     }
     __shared__ double red[kOwnMax][16];
     group_reduce<13>(acc, first, na, nw, sc, red, 13);
@@ -763,6 +764,7 @@ __device__ void ext_fields(const SysDev &S, const Own *own, int nb, int buf, Scr
     if (gp_warp) {
         const int t0 = single ? lane : threadIdx.x - first_warp * 32;
         const int stride = single ? 32 : (kWarps - 1 - first_warp) * 32;
+        #pragma unroll 1
         for (int item = t0; item < nb * n_ext; item += stride) {
             const int b = item / n_ext, e = item % n_ext;
             const Own &o = own[b];
@@ -801,6 +803,7 @@ __device__ void ext_fields(const SysDev &S, const Own *own, int nb, int buf, Scr
     __syncwarp();
     const int nr = sc.n_ring_e, dmax = sc.ring_dmax;
     const bool parallel = nr <= kRingPar && dmax <= kRingDiskPar;
+    #pragma unroll 1
     for (int item = lane; item < nb * n_ext; item += 32) {   // zero the slots of hosts without a ring
         const int b = item / n_ext, e = item % n_ext;
         const int E = __ldg(S.ext_body + e);
@@ -820,6 +823,7 @@ __device__ void ext_fields(const SysDev &S, const Own *own, int nb, int buf, Scr
         put(1, b, e, o, r, an, GME, live);
     }
     if (!parallel) return;
+    #pragma unroll 1
     for (int item = lane; item < nb * nr * dmax; item += 32) {
         const int b = item / (nr * dmax), h = (item / dmax) % nr, d = item % dmax;
         const Own &o = own[b];
@@ -834,6 +838,7 @@ __device__ void ext_fields(const SysDev &S, const Own *own, int nb, int buf, Scr
         sc.rterm[b][h][d][0] = t.x; sc.rterm[b][h][d][1] = t.y; sc.rterm[b][h][d][2] = t.z;
     }
     __syncwarp();
+    #pragma unroll 1
     for (int item = lane; item < nb * nr; item += 32) {
         const int b = item / nr, h = item % nr;
         const Own &o = own[b];
@@ -877,6 +882,7 @@ __device__ bool pass_a(const SysDev &S, Own *own, int nb, int buf, bool deform_o
     // first angular-velocity update (one tile only: streaming tiles needs every warp)
     const bool ext_overlap = !deform_only && S.n_ext > 0 && one_tile;
     const int max_iter = deform_only ? 1 : 4;   // MAX_ANGULAR_VELOCITY_ITER (mass.impl:74)
+    #pragma unroll 1
     for (int it = 0; it < max_iter; ++it) {
         const int nw = (it == 0 && ext_overlap) ? kWarps - kExtWarps : kWarps;
         if ((threadIdx.x >> 5) < nw) {
@@ -910,6 +916,7 @@ __device__ bool pass_a(const SysDev &S, Own *own, int nb, int buf, bool deform_o
     if (deform_only) return true;
     // PREPARE_RELATIVITY (mass.impl:76-80) and the pass-A outputs other CTAs read in pass B
     const double c2 = kC * kC;
+    #pragma unroll 1
     for (int b = threadIdx.x; b < nb; b += blockDim.x) {
         Own &o = own[b];
         v3 beta = vdiv(fast3(o.v), kC);
@@ -1013,12 +1020,9 @@ __device__ __forceinline__ void pair_b(const Own &o, const double *T, int ts, in
 template <bool IF, bool JF>
 __device__ __forceinline__ void sweep_b_range(const Own &o, const double *tile, int T, int lo, int hi, int self,
                                               const Group &g, double acc[9], Extremes &x) {
-    int jj = lo + g.tid;
-    for (; jj + g.size < hi; jj += 2 * g.size) {
+#pragma unroll 1
+    for (int jj = lo + g.tid; jj < hi; jj += g.size)
         if (jj != self) pair_b<IF, JF>(o, tile, T, jj, acc, x);
-        if (jj + g.size != self) pair_b<IF, JF>(o, tile, T, jj + g.size, acc, x);
-    }
-    if (jj < hi && jj != self) pair_b<IF, JF>(o, tile, T, jj, acc, x);
 }
 
 __device__ bool pass_b(const SysDev &S, Own *own, int nb, int buf, Scratch &sc, TileState &ts, double *tile) {
@@ -1031,6 +1035,7 @@ __device__ bool pass_b(const SysDev &S, Own *own, int nb, int buf, Scratch &sc, 
 #pragma unroll
     for (int c = 0; c < 9; ++c) acc[c] = 0;
     Extremes x{__longlong_as_double(0x7ff0000000000000ll), 0.0, 0.0, 0.0};   // m_min = +inf
+    #pragma unroll 1
     for (int j0 = 0; j0 < n; j0 += T) {
         const int cnt = min(T, n - j0);
         const int cnt_full = max(0, min(cnt, S.n_full - j0));
@@ -1081,11 +1086,13 @@ __device__ bool pass_b(const SysDev &S, Own *own, int nb, int buf, Scratch &sc, 
     __syncthreads();
     mark(S, sc, PH_B_SWEEP);
     // reactions of the owned extended bodies: sum over all bodies i of the table written in pass A
+    #pragma unroll 1
     for (int b = 0; b < nb; ++b) {
         const int e = own[b].ext_slot;
         if (e < 0) continue;   // uniform over the CTA
         double part[6] = {0, 0, 0, 0, 0, 0};
         const double *rc = S.react + (size_t)e * ld * 12;   // [i][geopotential, ring][6]
+        #pragma unroll 1
         for (int i = threadIdx.x; i < n; i += blockDim.x)
             for (int c = 0; c < 6; ++c) part[c] += __ldcg(rc + (size_t)i * 12 + c) + __ldcg(rc + (size_t)i * 12 + 6 + c);
         const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1105,6 +1112,7 @@ __device__ bool pass_b(const SysDev &S, Own *own, int nb, int buf, Scratch &sc, 
     // finalisation (mass.cpp:389-396): FINALIZE_RELATIVITY and RING_CORRECTION
     const double c2 = kC * kC;
     const int n_ext = S.n_ext;
+    #pragma unroll 1
     for (int b = threadIdx.x; b < nb; b += blockDim.x) {
         Own &ob = own[b];
         v3 da = ldv(ob.dacc);
@@ -1148,6 +1156,7 @@ __device__ void rk_stage(const SysDev &S, Own *own, int nb, int s, long long i_s
                          int buf_out, const Scratch &sc) {
     const double dt = P.dt;
     if (s == 0) {   // start of a step: x0 = x; Egrad = dtorque (RungeKutta.impl:113-116), 24 items per body
+        #pragma unroll 1
         for (int item = threadIdx.x; item < nb * 24; item += blockDim.x) {
             Own &o = own[item / 24];
             const int f = item % 24;
@@ -1182,6 +1191,7 @@ __device__ void rk_stage(const SysDev &S, Own *own, int nb, int s, long long i_s
     __syncthreads();
     // incremental combination: 12 components (velocity as double-double) per later stage
     const int nk = kStages - s;   // stages s+1..25
+    #pragma unroll 1
     for (int item = threadIdx.x; item < nb * nk * 12; item += blockDim.x) {
         const int b = item / (nk * 12);
         const int rem = item % (nk * 12);
@@ -1230,6 +1240,7 @@ __device__ void rk_stage(const SysDev &S, Own *own, int nb, int s, long long i_s
         __syncwarp();
         const v3 wv = ldv(o.wnew), dwv = ldv(o.dw);
         // s += R % fast(s), element (col, row) = sum_m R[m][row] * s[col][m]
+        #pragma unroll 1
         for (int pass = 0; pass < (k == kStages ? 3 : 2); ++pass) {
             m3 R = pass == 0 ? rotation_matrix(wv - dwv, dt * dt_k / 2)
                  : pass == 1 ? rotation_matrix(wv + dwv, dt * dt_k / 2)
@@ -1348,7 +1359,9 @@ __global__ void __launch_bounds__(kThreads, 1) step_kernel(SysDev S, StepParams 
     }
     __syncthreads();
     int buf = 0;
+    #pragma unroll 1
     for (long long step = 0; step < P.n_step; ++step) {
+        #pragma unroll 1
         for (int s = 0; s < kStages; ++s) {
             rk_stage(S, own, nb, s, step, P, buf ^ 1, sc);
             mark(S, sc, PH_RK);
