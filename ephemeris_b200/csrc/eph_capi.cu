@@ -329,6 +329,8 @@ static int run(eph_ctx *ctx, const StepParams &P) {
     CK(cudaMemcpyAsync(&status, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream), "read status");
     CK(cudaStreamSynchronize(ctx->stream), "RK12 kernel");
     if (status == ST_BARRIER_TIMEOUT) return fail(ctx, EPH_ERR_TIMEOUT, "grid barrier wait timed out");
+    if (status == ST_COPY_TIMEOUT) return fail(ctx, EPH_ERR_TIMEOUT, "tile copy wait timed out");
+    if (status != ST_OK) return fail(ctx, EPH_ERR_CUDA, "step kernel reported an unknown status");
     return EPH_OK;
 }
 

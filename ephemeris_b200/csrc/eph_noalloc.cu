@@ -211,7 +211,7 @@ int body(int device, cudaStream_t stream, int n, double *d_planes, const eph_mod
     int status = 0;
     NA_CK(cudaMemcpyAsync(&status, S.status, sizeof(int), cudaMemcpyDeviceToHost, stream));
     NA_CK(cudaStreamSynchronize(stream));
-    if (status == ST_BARRIER_TIMEOUT) return EPH_ERR_TIMEOUT;
+    if (status != ST_OK) return EPH_ERR_TIMEOUT;   // a bounded grid-barrier or tile-copy wait gave up
     // t_eph += dt*n_step in double-double (mass.cpp:441)
     double a = *t_eph_hi, b = dt * (double)n_step;
     double s = a + b, t = s - a;
