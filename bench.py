@@ -35,6 +35,10 @@ sys.path.insert(0, ROOT)
 
 METRIC = "body-steps/s vs plain FP64 at <=1e-12 pos err; small-body p50/p99 latency"
 UNIT = "body-steps/s"
+# DRAM bytes (read + write) of one step_kernel launch of one RK12 step on the config2 workload, from the
+# ncu capture summarised in profiles/step_kernel_config2.md; the system stays in L2, so the traffic of a
+# launch of k steps is taken as k times this figure.
+DRAM_BYTES_PER_RK_STEP = {"config2": 869632}
 
 # Algorithmic flop convention per ordered pair and stage evaluation ("Roofline"):
 FLOP_PASS_A = 20            # potential + Newtonian acceleration
@@ -317,7 +321,10 @@ def run_b200(args):
                 "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(planes0.nbytes),
                         "d2h_bytes_per_step": int(planes0.nbytes)},
                 "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                             "frac": achieved / peak if peak else None, "traffic": None,
+                             "frac": achieved / peak if peak else None,
+                             "traffic": (DRAM_BYTES_PER_RK_STEP[args.workload] * rk
+                                         if args.workload in DRAM_BYTES_PER_RK_STEP else None),
+                             "traffic_unit": "bytes per launch (ncu, scaled by RK12 steps per launch)",
                              "peak_source": peak_src, "flops_per_launch": flops_step * rk},
                 "gpu_launches": launches,
                 "clocks": clk,
