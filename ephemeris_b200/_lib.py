@@ -48,6 +48,14 @@ SIGNATURES = [
     ("eph_profile_phases", ctypes.c_int, [_VP, ctypes.c_int]),
     ("eph_phase_times", ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_int),
                                        ctypes.POINTER(ctypes.c_int)]),
+    ("eph_batch_create", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_VP)]),
+    ("eph_batch_destroy", ctypes.c_int, [_VP]),
+    ("eph_batch_last_error", ctypes.c_char_p, [_VP]),
+    ("eph_batch_upload", ctypes.c_int, [_VP, ctypes.c_int32, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(_D),
+                                        ctypes.POINTER(ctypes.POINTER(EphModels))]),
+    ("eph_batch_integrate", ctypes.c_int, [_VP, _D, ctypes.POINTER(ctypes.c_int64), _D, _D]),
+    ("eph_batch_download", ctypes.c_int, [_VP, ctypes.POINTER(_D)]),
+    ("eph_batch_info", ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int64)]),
     ("eph_integrate_noalloc", ctypes.c_int, [ctypes.c_int, _VP, ctypes.c_int64, _VP, ctypes.POINTER(EphModels),
                                              ctypes.c_double, ctypes.c_int64, _D, _D]),
     ("eph_msystem_load", ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(_VP)]),

@@ -36,7 +36,7 @@
 #include "eph_models.cuh"
 #include "eph_system.cuh"
 #include "../../include/eph_planes.h"
-#include "../../include/eph_rk12_table.h"
+#include "eph_rk12_host.h"
 
 namespace eph {
 
@@ -1395,20 +1395,7 @@ static bool g_consts_ready[64];
 cudaError_t upload_constants(int device) {
     if (device >= 0 && device < 64 && g_consts_ready[device]) return cudaSuccess;
     double hi[EPH_RK12_NCOEF], lo[EPH_RK12_NCOEF], dtk[kStages + 1];
-    for (int q = 0; q < EPH_RK12_NCOEF; ++q) {
-        memcpy(&hi[q], &EPH_RK12_COEF_BITS[2 * q], 8);
-        memcpy(&lo[q], &EPH_RK12_COEF_BITS[2 * q + 1], 8);
-    }
-    // c_k accumulated exactly as RungeKutta.impl:118-152: skip zero coefficients, add hi+lo in j order
-    dtk[0] = 0;
-    for (int k = 1; k <= kStages; ++k) {
-        double acc = 0;
-        for (int j = 0; j < k; ++j) {
-            const int ci = k * (k - 1) / 2 + j;
-            if (hi[ci] != 0) acc += hi[ci] + lo[ci];
-        }
-        dtk[k] = acc;
-    }
+    rk12_expand(hi, lo, dtk);
     cudaError_t e = cudaMemcpyToSymbol(c_rk_hi, hi, sizeof(hi));
     if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_rk_lo, lo, sizeof(lo));
     if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_dtk, dtk, sizeof(dtk));

@@ -137,6 +137,61 @@ class Context:
         return out[:gg.value * pp.value].reshape(gg.value, pp.value)
 
 
+class Batch:
+    """Many independent systems integrated together (eph_batch_* of include/eph_b200.h): the point-like
+    (Newtonian + 1PN) ones in one persistent launch, one CTA per system; the others one by one."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load_library()
+        h = ctypes.c_void_p()
+        check(self.lib.eph_batch_create(device, ctypes.byref(h)), None, "eph_batch_create")
+        self.h = h
+        self.sizes = []
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.eph_batch_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def _check(self, rc, what):
+        if rc:
+            from ._lib import EphError
+            raise EphError(rc, f"{what}: {self.lib.eph_batch_last_error(self.h).decode()}")
+
+    def upload(self, planes: list, models: list | None = None):
+        pls = [np.ascontiguousarray(p, np.float64) for p in planes]
+        mods = [m or Models.empty() for m in (models or [None] * len(pls))]
+        self._keep = (pls, mods)
+        n = (ctypes.c_int64 * len(pls))(*[p.shape[1] for p in pls])
+        ptrs = (ctypes.POINTER(ctypes.c_double) * len(pls))(*[_dptr(p) for p in pls])
+        self._structs = [m.struct() for m in mods]
+        mptrs = (ctypes.POINTER(EphModels) * len(pls))(*[ctypes.pointer(st) for st in self._structs])
+        self._check(self.lib.eph_batch_upload(self.h, len(pls), n, ptrs, mptrs), "batch upload")
+        self.sizes = [p.shape[1] for p in pls]
+
+    def integrate(self, dt, n_step, t_eph=None):
+        k = len(self.sizes)
+        dts = np.ascontiguousarray(np.broadcast_to(np.asarray(dt, np.float64), (k,)))
+        ns = (ctypes.c_int64 * k)(*np.broadcast_to(np.asarray(n_step, np.int64), (k,)).tolist())
+        hi = np.zeros(k) if t_eph is None else np.ascontiguousarray(np.asarray(t_eph, np.float64)[:, 0])
+        lo = np.zeros(k) if t_eph is None else np.ascontiguousarray(np.asarray(t_eph, np.float64)[:, 1])
+        self._check(self.lib.eph_batch_integrate(self.h, _dptr(dts), ns, _dptr(hi), _dptr(lo)), "batch integrate")
+        return np.stack([hi, lo], 1)
+
+    def download(self) -> list:
+        outs = [np.empty((NPLANES, n)) for n in self.sizes]
+        ptrs = (ctypes.POINTER(ctypes.c_double) * len(outs))(*[_dptr(o) for o in outs])
+        self._check(self.lib.eph_batch_download(self.h, ptrs), "batch download")
+        return outs
+
+    def info(self):
+        k, l = ctypes.c_int32(), ctypes.c_int64()
+        self._check(self.lib.eph_batch_info(self.h, ctypes.byref(k), ctypes.byref(l)), "batch info")
+        return k.value, l.value
+
+
 class MSystem:
     """A system of bodies loaded from the reference's initials files and integrated on the GPU."""
 

@@ -196,6 +196,49 @@ def make_config1(seed: int = 1001) -> System:
     return System(bodies=bodies)
 
 
+def make_ensemble_member(seed: int, n_bodies: int, sigma: float = 1e-9) -> System:
+    """The config1 recipe at any size: a star, ceil(n/4) planets and the rest moons (cycled over the
+    planets from the third on, or over all planets when there are at most two), point-mass Newtonian +
+    1PN. Every planet and moon position and velocity component is then scaled by (1 + sigma * N(0, 1))."""
+    rng = np.random.default_rng(seed)
+    n_planets = max(1, math.ceil(n_bodies / 4))
+    n_moons = max(0, n_bodies - 1 - n_planets)
+    star = Body(name="Star", sid="S0", GM=GM_SUN, R_km=6.96e5, inertia=0.4)
+    bodies = [star]
+    planets = []
+    for k in range(n_planets):
+        gm = _loguniform(rng, 1e-9, 1e-3) * GM_SUN
+        a = _loguniform(rng, 0.4, 30.0) * AU
+        r, v = _kepler_state(GM_SUN + gm, a, rng.uniform(0, 0.1), rng.uniform(0, 3 * DEG),
+                             rng.uniform(0, 2 * math.pi), rng.uniform(0, 2 * math.pi),
+                             rng.uniform(0, 2 * math.pi))
+        p = Body(name=f"Planet{k + 1}", sid=f"P{k + 1}", GM=gm, R_km=_radius_km(gm), r=tuple(r), v=tuple(v))
+        planets.append(p)
+        bodies.append(p)
+    first = 2 if n_planets > 2 else 0
+    for k in range(n_moons):
+        host = planets[first + k % (n_planets - first)]
+        ratio = _loguniform(rng, 1e-8, 1e-4)
+        bodies.append(_moon(rng, k + 1, host, host.R_km, ratio, (5, 60), 0.05, 3 * DEG, "M", tidal=False))
+    for b in bodies[1:]:
+        b.r = tuple(np.asarray(b.r) * (1 + sigma * rng.standard_normal(3)))
+        b.v = tuple(np.asarray(b.v) * (1 + sigma * rng.standard_normal(3)))
+    _barycentric(bodies)
+    return System(bodies=bodies)
+
+
+def make_ensemble(n_sys: int = 512, seed: int = 3003, n_range=(8, 300), steps=(500, 20000)):
+    """A batched ensemble: n_sys members of log-uniform size in n_range (member s seeded seed*10^6 + s)
+    and integration lengths uniform in `steps`. Returns [(System, n_steps)]."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for s in range(n_sys):
+        n = int(round(_loguniform(rng, *n_range)))
+        k = int(rng.integers(steps[0], steps[1] + 1))
+        out.append((make_ensemble_member(seed * 1_000_000 + s, n), k))
+    return out
+
+
 def _gp_model(rng, nz=6, nt=4):
     terms = []
     for n in range(3, nz + 1):

@@ -100,6 +100,27 @@ int64_t eph_launch_count(const eph_ctx *ctx);
 int eph_profile_phases(eph_ctx *ctx, int enable);
 int eph_phase_times(eph_ctx *ctx, uint64_t *out, int *grid, int *phases);
 
+/* ---- Batched ensembles (no counterpart in the reference, which integrates one msystem per call; its
+ * combined integrator runs subsystems one at a time, mass_combined.cpp:286-321). Many independent systems,
+ * each with its own dt, step count and ephemeris time, integrated with msystem::integrate semantics
+ * (mass.cpp:399-442). Systems whose bodies are all point-like (Newtonian + 1PN only) share one persistent
+ * launch, one CTA per system; any other system runs through the single-system kernel. */
+typedef struct eph_batch eph_batch;
+int eph_batch_create(int device, eph_batch **out);
+int eph_batch_destroy(eph_batch *b);
+const char *eph_batch_last_error(const eph_batch *b);
+/* n_sys systems: system s has n_body[s] bodies, planes[s] = [EPH_NPLANES][n_body[s]] (host), models[s]
+ * (NULL array or NULL entry: no geopotential / ring models). Replaces any previous batch. */
+int eph_batch_upload(eph_batch *b, int32_t n_sys, const int64_t *n_body, const double *const *planes,
+                     const eph_models *const *models);
+/* Integrate system s by n_step[s] steps of dt[s] (negative n_step: backwards) from t_eph[s] =
+ * t_eph_hi[s] + t_eph_lo[s], which advances in double-double. */
+int eph_batch_integrate(eph_batch *b, const double *dt, const int64_t *n_step, double *t_eph_hi, double *t_eph_lo);
+/* Copy every system's planes back into planes[s]. */
+int eph_batch_download(eph_batch *b, double *const *planes);
+/* Systems in the shared ensemble launch, and launches issued so far. */
+int eph_batch_info(const eph_batch *b, int32_t *n_ensemble, int64_t *launches);
+
 /* Limits of eph_integrate_noalloc's fixed scratch (about 2.5 MB of device memory per GPU). */
 #define EPH_NOALLOC_MAX_BODIES 1024
 #define EPH_NOALLOC_MAX_EXT 16     /* bodies with a geopotential or ring model */
