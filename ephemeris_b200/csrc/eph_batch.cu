@@ -5,8 +5,9 @@
 // harmonics, spin, luminosity, radiation receptance, geopotential or ring: the Newtonian + 1PN systems of
 // an ensemble) run in `ensemble_kernel`: one CTA integrates one whole system, so a stage needs only
 // CTA barriers, and persistent CTAs take systems from an atomic queue, heaviest (bodies^2 x steps) first.
-// The bodies' stage data sit in shared memory as structure-of-arrays rows; the RK12 stage accumulators
-// and the start-of-step state sit in global scratch (L2-resident for ensemble sizes). Any other system
+// The bodies' stage data sit in shared memory as structure-of-arrays rows; the stage values f_j and the
+// start-of-step state sit in global scratch (L2-resident for ensemble sizes), and each body's thread
+// forms sum_j a_kj f_j at its state update (independent loads, ascending j as in the reference). Any other system
 // of the batch (a full-physics body, or more bodies than one CTA's shared memory holds) is integrated by
 // the per-system persistent kernel of eph_step.cu through a context, one after another.
 //
@@ -20,6 +21,7 @@
 // For such bodies the reference's angular velocity, G*L and harmonics stay constant (w = G*L = 0), the
 // frame rotations are the identity and only the end-of-step orthogonalisation of the frame acts
 // (mass.h:147-150); the RK12 combination and state update are those of RungeKutta.impl:148-186.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -41,9 +43,10 @@ namespace eph {
 namespace {
 
 constexpr int kBThreads = 256;          // threads per ensemble CTA
-constexpr int kBRed = 5;                // reduction slots per thread
+constexpr int kCluster = 8;             // CTAs of a thread-block cluster that share one large system
+constexpr int kCoopMin = 96;            // bodies from which a system is shared by a cluster
 constexpr double kCB = 299792458.0;     // src/math/basic_math.h:10,18
-constexpr int kAcc = 9;                 // accumulators per (body, stage): velocity dd (hi 3, lo 3), acceleration 3
+constexpr int kAcc = 9;                 // stored values per (body, stage): velocity dd (hi 3, lo 3), acceleration 3
 
 __constant__ double b_rk_hi[EPH_RK12_NCOEF];
 __constant__ double b_rk_lo[EPH_RK12_NCOEF];
@@ -56,7 +59,7 @@ struct BatchSys {
     double dt;            // signed step
     double t_eph;         // double(t_eph) at the start
     double *planes;       // [EPH_NPLANES][n], in and out
-    double *acc;          // [n][kStages][kAcc] stage accumulators
+    double *acc;          // [kStages][kAcc][n] stage values f_j: velocity (hi 3, lo 3), acceleration 3
     double *x0;           // [12][n] start-of-step r, v (hi, lo)
 };
 
@@ -67,7 +70,6 @@ enum BRow { BR_R_HI = 0, BR_R_LO = 3, BR_GM = 6, BR_SR2 = 7, BR_PHI = 8, BR_NACC
 
 struct BatchView {
     double *T;    // rows
-    double *red;  // [kBThreads][kBRed]
     int ld;
 };
 
@@ -126,21 +128,37 @@ __device__ __forceinline__ void pair_point_b(const BatchView &V, int i, int j, d
     acc[2] += g.z;
 }
 
-// Threads of a pass: with n <= blockDim bodies, G = blockDim / n consecutive threads share body i and
-// split its j range (their partial sums are added in thread order afterwards); with more bodies each
-// thread takes whole bodies.
+// Threads of a pass: with n <= blockDim bodies, G consecutive lanes of a warp share body i and split its j
+// range (G = the largest power of two <= min(32, blockDim / n)); their partial sums are combined by warp
+// shuffles. With more bodies than threads each thread takes whole bodies.
 struct PassMap {
     int G, i, sub;
     bool grouped, active;
 };
-__device__ __forceinline__ PassMap pass_map(int n) {
+__device__ __forceinline__ PassMap pass_map(int lo, int hi) {
+    const int cnt = hi - lo;
     PassMap m;
-    m.grouped = n <= (int)blockDim.x;
-    m.G = m.grouped ? (int)blockDim.x / n : 1;
-    m.i = threadIdx.x / m.G;
-    m.sub = threadIdx.x % m.G;
-    m.active = m.grouped && m.i < n;
+    m.grouped = cnt <= (int)blockDim.x;
+    int g = 1;
+    if (m.grouped)
+        while (g < 32 && 2 * g * cnt <= (int)blockDim.x) g *= 2;
+    m.G = g;
+    m.i = lo + (int)threadIdx.x / g;
+    m.sub = threadIdx.x % g;
+    m.active = m.grouped && m.i < hi;
     return m;
+}
+// sum (or NaN-propagating maximum) over the G lanes of a group; every lane of the warp takes part
+__device__ __forceinline__ double group_sum(double v, int G) {
+    for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ double group_max(double v, int G) {
+    for (int o = G / 2; o > 0; o >>= 1) {
+        const double u = __shfl_xor_sync(0xffffffffu, v, o);
+        checked_maximize(v, u);
+    }
+    return v;
 }
 
 // pass A for body i over j ≡ sub (mod G), then PREPARE_RELATIVITY by whoever holds the total
@@ -160,30 +178,37 @@ __device__ __forceinline__ void prepare_body(const BatchView &V, int i, const do
     row(V, BR_NACC + 2, i) = na.z;
 }
 
-__device__ void pass_point_a(const BatchView &V, int n) {
-    const PassMap m = pass_map(n);
+// pass A (and PREPARE_RELATIVITY) of the bodies i in [lo, hi) against all n bodies
+__device__ void pass_point_a(const BatchView &V, int n, int lo, int hi) {
+    const PassMap m = pass_map(lo, hi);
     if (m.grouped) {
-        double acc[4] = {0, 0, 0, 0};
-        if (m.active)
+        // two independent pair chains per thread (j and j + G), added at the end
+        double acc[4] = {0, 0, 0, 0}, acc2[4] = {0, 0, 0, 0};
+        if (m.active) {
+            int j = m.sub;
 #pragma unroll 1
-            for (int j = m.sub; j < n; j += m.G)
+            for (; j + m.G < n; j += 2 * m.G) {
                 if (j != m.i) pair_point_a(V, m.i, j, acc);
-        for (int c = 0; c < 4; ++c) V.red[threadIdx.x * kBRed + c] = acc[c];
-        __syncthreads();
-        if (m.active && m.sub == 0) {
-            double s[4] = {0, 0, 0, 0};
-            for (int q = 0; q < m.G; ++q)
-                for (int c = 0; c < 4; ++c) s[c] += V.red[(threadIdx.x + q) * kBRed + c];
-            prepare_body(V, m.i, s);
+                if (j + m.G != m.i) pair_point_a(V, m.i, j + m.G, acc2);
+            }
+            if (j < n && j != m.i) pair_point_a(V, m.i, j, acc);
         }
+        double s[4];
+        for (int c = 0; c < 4; ++c) s[c] = group_sum(acc[c] + acc2[c], m.G);
+        if (m.active && m.sub == 0) prepare_body(V, m.i, s);
     } else {
         // whole bodies per thread: prepare_body writes only rows pass A does not read (it reads r, GM, sR2)
 #pragma unroll 1
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            double s[4] = {0, 0, 0, 0};
+        for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+            double s[4] = {0, 0, 0, 0}, s2[4] = {0, 0, 0, 0};
+            int j = 0;
 #pragma unroll 1
-            for (int j = 0; j < n; ++j)
+            for (; j + 1 < n; j += 2) {
                 if (j != i) pair_point_a(V, i, j, s);
+                if (j + 1 != i) pair_point_a(V, i, j + 1, s2);
+            }
+            if (j < n && j != i) pair_point_a(V, i, j, s);
+            for (int c = 0; c < 4; ++c) s[c] += s2[c];
             prepare_body(V, i, s);
         }
     }
@@ -217,41 +242,51 @@ __device__ __forceinline__ void extremes_of(const PairMax &x, double &inv_r, dou
     } else infl = 0.0;
 }
 
-__device__ void pass_point_b(const BatchView &V, int n) {
-    const PassMap m = pass_map(n);
+// pass B and finalisation of the bodies i in [lo, hi) against all n bodies
+__device__ void pass_point_b(const BatchView &V, int n, int lo, int hi) {
+    const PassMap m = pass_map(lo, hi);
     const double inf = __longlong_as_double(0x7ff0000000000000ll);
     if (m.grouped) {
-        double acc[3] = {0, 0, 0};
-        PairMax x{inf, 0.0, 0.0, 0.0};
-        if (m.active)
+        double acc[3] = {0, 0, 0}, acc2[3] = {0, 0, 0};
+        PairMax x{inf, 0.0, 0.0, 0.0}, x2{inf, 0.0, 0.0, 0.0};
+        if (m.active) {
+            int j = m.sub;
 #pragma unroll 1
-            for (int j = m.sub; j < n; j += m.G)
+            for (; j + m.G < n; j += 2 * m.G) {
                 if (j != m.i) pair_point_b(V, m.i, j, acc, x);
-        double e0, e1;
-        extremes_of(x, e0, e1);
-        double *r = V.red + threadIdx.x * kBRed;
-        r[0] = acc[0]; r[1] = acc[1]; r[2] = acc[2]; r[3] = e0; r[4] = e1;
-        __syncthreads();
-        if (m.active && m.sub == 0) {
-            double s[5] = {0, 0, 0, V.red[threadIdx.x * kBRed + 3], V.red[threadIdx.x * kBRed + 4]};
-            for (int q = 0; q < m.G; ++q) {
-                const double *t = V.red + (threadIdx.x + q) * kBRed;
-                s[0] += t[0]; s[1] += t[1]; s[2] += t[2];
-                if (q) { checked_maximize(s[3], t[3]); checked_maximize(s[4], t[4]); }
+                if (j + m.G != m.i) pair_point_b(V, m.i, j + m.G, acc2, x2);
             }
-            finish_body(V, m.i, s);
+            if (j < n && j != m.i) pair_point_b(V, m.i, j, acc, x);
         }
+        double e0, e1, f0, f1;
+        extremes_of(x, e0, e1);
+        extremes_of(x2, f0, f1);
+        checked_maximize(e0, f0);
+        checked_maximize(e1, f1);
+        double s[5];
+        for (int c = 0; c < 3; ++c) s[c] = group_sum(acc[c] + acc2[c], m.G);
+        s[3] = group_max(e0, m.G);
+        s[4] = group_max(e1, m.G);
+        if (m.active && m.sub == 0) finish_body(V, m.i, s);
     } else {
         // finish_body writes only rows pass B does not read (GA, FA, MIND, MAXI)
 #pragma unroll 1
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            double acc[3] = {0, 0, 0};
-            PairMax x{inf, 0.0, 0.0, 0.0};
+        for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+            double acc[3] = {0, 0, 0}, acc2[3] = {0, 0, 0};
+            PairMax x{inf, 0.0, 0.0, 0.0}, x2{inf, 0.0, 0.0, 0.0};
+            int j = 0;
 #pragma unroll 1
-            for (int j = 0; j < n; ++j)
+            for (; j + 1 < n; j += 2) {
                 if (j != i) pair_point_b(V, i, j, acc, x);
-            double s[5] = {acc[0], acc[1], acc[2], 0, 0};
+                if (j + 1 != i) pair_point_b(V, i, j + 1, acc2, x2);
+            }
+            if (j < n && j != i) pair_point_b(V, i, j, acc, x);
+            double s[5] = {acc[0] + acc2[0], acc[1] + acc2[1], acc[2] + acc2[2], 0, 0};
+            double f0, f1;
             extremes_of(x, s[3], s[4]);
+            extremes_of(x2, f0, f1);
+            checked_maximize(s[3], f0);
+            checked_maximize(s[4], f1);
             finish_body(V, i, s);
         }
     }
@@ -281,8 +316,31 @@ __device__ void orthogonalize_frame(double *pl, int n, int i) {
     }
 }
 
-__device__ void integrate_system(const BatchSys &Y, const BatchView &V) {
+namespace cg = cooperative_groups;
+
+// Copy rows [row0, row0 + nrows) of the bodies [lo, hi) into the shared memory of every other CTA of the
+// cluster (distributed shared memory); the cluster barrier that follows publishes them.
+__device__ void broadcast_rows(const BatchView &V, int row0, int nrows, int lo, int hi, int rank) {
+    cg::cluster_group cl = cg::this_cluster();
+    const int cnt = hi - lo;
+    for (int q = 0; q < kCluster; ++q) {
+        if (q == rank) continue;
+        double *peer = cl.map_shared_rank(V.T, q);
+        for (int idx = threadIdx.x; idx < nrows * cnt; idx += blockDim.x) {
+            const int r = row0 + idx / cnt, i = lo + idx % cnt;
+            peer[r * V.ld + i] = V.T[r * V.ld + i];
+        }
+    }
+}
+
+// One system on one CTA (coop = false) or on the kCluster CTAs of a cluster (coop = true), this CTA
+// owning bodies [lo, hi): every CTA holds all bodies' rows, computes its own bodies' stages and passes,
+// and sends the rows the other CTAs read (positions and GM after the state update, the pass-A outputs
+// after pass A) to their shared memory.
+__device__ void integrate_system(const BatchSys &Y, const BatchView &V, bool coop, int rank) {
     const int n = Y.n;
+    const int lo = coop ? (int)((long long)rank * n / kCluster) : 0;
+    const int hi = coop ? (int)((long long)(rank + 1) * n / kCluster) : n;
     double *pl = Y.planes;
 #define PLV(p, i) pl[(size_t)(p) * n + (i)]
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
@@ -315,48 +373,45 @@ __device__ void integrate_system(const BatchSys &Y, const BatchView &V) {
     for (long long step = 0; step < Y.n_step; ++step) {
 #pragma unroll 1
         for (int s = 0; s < kStages; ++s) {
-            if (s == 0) {   // x0 = x (RungeKutta.impl:113)
-                for (int i = threadIdx.x; i < n; i += blockDim.x)
+            // f_s of every body into the stage store; at s == 0 also x0 = x (RungeKutta.impl:113-121).
+            // Each thread keeps the same bodies throughout, so what it stores it reads back itself.
+            const int k = s + 1;
+            const double t = Y.t_eph + dt * (b_dtk[k] + (double)step);
+            const int ci0 = k * (k - 1) / 2;
+#pragma unroll 1
+            for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+                double *F = Y.acc + (size_t)s * kAcc * n + i;   // [stage][component][body]
+                for (int c = 0; c < 3; ++c) {
+                    F[(size_t)c * n] = row(V, BR_V_HI + c, i);
+                    F[(size_t)(3 + c) * n] = row(V, BR_V_LO + c, i);
+                    F[(size_t)(6 + c) * n] = row(V, BR_FA + c, i);
+                }
+                if (s == 0)
                     for (int c = 0; c < 3; ++c) {
                         Y.x0[(0 + c) * n + i] = row(V, BR_R_HI + c, i);
                         Y.x0[(3 + c) * n + i] = row(V, BR_R_LO + c, i);
                         Y.x0[(6 + c) * n + i] = row(V, BR_V_HI + c, i);
                         Y.x0[(9 + c) * n + i] = row(V, BR_V_LO + c, i);
                     }
-            }
-            // a_{k,s} f_s into the accumulators of stages k = s+1..25, ascending in s (RungeKutta.impl:148-162)
-            const int nk = kStages - s;
-#pragma unroll 1
-            for (int item = threadIdx.x; item < n * nk * 6; item += blockDim.x) {
-                const int i = item / (nk * 6), rem = item % (nk * 6);
-                const int k = s + 1 + rem / 6, c = rem % 6;
-                const int ci = k * (k - 1) / 2 + s;
-                const dd a = dd{b_rk_hi[ci], b_rk_lo[ci]};
-                const bool nz = a.hi != 0;
-                double *A = Y.acc + ((size_t)i * kStages + (k - 1)) * kAcc;
-                if (c < 3) {
-                    dd cur = (s == 0) ? dd_make(0) : dd{A[c], A[3 + c]};
-                    if (nz) cur = dd_add(cur, dd_mul(a, dd{row(V, BR_V_HI + c, i), row(V, BR_V_LO + c, i)}));
-                    A[c] = cur.hi;
-                    A[3 + c] = cur.lo;
-                } else {
-                    const int cc = c - 3;
-                    double cur = (s == 0) ? 0.0 : A[6 + cc];
-                    if (nz) cur = __dadd_rn(cur, __dmul_rn(dd_val(a), row(V, BR_FA + cc, i)));
-                    A[6 + cc] = cur;
+                // state of stage k: sum_j a_kj f_j in ascending j, zero coefficients skipped
+                // (RungeKutta.impl:148-162), then r = r0 + dt v, v = v0 + dt a (RungeKutta.impl:164-186)
+                dd sv[3] = {dd_make(0), dd_make(0), dd_make(0)};
+                double sa[3] = {0.0, 0.0, 0.0};
+#pragma unroll 4
+                for (int j = 0; j < k; ++j) {
+                    const dd a = dd{b_rk_hi[ci0 + j], b_rk_lo[ci0 + j]};
+                    if (a.hi == 0) continue;
+                    const double fa = dd_val(a);
+                    const double *Fj = Y.acc + (size_t)j * kAcc * n + i;
+                    for (int c = 0; c < 3; ++c) {
+                        sv[c] = dd_add(sv[c], dd_mul(a, dd{Fj[(size_t)c * n], Fj[(size_t)(3 + c) * n]}));
+                        sa[c] = __dadd_rn(sa[c], __dmul_rn(fa, Fj[(size_t)(6 + c) * n]));
+                    }
                 }
-            }
-            __syncthreads();
-            // state of stage k = s+1 (RungeKutta.impl:164-186)
-            const int k = s + 1;
-            const double t = Y.t_eph + dt * (b_dtk[k] + (double)step);
-#pragma unroll 1
-            for (int i = threadIdx.x; i < n; i += blockDim.x) {
-                const double *A = Y.acc + ((size_t)i * kStages + (k - 1)) * kAcc;
                 const dd ddt = dd_make(dt);
                 for (int c = 0; c < 3; ++c) {
-                    const dd r = dd_add(dd{Y.x0[(0 + c) * n + i], Y.x0[(3 + c) * n + i]}, dd_mul(ddt, dd{A[c], A[3 + c]}));
-                    const dd v = dd_add(dd{Y.x0[(6 + c) * n + i], Y.x0[(9 + c) * n + i]}, dd_make(dt * A[6 + c]));
+                    const dd r = dd_add(dd{Y.x0[(0 + c) * n + i], Y.x0[(3 + c) * n + i]}, dd_mul(ddt, sv[c]));
+                    const dd v = dd_add(dd{Y.x0[(6 + c) * n + i], Y.x0[(9 + c) * n + i]}, dd_make(dt * sa[c]));
                     row(V, BR_R_HI + c, i) = r.hi;
                     row(V, BR_R_LO + c, i) = r.lo;
                     row(V, BR_V_HI + c, i) = v.hi;
@@ -366,13 +421,21 @@ __device__ void integrate_system(const BatchSys &Y, const BatchView &V) {
                 if (k == kStages) orthogonalize_frame(pl, n, i);
             }
             __syncthreads();
-            pass_point_a(V, n);
-            pass_point_b(V, n);
+            if (coop) {
+                broadcast_rows(V, BR_R_HI, BR_GM + 1 - BR_R_HI, lo, hi, rank);
+                cg::this_cluster().sync();
+            }
+            pass_point_a(V, n, lo, hi);
+            if (coop) {
+                broadcast_rows(V, BR_PHI, BR_BETA2 + 1 - BR_PHI, lo, hi, rank);
+                cg::this_cluster().sync();
+            }
+            pass_point_b(V, n, lo, hi);
         }
     }
     // store (cuda_rungekutta_kernel_config::save of RungeKutta.cu:124-133); min_distance inverted (mass.cpp:436)
     const double c2 = kCB * kCB;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
         for (int c = 0; c < 3; ++c) {
             PLV(EPH_P_R_HI + c, i) = row(V, BR_R_HI + c, i);
             PLV(EPH_P_R_LO + c, i) = row(V, BR_R_LO + c, i);
@@ -394,25 +457,47 @@ __device__ void integrate_system(const BatchSys &Y, const BatchView &V) {
     __syncthreads();
 }
 
-__global__ void __launch_bounds__(kBThreads) ensemble_kernel(const BatchSys *sys, const int *order, int n_sys, int *next,
-                                                             int ld) {
+// Persistent CTAs in clusters of kCluster. Jobs [0, n_coop) of the queue (the large systems) are taken a
+// cluster at a time and shared by its CTAs; once a cluster draws a job past them, its CTAs take the
+// remaining jobs one CTA each.
+__global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kBThreads, 2)
+    ensemble_kernel(const BatchSys *sys, const int *order, int n_sys, int n_coop, int *next, int ld) {
     extern __shared__ __align__(16) double bsm[];
     __shared__ int s_job;
-    const BatchView V{bsm, bsm + (size_t)BR_ROWS * ld, ld};
+    const BatchView V{bsm, ld};
+    cg::cluster_group cl = cg::this_cluster();
+    const int rank = (int)cl.block_rank();
+    bool together = true;
 #pragma unroll 1
     for (;;) {
-        if (threadIdx.x == 0) s_job = atomicAdd(next, 1);
-        __syncthreads();
-        const int job = s_job;
-        __syncthreads();
-        if (job >= n_sys) return;
-        integrate_system(sys[order[job]], V);
+        int job;
+        if (together) {
+            cl.sync();   // every CTA of the cluster is done with the previous job and its shared memory
+            if (rank == 0 && threadIdx.x == 0) s_job = atomicAdd(next, 1);
+            cl.sync();
+            job = *cl.map_shared_rank(&s_job, 0);
+            cl.sync();   // read by all before rank 0 may reuse s_job
+            if (job >= n_sys) return;
+            if (job < n_coop) {
+                integrate_system(sys[order[job]], V, true, rank);
+                continue;
+            }
+            together = false;
+            if (rank != 0) continue;   // rank 0 keeps this job, the others draw their own
+        } else {
+            if (threadIdx.x == 0) s_job = atomicAdd(next, 1);
+            __syncthreads();
+            job = s_job;
+            __syncthreads();
+            if (job >= n_sys) return;
+        }
+        integrate_system(sys[order[job]], V, false, 0);
     }
 }
 
-size_t ensemble_smem(int ld) { return ((size_t)BR_ROWS * ld + (size_t)kBThreads * kBRed) * sizeof(double); }
+size_t ensemble_smem(int ld) { return (size_t)BR_ROWS * ld * sizeof(double); }
 constexpr size_t kBMaxSmem = 227 * 1024 - 1024;
-int ensemble_max_bodies() { return (int)((kBMaxSmem / sizeof(double) - (size_t)kBThreads * kBRed) / BR_ROWS) / kPad * kPad; }
+int ensemble_max_bodies() { return (int)(kBMaxSmem / sizeof(double) / BR_ROWS) / kPad * kPad; }
 
 bool g_batch_ready[64];
 cudaError_t batch_setup(int device) {
@@ -602,8 +687,15 @@ int eph_batch_integrate(eph_batch *b, const double *dt, const int64_t *n_step, d
         work[s] = (double)n * (double)n * (double)Y.n_step;
         order.push_back(s);
     }
-    // heaviest systems first, so the last systems to start are short ones
-    std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return work[a] > work[c]; });
+    // the large systems (shared by a cluster) first, then the others; each group heaviest first, so the
+    // last systems to start are short ones
+    std::stable_sort(order.begin(), order.end(), [&](int a, int c) {
+        const bool ca = b->n_body[a] >= kCoopMin, cc = b->n_body[c] >= kCoopMin;
+        if (ca != cc) return ca;
+        return work[a] > work[c];
+    });
+    int n_coop = 0;
+    for (int s : order) n_coop += b->n_body[s] >= kCoopMin;
     if (!order.empty()) {
         BCK(cudaMemcpyAsync(b->d_sys, tab.data(), (size_t)n_sys * sizeof(BatchSys), cudaMemcpyHostToDevice, b->stream),
             "upload batch table");
@@ -614,8 +706,11 @@ int eph_batch_integrate(eph_batch *b, const double *dt, const int64_t *n_step, d
         int per_sm = 0, sms = 0;
         BCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ensemble_kernel, kBThreads, smem), "occupancy");
         BCK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device), "SM count");
-        const int grid = std::max(1, std::min((int)order.size(), per_sm * sms));
-        ensemble_kernel<<<grid, kBThreads, smem, b->stream>>>(b->d_sys, b->d_order, (int)order.size(), b->d_next, b->ld);
+        // whole clusters; clusters that find no room start when others finish (no CTA waits on another cluster)
+        int grid = std::min((int)order.size() * kCluster, std::max(per_sm * sms, kCluster));
+        grid = std::max(kCluster, grid / kCluster * kCluster);
+        ensemble_kernel<<<grid, kBThreads, smem, b->stream>>>(b->d_sys, b->d_order, (int)order.size(), n_coop, b->d_next,
+                                                              b->ld);
         BCK(cudaGetLastError(), "launch ensemble kernel");
         b->launches++;
     }

@@ -1,10 +1,10 @@
 """Batched ensembles (eph_batch_*): every system of a batch against the oracle and the single-system path.
 
 Members follow the config1 recipe at sizes from 2 to 300 bodies (Newtonian + 1PN: they share the one
-persistent ensemble launch); a full-physics system in the same batch goes through the single-system
-kernel. Tolerances are those of tests/test_gpu_parity.py: position 1e-12 of |r - r_star|, acceleration
-1e-14 of sum_j |GM_j/r_ij^2|, and the reference's own maxima bound (1e-15 relative,
-src/tests/test_integrator.cpp:15-20).
+persistent ensemble launch; from 96 bodies on a system is shared by the CTAs of a cluster); a
+full-physics system in the same batch goes through the single-system kernel. Tolerances are those of
+tests/test_gpu_parity.py: position 1e-12 of |r - r_star|, acceleration 1e-14 of sum_j |GM_j/r_ij^2|,
+and the reference's own maxima bound (1e-15 relative, src/tests/test_integrator.cpp:15-20).
 """
 import os
 
@@ -59,8 +59,8 @@ def test_ensemble_matches_oracle(tmp_path, oracle):
         assert tuple(tt) == tuple(tref)
 
 
-def test_ensemble_more_bodies_than_threads(tmp_path, oracle):
-    """300 bodies: more than the CTA's 256 threads, so every thread takes whole bodies."""
+def test_ensemble_cluster_shared_system(tmp_path, oracle):
+    """300 bodies: shared by the CTAs of a thread-block cluster, each owning a slice of the bodies."""
     from ephemeris_b200 import Batch
     mem = _members(tmp_path, [300], seed=3004)
     b = Batch(0)
