@@ -43,7 +43,7 @@ namespace eph {
 namespace {
 
 constexpr int kBThreads = 256;          // threads per ensemble CTA
-constexpr int kCluster = 8;             // CTAs of a thread-block cluster that share one large system
+constexpr int kCluster = 4;             // CTAs of a thread-block cluster that share one large system
 constexpr int kCoopMin = 96;            // bodies from which a system is shared by a cluster
 constexpr double kCB = 299792458.0;     // src/math/basic_math.h:10,18
 constexpr int kAcc = 9;                 // stored values per (body, stage): velocity dd (hi 3, lo 3), acceleration 3
@@ -519,7 +519,8 @@ using namespace eph;
 
 struct eph_batch {
     int device = 0;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;     // work stream (own_stream unless eph_batch_set_stream chose another)
+    cudaStream_t own_stream = nullptr;
     std::mutex mu;
     char err[512] = {0};
     int n_sys = 0;
@@ -584,7 +585,8 @@ int eph_batch_destroy(eph_batch *b) {
     cudaSetDevice(b->device);
     batch_free(b);
     if (b->ctx) eph_ctx_destroy(b->ctx);
-    if (b->stream) cudaStreamDestroy(b->stream);
+    if (b->own_stream) cudaStreamDestroy(b->own_stream);
+    else if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
     return EPH_OK;
 }
@@ -768,6 +770,14 @@ int eph_batch_download(eph_batch *b, double *const *planes) {
             memcpy(planes[s], b->h_full[s].data(), bytes);
     }
     BCK(cudaStreamSynchronize(b->stream), "download batch");
+    return EPH_OK;
+}
+
+int eph_batch_set_stream(eph_batch *b, void *stream) {
+    if (!b) return EPH_ERR_ARG;
+    std::lock_guard<std::mutex> lock(b->mu);
+    if (!b->own_stream) b->own_stream = b->stream;
+    b->stream = stream ? (cudaStream_t)stream : b->own_stream;
     return EPH_OK;
 }
 

@@ -186,6 +186,9 @@ class Batch:
         self._check(self.lib.eph_batch_download(self.h, ptrs), "batch download")
         return outs
 
+    def set_stream(self, stream_handle: int | None):
+        self._check(self.lib.eph_batch_set_stream(self.h, ctypes.c_void_p(stream_handle or 0)), "batch set_stream")
+
     def info(self):
         k, l = ctypes.c_int32(), ctypes.c_int64()
         self._check(self.lib.eph_batch_info(self.h, ctypes.byref(k), ctypes.byref(l)), "batch info")

@@ -118,6 +118,9 @@ int eph_batch_upload(eph_batch *b, int32_t n_sys, const int64_t *n_body, const d
 int eph_batch_integrate(eph_batch *b, const double *dt, const int64_t *n_step, double *t_eph_hi, double *t_eph_lo);
 /* Copy every system's planes back into planes[s]. */
 int eph_batch_download(eph_batch *b, double *const *planes);
+/* Issue the batch's device work on `stream` (a cudaStream_t of its device; NULL restores its own stream).
+ * Calls still return only after their work has finished. */
+int eph_batch_set_stream(eph_batch *b, void *stream);
 /* Systems in the shared ensemble launch, and launches issued so far. */
 int eph_batch_info(const eph_batch *b, int32_t *n_ensemble, int64_t *launches);
 
