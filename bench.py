@@ -221,6 +221,197 @@ def run_reference(args):
         print(json.dumps(line), flush=True)
 
 
+def load_ensemble(args, tmpdir, device=0):
+    """The batched-ensemble workload: members of the config1 recipe (8-300 bodies), each loaded by the
+    product loader; durations scaled by --ens-frac (at least one step)."""
+    from ephemeris_b200 import MSystem, synth
+    ens = synth.make_ensemble(args.ens_systems)
+    pls, mds, dts, ks, cfgs = [], [], [], [], []
+    for s, (m, k) in enumerate(ens):
+        cfg = synth.write_system(m, os.path.join(tmpdir, f"s{s}"))
+        ms = MSystem(device)
+        if not ms.load(cfg):
+            raise RuntimeError("ensemble member failed to load")
+        pls.append(ms.planes())
+        mds.append(ms.models())
+        dts.append(ms.delta_t)
+        ks.append(max(1, int(round(k * args.ens_frac))))
+        cfgs.append(cfg)
+        ms.close()
+    return pls, mds, dts, ks, cfgs
+
+
+def _ensemble_flops(pls, ks):
+    """Algorithmic FLOPs of the ensemble run: Newtonian + 1PN pairs and the RK update, per the convention."""
+    return float(sum(k * (25 * n * (n - 1) * (FLOP_PASS_A + FLOP_1PN) + n * FLOP_RK)
+                     for n, k in ((p.shape[1], k) for p, k in zip(pls, ks))))
+
+
+def _ref_member(args):
+    """One ensemble member through the reference's serial integrator (a worker process)."""
+    cfg, n_step = args
+    from oracle.pyoracle import RefSystem
+    ref = RefSystem(cfg)
+    dt = ref.lib().ref_delta_t(ref.h)
+    t0 = time.perf_counter()
+    ref.integrate(dt, n_step)
+    return ref.n * n_step, time.perf_counter() - t0
+
+
+# The reference's msystem::load ends with an orbit-structure analysis (msystem::analyse) that does not
+# finish within seconds for about a quarter of the synthetic ensemble members (found by loading each with a
+# time limit); the integrator is not involved. The CPU sample therefore takes members of at most this many
+# bodies whose reference load finishes within ENS_CPU_LOAD_S seconds. Smaller systems cost the CPU less per
+# body-step, so the sample favours the CPU.
+ENS_CPU_MAX_BODIES = 100
+ENS_CPU_LOAD_S = 5.0
+
+
+def _loadable(cfgs):
+    """The configs whose reference load finishes within ENS_CPU_LOAD_S (one child process each)."""
+    code = ("import sys; sys.path.insert(0, %r); from oracle.pyoracle import RefSystem; RefSystem(sys.argv[1])"
+            % os.path.dirname(os.path.abspath(__file__)))
+    procs = [subprocess.Popen([sys.executable, "-c", code, c], stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+             for c in cfgs]
+    t_end = time.perf_counter() + ENS_CPU_LOAD_S + 10.0   # interpreter start-up on top of the load itself
+    ok = []
+    for c, p in zip(cfgs, procs):
+        try:
+            p.wait(timeout=max(0.1, t_end - time.perf_counter()))
+            if p.returncode == 0:
+                ok.append(c)
+        except subprocess.TimeoutExpired:
+            p.kill()
+            p.wait()
+    return ok
+
+
+def ensemble_cpu(cfgs, sizes, n_members, n_step):
+    """Reference CPU throughput on the ensemble: one member per worker process, all host cores."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+    cores = os.cpu_count() or 1
+    picks = _loadable([c for c, n in zip(cfgs, sizes) if n <= ENS_CPU_MAX_BODIES][:2 * n_members])[:n_members]
+    jobs = [(c, n_step) for c in picks]
+    with cf.ProcessPoolExecutor(max_workers=cores, mp_context=mp.get_context("spawn")) as ex:
+        list(ex.map(_ref_member, [(c, 1) for c in picks[:cores]]))   # start the workers
+        t0 = time.perf_counter()
+        done = list(ex.map(_ref_member, jobs))
+        el = time.perf_counter() - t0
+    body_steps = sum(b for b, _ in done)
+    return {"value": body_steps / el, "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": f"{len(jobs)} ensemble members of <= {ENS_CPU_MAX_BODIES} bodies (reference load within "
+                      f"{ENS_CPU_LOAD_S:.0f} s) x {n_step} RK12 steps, "
+                      f"reference msystem::integrate(dt,n,0) serial, one member per process on {cores} processes, "
+                      f"{el:.1f} s"}
+
+
+def run_b200_ensemble(args):
+    import torch
+    from ephemeris_b200 import Batch
+    rank, world, local, pg = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    with tempfile.TemporaryDirectory() as td:
+        pls, mds, dts, ks, cfgs = load_ensemble(args, td, local)
+        stream = torch.cuda.Stream(dev)
+        torch.cuda.set_stream(stream)
+        b = Batch(local)
+        b.set_stream(stream.cuda_stream)
+        flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+        for _ in range(args.warmup):   # warm-up: every member, 20 steps at most
+            b.upload(pls, mds)
+            b.integrate(dts, [min(k, 20) for k in ks])
+        barrier(pg, dev)
+        torch.cuda.synchronize(dev)
+        clocks = ClockSampler(local)
+        clocks.start()
+        l0 = b.info()[1]
+        dev_ms = 0.0
+        for k in range(args.steps):
+            b.upload(pls, mds)                     # inputs in HBM before the timed region
+            flush.fill_(float(k))
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            b.integrate(dts, ks)
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            dev_ms += e0.elapsed_time(e1)
+        clk = clocks.stop()
+        launches = b.info()[1] - l0
+        dev_ms_max = reduce_max(pg, dev_ms, dev)
+        body_steps = float(sum(p.shape[1] * k for p, k in zip(pls, ks)))
+        value = world * body_steps * args.steps / (dev_ms_max / 1e3)
+        # end to end: host planes up, integrate, host planes down
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            b.upload(pls, mds)
+            b.integrate(dts, ks)
+            b.download()
+        e2e_s = reduce_max(pg, time.perf_counter() - t0, dev)
+        e2e = world * body_steps * args.steps / e2e_s
+        bytes_io = int(sum(p.nbytes for p in pls))
+        flops = _ensemble_flops(pls, ks)
+        achieved = flops / (dev_ms / args.steps / 1e3) / 1e12
+        peak, peak_src = fp64_peak(dev)
+        cpu = None
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            try:
+                cpu = ensemble_cpu(cfgs, [p.shape[1] for p in pls], args.ens_cpu_members, args.ens_cpu_steps)
+            except Exception as exc:
+                cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "unavailable", "sample": str(exc)}
+        if rank == 0:
+            sizes = [p.shape[1] for p in pls]
+            line = {
+                "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64 (double-double state)", "data": "synthetic",
+                "config": {"workload": f"config3: {len(pls)}-system ensemble, {min(sizes)}-{max(sizes)} bodies "
+                                       f"(Newtonian + 1PN), durations {min(ks)}-{max(ks)} RK12 steps "
+                                       f"(the 500-20000 draw scaled by {args.ens_frac}), dt=0.05 day",
+                           "systems": len(pls), "bodies": int(sum(sizes)), "body_steps_per_step": body_steps,
+                           "parallelism": f"replicas x{world}" if world > 1 else "one persistent launch, 1 GPU",
+                           "l2": "flushed between timed steps (256 MB write)"},
+                "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": bytes_io, "d2h_bytes_per_step": bytes_io},
+                "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                             "frac": achieved / peak if peak else None, "traffic": None, "peak_source": peak_src,
+                             "flops_per_launch": flops},
+                "gpu_launches": launches,
+                "clocks": clk,
+            }
+            if cpu is not None:
+                line["cpu_baseline"] = cpu
+            print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+def run_reference_ensemble(args):
+    """--impl reference --workload config3: the reference CPU integrator on a sample of the ensemble."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    with tempfile.TemporaryDirectory() as td:
+        from ephemeris_b200 import synth
+        ens = [(m, k) for m, k in synth.make_ensemble(args.ens_systems) if len(m.bodies) <= ENS_CPU_MAX_BODIES]
+        ens = ens[:2 * args.ens_cpu_members]
+        cfgs = [synth.write_system(m, os.path.join(td, f"s{s}")) for s, (m, _) in enumerate(ens)]
+        sizes = [len(m.bodies) for m, _ in ens]
+        vals, cpu = [], None
+        for _ in range(max(1, args.steps)):
+            cpu = ensemble_cpu(cfgs, sizes, args.ens_cpu_members, args.ens_cpu_steps)
+            vals.append(cpu["value"])
+        value = statistics.median(vals)
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64 (double-double state)", "data": "synthetic", "impl": "reference",
+                "config": {"workload": "config3 ensemble, reference CPU sample (see cpu_baseline.sample)"},
+                "cpu_baseline": dict(cpu, value=value),
+                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+
+
 def run_b200(args):
     import torch
     from ephemeris_b200 import Context, MSystem
@@ -372,8 +563,17 @@ def main():
     ap.add_argument("--grid", type=int, default=0)
     ap.add_argument("--per-cta", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ens-systems", type=int, default=512, help="config3: ensemble members")
+    ap.add_argument("--ens-frac", type=float, default=0.1, help="config3: fraction of each member's drawn duration")
+    ap.add_argument("--ens-cpu-members", type=int, default=64, help="config3: members in the CPU sample")
+    ap.add_argument("--ens-cpu-steps", type=int, default=20, help="config3: RK12 steps per member in the CPU sample")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.workload == "config3":
+        if args.impl == "reference":
+            run_reference_ensemble(args)
+        else:
+            run_b200_ensemble(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_b200(args)
