@@ -566,7 +566,7 @@ def main():
     ap.add_argument("--ens-systems", type=int, default=512, help="config3: ensemble members")
     ap.add_argument("--ens-frac", type=float, default=0.1, help="config3: fraction of each member's drawn duration")
     ap.add_argument("--ens-cpu-members", type=int, default=64, help="config3: members in the CPU sample")
-    ap.add_argument("--ens-cpu-steps", type=int, default=20, help="config3: RK12 steps per member in the CPU sample")
+    ap.add_argument("--ens-cpu-steps", type=int, default=200, help="config3: RK12 steps per member in the CPU sample")
     args = ap.parse_args()
     if args.workload == "config3":
         if args.impl == "reference":
