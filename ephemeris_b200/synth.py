@@ -353,6 +353,37 @@ def make_config2(seed: int = 2002, n_planet_moons: int = 77, n_dwarfs: int = 5, 
     return sysm
 
 
+def make_ringed_subsystem(seed: int = 6006, n_moons: int = 4, ring_ratio: float = 0.05,
+                          gp_scale: float = 3.0) -> System:
+    """An isolated planetary subsystem for conservation checks: a spinning, oblate, tidally deformable
+    planet with J3..J6 / degree-4 geopotential (scaled by gp_scale), a massive ring annulus of 1.2-2.3
+    radii (ring_ratio of the planet's GM) and n_moons synchronous, tidally locked moons. The subsystem's
+    barycentre sits at 9.5 AU and moves at 9.6 km/s, so its total momenta are far from zero."""
+    rng = np.random.default_rng(seed)
+    sysm = System(bodies=[], delta_t=900.0)
+    gm = 3.7931e16
+    p = Body(name="Planet", sid="P6", GM=gm, R_km=58232.0, inertia=0.22, k2=0.34, k2r=0.34, td=600.0)
+    p.j2 = 0.0163
+    p.c21, p.c22, p.s21, p.s22 = (rng.normal(0, 1e-6) / 2 for _ in range(4))
+    p.x_axis, p.z_axis, p.w = _spin_frame(rng, (0, 0, 1), 26.7 * DEG, 10.6 * 3600.0)
+    p.gp_factor = gp_scale
+    _add_rotational_j2(p)
+    sysm.geopotentials[p.sid] = _gp_model(rng)
+    p.ring_factor = 1.0
+    sysm.rings[p.sid] = [("Annulus", 1.2 * p.R_km, 2.3 * p.R_km, 2.0, ring_ratio * gm)]
+    bodies = [p]
+    for k in range(n_moons):
+        bodies.append(_moon(rng, k + 1, p, p.R_km, _loguniform(rng, 1e-6, 1e-4), (3, 20), 0.02, 1 * DEG, "M",
+                            tidal=True))
+    _barycentric(bodies)
+    bulk_r, bulk_v = np.array([9.5 * AU, 0.0, 0.0]), np.array([0.0, 9.6e3, 0.4e3])
+    for b in bodies:
+        b.r = tuple(np.asarray(b.r) + bulk_r)
+        b.v = tuple(np.asarray(b.v) + bulk_v)
+    sysm.bodies = bodies
+    return sysm
+
+
 def make_small_full(seed: int = 7007, n_bodies: int = 48) -> System:
     """The config2 recipe at reduced counts: every force term present, ~n_bodies bodies."""
     rest = max(n_bodies - 9, 8)
