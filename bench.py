@@ -318,7 +318,6 @@ def run_b200_ensemble(args):
         torch.cuda.set_stream(stream)
         b = Batch(local)
         b.set_stream(stream.cuda_stream)
-        b.set_precision(args.mixed)
         flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
         for _ in range(args.warmup):   # warm-up: every member, 20 steps at most
             b.upload(pls, mds)
@@ -367,9 +366,7 @@ def run_b200_ensemble(args):
             line = {
                 "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None,
-                "dtype": "f64 state, f64 Newtonian, f32 1PN" if args.mixed else "f64 (double-double state)",
-                "data": "synthetic",
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64 (double-double state)", "data": "synthetic",
                 "config": {"workload": f"config3: {len(pls)}-system ensemble, {min(sizes)}-{max(sizes)} bodies "
                                        f"(Newtonian + 1PN), durations {min(ks)}-{max(ks)} RK12 steps "
                                        f"(the 500-20000 draw scaled by {args.ens_frac}), dt=0.05 day",
@@ -567,7 +564,6 @@ def main():
     ap.add_argument("--per-cta", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ens-systems", type=int, default=512, help="config3: ensemble members")
-    ap.add_argument("--mixed", action="store_true", help="config3: 1PN terms in FP32 (mixed precision)")
     ap.add_argument("--ens-frac", type=float, default=0.1, help="config3: fraction of each member's drawn duration")
     ap.add_argument("--ens-cpu-members", type=int, default=64, help="config3: members in the CPU sample")
     ap.add_argument("--ens-cpu-steps", type=int, default=200, help="config3: RK12 steps per member in the CPU sample")
