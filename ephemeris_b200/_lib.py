@@ -56,7 +56,6 @@ SIGNATURES = [
     ("eph_batch_integrate", ctypes.c_int, [_VP, _D, ctypes.POINTER(ctypes.c_int64), _D, _D]),
     ("eph_batch_download", ctypes.c_int, [_VP, ctypes.POINTER(_D)]),
     ("eph_batch_set_stream", ctypes.c_int, [_VP, _VP]),
-    ("eph_batch_set_precision", ctypes.c_int, [_VP, ctypes.c_int]),
     ("eph_batch_info", ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int64)]),
     ("eph_integrate_noalloc", ctypes.c_int, [ctypes.c_int, _VP, ctypes.c_int64, _VP, ctypes.POINTER(EphModels),
                                              ctypes.c_double, ctypes.c_int64, _D, _D]),

@@ -128,51 +128,6 @@ __device__ __forceinline__ void pair_point_b(const BatchView &V, int i, int j, d
     acc[2] += g.z;
 }
 
-// The same pass-B pair with the 1PN terms in FP32 (the mixed-precision form): the separation and its
-// floored square stay FP64 (so the per-pair maxima keep the reference's exact recomputation), the 1PN
-// acceleration (about 1e-8 of the Newtonian one, so FP32's 6e-8 relative rounding is ~1e-15 of the total)
-// is formed in FP32 and accumulated in FP64. The extremal pair of max_influence is chosen on the FP32
-// value, so in a near-tie (within FP32 rounding) a slightly smaller maximum may be reported.
-__device__ __forceinline__ void pair_point_b32(const BatchView &V, int i, int j, double acc[3], PairMax &x) {
-    const v3 r = mk(sep_diff(row(V, BR_R_HI + 0, j), row(V, BR_R_LO + 0, j), row(V, BR_R_HI + 0, i), row(V, BR_R_LO + 0, i)),
-                    sep_diff(row(V, BR_R_HI + 1, j), row(V, BR_R_LO + 1, j), row(V, BR_R_HI + 1, i), row(V, BR_R_LO + 1, i)),
-                    sep_diff(row(V, BR_R_HI + 2, j), row(V, BR_R_LO + 2, j), row(V, BR_R_HI + 2, i), row(V, BR_R_LO + 2, i)));
-    const double GMj = row(V, BR_GM, j);
-    const double q = dot(r, r), sm = row(V, BR_SR2, i) + row(V, BR_SR2, j);
-    const double m = (q < sm) ? sm : q;
-    const float rr = rsqrtf((float)m);
-    const float rr2 = rr * rr;
-    const float tp_dphi = rr * (float)GMj;
-    const float tp_dg = rr2 * tp_dphi;
-    if (x.m_min == x.m_min) x.m_min = (m != m || m < x.m_min) ? m : x.m_min;
-    if (x.tq == x.tq) {
-        const double t = (double)tp_dg;
-        if (t != t) x.tq = t;
-        else if (t > x.tq) { x.tq = t; x.tq_m = m; x.tq_gm = GMj; }
-    }
-    const float rx = (float)r.x, ry = (float)r.y, rz = (float)r.z;
-    const float bjx = (float)row(V, BR_BETA + 0, j), bjy = (float)row(V, BR_BETA + 1, j), bjz = (float)row(V, BR_BETA + 2, j);
-    const float bix = (float)row(V, BR_BETA + 0, i), biy = (float)row(V, BR_BETA + 1, i), biz = (float)row(V, BR_BETA + 2, i);
-    const float rbj = rx * bjx + ry * bjy + rz * bjz;
-    float tp = rbj * rr;
-    tp *= tp;
-    const float nax = (float)row(V, BR_NACC + 0, j), nay = (float)row(V, BR_NACC + 1, j), naz = (float)row(V, BR_NACC + 2, j);
-    const float delta1 = 4 * (float)row(V, BR_PHI, i) + (float)row(V, BR_PHI, j) + (float)row(V, BR_BETA2, i) +
-                         2 * (float)row(V, BR_BETA2, j) - 4 * (bix * bjx + biy * bjy + biz * bjz) +
-                         ((rx * nax + ry * nay + rz * naz) - 3 * tp) / 2;
-    const float bx = bjx - bix, by = bjy - biy, bz = bjz - biz;
-    const float c1 = 7 * tp_dphi / 2, c2 = tp_dg * delta1, c3 = tp_dg * (rbj - (rx * bx + ry * by + rz * bz) * 4);
-    acc[0] += (double)(c1 * nax + c2 * rx + c3 * bx);
-    acc[1] += (double)(c1 * nay + c2 * ry + c3 * by);
-    acc[2] += (double)(c1 * naz + c2 * rz + c3 * bz);
-}
-
-template <bool MIXED>
-__device__ __forceinline__ void pair_b_of(const BatchView &V, int i, int j, double acc[3], PairMax &x) {
-    if (MIXED) pair_point_b32(V, i, j, acc, x);
-    else pair_point_b(V, i, j, acc, x);
-}
-
 // Threads of a pass: with n <= blockDim bodies, G consecutive lanes of a warp share body i and split its j
 // range (G = the largest power of two <= min(32, blockDim / n)); their partial sums are combined by warp
 // shuffles. With more bodies than threads each thread takes whole bodies.
@@ -288,7 +243,6 @@ __device__ __forceinline__ void extremes_of(const PairMax &x, double &inv_r, dou
 }
 
 // pass B and finalisation of the bodies i in [lo, hi) against all n bodies
-template <bool MIXED>
 __device__ void pass_point_b(const BatchView &V, int n, int lo, int hi) {
     const PassMap m = pass_map(lo, hi);
     const double inf = __longlong_as_double(0x7ff0000000000000ll);
@@ -299,10 +253,10 @@ __device__ void pass_point_b(const BatchView &V, int n, int lo, int hi) {
             int j = m.sub;
 #pragma unroll 1
             for (; j + m.G < n; j += 2 * m.G) {
-                if (j != m.i) pair_b_of<MIXED>(V, m.i, j, acc, x);
-                if (j + m.G != m.i) pair_b_of<MIXED>(V, m.i, j + m.G, acc2, x2);
+                if (j != m.i) pair_point_b(V, m.i, j, acc, x);
+                if (j + m.G != m.i) pair_point_b(V, m.i, j + m.G, acc2, x2);
             }
-            if (j < n && j != m.i) pair_b_of<MIXED>(V, m.i, j, acc, x);
+            if (j < n && j != m.i) pair_point_b(V, m.i, j, acc, x);
         }
         double e0, e1, f0, f1;
         extremes_of(x, e0, e1);
@@ -323,10 +277,10 @@ __device__ void pass_point_b(const BatchView &V, int n, int lo, int hi) {
             int j = 0;
 #pragma unroll 1
             for (; j + 1 < n; j += 2) {
-                if (j != i) pair_b_of<MIXED>(V, i, j, acc, x);
-                if (j + 1 != i) pair_b_of<MIXED>(V, i, j + 1, acc2, x2);
+                if (j != i) pair_point_b(V, i, j, acc, x);
+                if (j + 1 != i) pair_point_b(V, i, j + 1, acc2, x2);
             }
-            if (j < n && j != i) pair_b_of<MIXED>(V, i, j, acc, x);
+            if (j < n && j != i) pair_point_b(V, i, j, acc, x);
             double s[5] = {acc[0] + acc2[0], acc[1] + acc2[1], acc[2] + acc2[2], 0, 0};
             double f0, f1;
             extremes_of(x, s[3], s[4]);
@@ -383,7 +337,6 @@ __device__ void broadcast_rows(const BatchView &V, int row0, int nrows, int lo, 
 // owning bodies [lo, hi): every CTA holds all bodies' rows, computes its own bodies' stages and passes,
 // and sends the rows the other CTAs read (positions and GM after the state update, the pass-A outputs
 // after pass A) to their shared memory.
-template <bool MIXED>
 __device__ void integrate_system(const BatchSys &Y, const BatchView &V, bool coop, int rank) {
     const int n = Y.n;
     const int lo = coop ? (int)((long long)rank * n / kCluster) : 0;
@@ -477,7 +430,7 @@ __device__ void integrate_system(const BatchSys &Y, const BatchView &V, bool coo
                 broadcast_rows(V, BR_PHI, BR_BETA2 + 1 - BR_PHI, lo, hi, rank);
                 cg::this_cluster().sync();
             }
-            pass_point_b<MIXED>(V, n, lo, hi);
+            pass_point_b(V, n, lo, hi);
         }
     }
     // store (cuda_rungekutta_kernel_config::save of RungeKutta.cu:124-133); min_distance inverted (mass.cpp:436)
@@ -507,7 +460,6 @@ __device__ void integrate_system(const BatchSys &Y, const BatchView &V, bool coo
 // Persistent CTAs in clusters of kCluster. Jobs [0, n_coop) of the queue (the large systems) are taken a
 // cluster at a time and shared by its CTAs; once a cluster draws a job past them, its CTAs take the
 // remaining jobs one CTA each.
-template <bool MIXED>
 __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kBThreads, 2)
     ensemble_kernel(const BatchSys *sys, const int *order, int n_sys, int n_coop, int *next, int ld) {
     extern __shared__ __align__(16) double bsm[];
@@ -527,7 +479,7 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kBThreads, 2)
             cl.sync();   // read by all before rank 0 may reuse s_job
             if (job >= n_sys) return;
             if (job < n_coop) {
-                integrate_system<MIXED>(sys[order[job]], V, true, rank);
+                integrate_system(sys[order[job]], V, true, rank);
                 continue;
             }
             together = false;
@@ -539,7 +491,7 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kBThreads, 2)
             __syncthreads();
             if (job >= n_sys) return;
         }
-        integrate_system<MIXED>(sys[order[job]], V, false, 0);
+        integrate_system(sys[order[job]], V, false, 0);
     }
 }
 
@@ -555,8 +507,7 @@ cudaError_t batch_setup(int device) {
     cudaError_t e = cudaMemcpyToSymbol(b_rk_hi, hi, sizeof(hi));
     if (e == cudaSuccess) e = cudaMemcpyToSymbol(b_rk_lo, lo, sizeof(lo));
     if (e == cudaSuccess) e = cudaMemcpyToSymbol(b_dtk, dtk, sizeof(dtk));
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(ensemble_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBMaxSmem);
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(ensemble_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBMaxSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(ensemble_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBMaxSmem);
     if (e == cudaSuccess && device >= 0 && device < 64) g_batch_ready[device] = true;
     return e;
 }
@@ -570,7 +521,6 @@ struct eph_batch {
     int device = 0;
     cudaStream_t stream = nullptr;     // work stream (own_stream unless eph_batch_set_stream chose another)
     cudaStream_t own_stream = nullptr;
-    int mixed = 0;                     // 1: 1PN terms of the ensemble kernel in FP32
     std::mutex mu;
     char err[512] = {0};
     int n_sys = 0;
@@ -756,16 +706,13 @@ int eph_batch_integrate(eph_batch *b, const double *dt, const int64_t *n_step, d
         BCK(cudaMemsetAsync(b->d_next, 0, sizeof(int), b->stream), "reset batch queue");
         const size_t smem = ensemble_smem(b->ld);
         int per_sm = 0, sms = 0;
-        BCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ensemble_kernel<false>, kBThreads, smem), "occupancy");
+        BCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ensemble_kernel, kBThreads, smem), "occupancy");
         BCK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device), "SM count");
         // whole clusters; clusters that find no room start when others finish (no CTA waits on another cluster)
         int grid = std::min((int)order.size() * kCluster, std::max(per_sm * sms, kCluster));
         grid = std::max(kCluster, grid / kCluster * kCluster);
-        const int nj = (int)order.size();
-        if (b->mixed)
-            ensemble_kernel<true><<<grid, kBThreads, smem, b->stream>>>(b->d_sys, b->d_order, nj, n_coop, b->d_next, b->ld);
-        else
-            ensemble_kernel<false><<<grid, kBThreads, smem, b->stream>>>(b->d_sys, b->d_order, nj, n_coop, b->d_next, b->ld);
+        ensemble_kernel<<<grid, kBThreads, smem, b->stream>>>(b->d_sys, b->d_order, (int)order.size(), n_coop, b->d_next,
+                                                              b->ld);
         BCK(cudaGetLastError(), "launch ensemble kernel");
         b->launches++;
     }
@@ -831,14 +778,6 @@ int eph_batch_set_stream(eph_batch *b, void *stream) {
     std::lock_guard<std::mutex> lock(b->mu);
     if (!b->own_stream) b->own_stream = b->stream;
     b->stream = stream ? (cudaStream_t)stream : b->own_stream;
-    return EPH_OK;
-}
-
-int eph_batch_set_precision(eph_batch *b, int mode) {
-    if (!b || (mode != EPH_PRECISION_FP64 && mode != EPH_PRECISION_FP32_CORRECTIONS))
-        return bfail(b, EPH_ERR_ARG, "eph_batch_set_precision: unknown mode");
-    std::lock_guard<std::mutex> lock(b->mu);
-    b->mixed = mode == EPH_PRECISION_FP32_CORRECTIONS;
     return EPH_OK;
 }
 

@@ -189,10 +189,6 @@ class Batch:
     def set_stream(self, stream_handle: int | None):
         self._check(self.lib.eph_batch_set_stream(self.h, ctypes.c_void_p(stream_handle or 0)), "batch set_stream")
 
-    def set_precision(self, mixed: bool):
-        """False: FP64 throughout (the reference's arithmetic); True: 1PN terms in FP32."""
-        self._check(self.lib.eph_batch_set_precision(self.h, 1 if mixed else 0), "batch set_precision")
-
     def info(self):
         k, l = ctypes.c_int32(), ctypes.c_int64()
         self._check(self.lib.eph_batch_info(self.h, ctypes.byref(k), ctypes.byref(l)), "batch info")

@@ -121,12 +121,6 @@ int eph_batch_download(eph_batch *b, double *const *planes);
 /* Issue the batch's device work on `stream` (a cudaStream_t of its device; NULL restores its own stream).
  * Calls still return only after their work has finished. */
 int eph_batch_set_stream(eph_batch *b, void *stream);
-/* Arithmetic of the shared ensemble launch: EPH_PRECISION_FP64 (default; the reference's arithmetic) or
- * EPH_PRECISION_FP32_CORRECTIONS (state, Newtonian sums and the RK12 combination in FP64/double-double,
- * the 1PN terms in FP32 accumulated in FP64). No counterpart in the reference. */
-#define EPH_PRECISION_FP64 0
-#define EPH_PRECISION_FP32_CORRECTIONS 1
-int eph_batch_set_precision(eph_batch *b, int mode);
 /* Systems in the shared ensemble launch, and launches issued so far. */
 int eph_batch_info(const eph_batch *b, int32_t *n_ensemble, int64_t *launches);
 

@@ -106,23 +106,3 @@ def test_full_physics_system_in_a_batch(golden, tmp_path):
     c.integrate(dt, 3)
     assert np.array_equal(out[0], c.download())
     assert np.array_equal(out[1], mem[0][0])   # zero steps: untouched
-
-
-def test_mixed_precision_ensemble_error(tmp_path, oracle):
-    """FP32 1PN terms (FP64 state, Newtonian sums and combination): the per-stage acceleration stays within
-    1e-14 and the position after 1000 steps within 1e-12 of the FP64 oracle; the maxima within 1e-6 (their
-    extremal pair is chosen on FP32 values)."""
-    from ephemeris_b200 import Batch
-    mem = _members(tmp_path, [33, 120], seed=3007)
-    steps = [1000, 20]
-    b = Batch(0)
-    b.set_precision(True)
-    b.upload([m[0] for m in mem], [m[1] for m in mem])
-    b.integrate([m[2] for m in mem], steps)
-    for (pl, md, dt), k, out in zip(mem, steps, b.download()):
-        ref = oracle.integrate(pl, _omodels(md), dt, k)[0]
-        assert np.isfinite(out[0:12]).all()
-        assert position_error(out, ref) <= POS_TOL
-        assert accel_error(out, ref) <= ACC_TOL
-        for p in (100, 101):
-            assert rel_err(out[p], ref[p]) <= 1e-6
