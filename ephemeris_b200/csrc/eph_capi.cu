@@ -47,7 +47,17 @@ struct eph_ctx {
     int64_t launches = 0;
     unsigned long long *d_timers = nullptr;   // phase timers of the last launch, when profiling
     int timers_grid = 0;
+    double *d_traj = nullptr;            // stage records for massless particles (caller-owned), or null
+    long long traj_base = 0;
 };
+
+namespace eph {
+// Stage records of the following launches go to d_buf, starting at slot `base` (null: off).
+void ctx_record_stages(eph_ctx *ctx, double *d_buf, long long base) {
+    ctx->d_traj = d_buf;
+    ctx->traj_base = base;
+}
+}  // namespace eph
 
 static int fail(eph_ctx *c, int code, const char *what, cudaError_t e = cudaSuccess) {
     if (c) {
@@ -312,6 +322,8 @@ static int run(eph_ctx *ctx, const StepParams &P) {
     S.bar = ctx->d_bar;
     S.status = ctx->d_status;
     S.timers = nullptr;
+    S.traj = ctx->d_traj;
+    S.traj_base = ctx->traj_base;
     if (ctx->d_timers) {
         if (ctx->timers_grid < ctx->grid) {
             cudaFree(ctx->d_timers);

@@ -13,7 +13,7 @@
 
 namespace eph {
 
-__device__ __noinline__ v3 gp_sum(const double *__restrict__ c_table, int Nz, int Nt, double R, v3 r) {
+static __device__ __noinline__ v3 gp_sum(const double *__restrict__ c_table, int Nz, int Nt, double R, v3 r) {
     double rho2 = r.x * r.x + r.y * r.y;
     double rr2 = 1.0 / (rho2 + r.z * r.z);
     double rho1 = sqrt(rho2);
@@ -147,7 +147,7 @@ __device__ __forceinline__ RingGeom ring_geom(v3 r) {
 
 // Contribution of one signed disk {GsR2, R_R, H_R} (ring.impl:2122-2190). sin and cos of
 // phi = atan2(rz, re - R) are formed from the same two legs instead of from phi.
-__device__ __noinline__ v3 ring_disk_term(const double *__restrict__ disk, double host_R, const RingGeom &g) {
+static __device__ __noinline__ v3 ring_disk_term(const double *__restrict__ disk, double host_R, const RingGeom &g) {
     const double pi = 3.1415926535897932;
     const double GsR2 = __ldg(disk), R_R = __ldg(disk + 1), H_R = __ldg(disk + 2);
     const double re = g.re, re2 = g.re2, rz = g.rz, rz2 = g.rz2, r2 = g.r2;
@@ -215,7 +215,7 @@ __device__ __noinline__ v3 ring_disk_term(const double *__restrict__ disk, doubl
 }
 
 // ring::sum: disks added in order, then the sign flip of the mirrored half-space (ring.impl:2109-2195)
-__device__ __noinline__ v3 ring_sum(const double *__restrict__ disks, int ndisk, double host_R, v3 r) {
+static __device__ __noinline__ v3 ring_sum(const double *__restrict__ disks, int ndisk, double host_R, v3 r) {
     const RingGeom g = ring_geom(r);
     v3 ret = mk(0, 0, 0);
     for (int i = 0; i < ndisk; ++i) ret += ring_disk_term(disks + 3 * i, host_R, g);

@@ -202,6 +202,8 @@ int body(int device, cudaStream_t stream, int n, double *d_planes, const eph_mod
     S.bar = (unsigned *)(scr + kOffWords);
     S.status = I(kOffWords) + 2;
     S.timers = nullptr;
+    S.traj = nullptr;
+    S.traj_base = 0;
     if (n_step < 0) {   // mass.cpp:401-404
         n_step = -n_step;
         dt = -dt;

@@ -1,0 +1,504 @@
+// eph_particles.cu - massless test particles integrated against massive perturbers.
+//
+// A particle feels the perturbers and nothing else, and the perturbers do not feel it, so the two
+// integrations separate: the perturbers run through the single-system kernel (eph_step.cu), which records
+// every stage evaluation of every perturber (position, potential, Newtonian acceleration, velocity/c,
+// harmonics, spin, frames: the TrajField record); then `particle_kernel` integrates each particle on its
+// own thread through the same 25 stage times, reading the perturber records of each stage from shared
+// memory. Per particle and stage (the reference's terms for a point-like body i and perturber j):
+//   pass A  phi_i, a_N,i of mass.impl:38-46 (floored at sR2_j: the particle has no radius)
+//   prepare beta_i = v_i / c, beta_i^2, phi_i / c^2, a_N,i / c^2 (mass.impl:76-80)
+//   pass B  EIH 1PN (mass.impl:82-97) with the perturbers' own prepared values; j's deformation force and
+//           j's Lense-Thirring field on i (mass.impl:99-125, the j-side terms)
+//   fields  geopotential and ring fields of the extended perturbers at i (mass.cpp:358-371; the reaction
+//           on the perturber is GM_i times the field, zero for a massless particle)
+//   final   f_i = (gaccel + daccel) + naccel (mass.cpp:389-396)
+// The RK12 combination and state update are those of RungeKutta.impl:148-186 (gather form: f_j stored per
+// stage, summed in ascending j). The reference has no massless bodies; bodies of negligible mass
+// (GM = 1e-20 m^3/s^2) in one system with the perturbers are its equivalent, and the tests compare with
+// exactly that.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "eph_math.cuh"
+#include "eph_models.cuh"
+#include "eph_rk12_host.h"
+#include "eph_system.cuh"
+#include "../../include/eph_b200.h"
+#include "../../include/eph_planes.h"
+
+namespace eph {
+void ctx_record_stages(eph_ctx *ctx, double *d_buf, long long base);
+}
+
+namespace eph {
+namespace {
+
+constexpr int kPThreads = 256;          // particles per CTA
+constexpr int kPMaxPert = 32;           // perturbers (their stage records live in shared memory)
+constexpr int kPChunk = 400;            // steps per round of perturbers then particles
+constexpr double kCP = 299792458.0;     // src/math/basic_math.h:10,18
+constexpr int kPF = 9;                  // stored values per (particle, stage): velocity dd (hi 3, lo 3), acceleration 3
+
+__constant__ double p_rk_hi[EPH_RK12_NCOEF];
+__constant__ double p_rk_lo[EPH_RK12_NCOEF];
+
+struct PertInfo {
+    int gp, ring;   // model indices, or -1
+    int full;       // its deformation / spin act on others (full-class body)
+    int pad;
+};
+
+struct PartArgs {
+    int n_part, n_pert;
+    long long n_step;
+    double dt;
+    const double *traj;         // [1 + kStages * n_step][n_pert][kTrajRec]
+    int start_accel;            // 1: form f_0 from record slot 0 (first round); 0: f_0 is in the state
+    double *state;              // [15][n_part]: r hi, r lo, v hi, v lo, f
+    double *fstore;             // [gridDim][kStages][kPF][kPThreads]
+    const PertInfo *info;
+    const int *gp_nz, *gp_nt;
+    const double *gp_coef;
+    const int *ring_nd;
+    const double *ring_disk;
+    int *next;                  // particle-block queue
+};
+
+// acceleration of particle (r, v) at the stage whose perturber records are in P
+__device__ __forceinline__ v3 particle_accel(const PartArgs &A, const double *P, const dd r[3], const dd v[3]) {
+    const int np = A.n_pert;
+    const double c2 = kCP * kCP;
+#define PR(j, f) P[(j) * kTrajRec + (f)]
+    // pass A
+    double phi = 0;
+    v3 na = mk(0, 0, 0);
+#pragma unroll 1
+    for (int j = 0; j < np; ++j) {
+        const v3 d = mk(sep_diff(PR(j, TR_R_HI + 0), PR(j, TR_R_LO + 0), r[0].hi, r[0].lo),
+                        sep_diff(PR(j, TR_R_HI + 1), PR(j, TR_R_LO + 1), r[1].hi, r[1].lo),
+                        sep_diff(PR(j, TR_R_HI + 2), PR(j, TR_R_LO + 2), r[2].hi, r[2].lo));
+        const double q = dot(d, d), sm = PR(j, TR_SR2);
+        const double rr = rsqrt((q < sm) ? sm : q);
+        const double tp_dphi = rr * PR(j, TR_GM);
+        const double tp_dg = rr * rr * tp_dphi;
+        phi -= tp_dphi;
+        na += tp_dg * d;
+    }
+    // PREPARE_RELATIVITY
+    const v3 bi = vdiv(mk(dd_val(v[0]), dd_val(v[1]), dd_val(v[2])), kCP);
+    const double beta2 = dot(bi, bi);
+    phi = phi / c2;
+    na = vdiv(na, c2);
+    // pass B: 1PN, and the deformation and Lense-Thirring fields of full-class perturbers
+    v3 ga = mk(0, 0, 0), da = mk(0, 0, 0);
+#pragma unroll 1
+    for (int j = 0; j < np; ++j) {
+        const v3 d = mk(sep_diff(PR(j, TR_R_HI + 0), PR(j, TR_R_LO + 0), r[0].hi, r[0].lo),
+                        sep_diff(PR(j, TR_R_HI + 1), PR(j, TR_R_LO + 1), r[1].hi, r[1].lo),
+                        sep_diff(PR(j, TR_R_HI + 2), PR(j, TR_R_LO + 2), r[2].hi, r[2].lo));
+        const double GMj = PR(j, TR_GM);
+        const double q = dot(d, d), sm = PR(j, TR_SR2);
+        const double rr = rsqrt((q < sm) ? sm : q);
+        const double rr2 = rr * rr, rr3 = rr * rr2;
+        const double tp_dphi = rr * GMj;
+        const double tp_dg = rr2 * tp_dphi;
+        const v3 bj = mk(PR(j, TR_BETA + 0), PR(j, TR_BETA + 1), PR(j, TR_BETA + 2));
+        const double rbj = dot(d, bj);
+        double tp = rbj * rr;
+        tp *= tp;
+        const v3 naj = mk(PR(j, TR_NACC + 0), PR(j, TR_NACC + 1), PR(j, TR_NACC + 2));
+        const double delta1 = 4 * phi + PR(j, TR_PHI) + beta2 + 2 * PR(j, TR_BETA2) - 4 * dot(bi, bj) +
+                              (dot(d, naj) - 3 * tp) / 2;
+        const v3 b = bj - bi;
+        ga += (7 * tp_dphi / 2) * naj + (tp_dg * delta1) * d + (tp_dg * (rbj - dot(d, b) * 4)) * b;
+        if (!A.info[j].full) continue;
+        const m3 Cj = m3{mk(PR(j, TR_CPOT + 0), PR(j, TR_CPOT + 1), PR(j, TR_CPOT + 2)),
+                         mk(PR(j, TR_CPOT + 3), PR(j, TR_CPOT + 4), PR(j, TR_CPOT + 5)),
+                         mk(PR(j, TR_CPOT + 6), PR(j, TR_CPOT + 7), PR(j, TR_CPOT + 8))};
+        const v3 Cjr = mul(Cj, d);
+        v3 dj = (GMj * rr3 * rr2 * PR(j, TR_R2)) * ((dot(d, Cjr) * 5 * rr2) * d - (Cjr + Cjr));
+        const double rcr32 = 2 * GMj / kCP * rr3;
+        const v3 GLj = mk(PR(j, TR_GL + 0), PR(j, TR_GL + 1), PR(j, TR_GL + 2));
+        dj += cross(rcr32 * (GLj - (3 * dot(GLj, d) * rr2) * d), b);
+        da += dj;
+    }
+    // fields of the extended perturbers, r = r_particle - r_host (mass.cpp:184,198)
+#pragma unroll 1
+    for (int j = 0; j < np; ++j) {
+        const int gp = A.info[j].gp, rg = A.info[j].ring;
+        if (gp < 0 && rg < 0) continue;
+        const v3 re = mk(dd_diff(r[0].hi, r[0].lo, PR(j, TR_R_HI + 0), PR(j, TR_R_LO + 0)),
+                         dd_diff(r[1].hi, r[1].lo, PR(j, TR_R_HI + 1), PR(j, TR_R_LO + 1)),
+                         dd_diff(r[2].hi, r[2].lo, PR(j, TR_R_HI + 2), PR(j, TR_R_LO + 2)));
+        if (gp >= 0) {
+            const m3 f = m3{mk(PR(j, TR_FRAME + 0), PR(j, TR_FRAME + 1), PR(j, TR_FRAME + 2)),
+                            mk(PR(j, TR_FRAME + 3), PR(j, TR_FRAME + 4), PR(j, TR_FRAME + 5)),
+                            mk(PR(j, TR_FRAME + 6), PR(j, TR_FRAME + 7), PR(j, TR_FRAME + 8))};
+            const v3 an = toworld(f, gp_sum(A.gp_coef + (size_t)gp * EPH_GP_TABLE_SIZE, A.gp_nz[gp], A.gp_nt[gp],
+                                            PR(j, TR_RADIUS), tolocal(f, re)));
+            da += PR(j, TR_GM) * an;
+        }
+        if (rg >= 0) {
+            const m3 f = m3{mk(PR(j, TR_RFRAME + 0), PR(j, TR_RFRAME + 1), PR(j, TR_RFRAME + 2)),
+                            mk(PR(j, TR_RFRAME + 3), PR(j, TR_RFRAME + 4), PR(j, TR_RFRAME + 5)),
+                            mk(PR(j, TR_RFRAME + 6), PR(j, TR_RFRAME + 7), PR(j, TR_RFRAME + 8))};
+            const v3 an = toworld(f, ring_sum(A.ring_disk + (size_t)rg * EPH_RING_MAX_DISKS * 3, A.ring_nd[rg],
+                                              PR(j, TR_RADIUS), tolocal(f, re)));
+            da += PR(j, TR_GM) * an;
+        }
+    }
+#undef PR
+    return (ga + da) + c2 * na;
+}
+
+__device__ __forceinline__ void load_records(const PartArgs &A, double *P, long long slot) {
+    const double *src = A.traj + (size_t)slot * A.n_pert * kTrajRec;
+    __syncthreads();   // everyone is done with the previous stage's records
+    for (int q = threadIdx.x; q < A.n_pert * kTrajRec; q += blockDim.x) P[q] = src[q];
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kPThreads, 2) particle_kernel(PartArgs A) {
+    __shared__ double P[kPMaxPert * kTrajRec];
+    __shared__ int s_blk;
+    double *F = A.fstore + (size_t)blockIdx.x * kStages * kPF * kPThreads + threadIdx.x;   // [stage][value] stride kPThreads
+    const int nb = (A.n_part + kPThreads - 1) / kPThreads;
+#pragma unroll 1
+    for (;;) {
+        if (threadIdx.x == 0) s_blk = atomicAdd(A.next, 1);
+        __syncthreads();
+        const int blk = s_blk;
+        __syncthreads();
+        if (blk >= nb) return;
+        const int ip = blk * kPThreads + threadIdx.x;
+        const bool live = ip < A.n_part;
+        const int n = A.n_part;
+        dd r[3], v[3];
+        v3 fa = mk(0, 0, 0);
+        for (int c = 0; c < 3; ++c) {
+            r[c] = live ? dd{A.state[(0 + c) * n + ip], A.state[(3 + c) * n + ip]} : dd_make(1e30);
+            v[c] = live ? dd{A.state[(6 + c) * n + ip], A.state[(9 + c) * n + ip]} : dd_make(0);
+        }
+        if (live) fa = mk(A.state[12 * n + ip], A.state[13 * n + ip], A.state[14 * n + ip]);
+        if (A.start_accel) {   // f_0 at the start state (the reference's loader runs accel(), mass_loader.cpp:555)
+            load_records(A, P, 0);
+            if (live) fa = particle_accel(A, P, r, v);
+        }
+        const double dt = A.dt;
+        const dd ddt = dd_make(dt);
+#pragma unroll 1
+        for (long long step = 0; step < A.n_step; ++step) {
+            dd r0[3], v0[3];
+            for (int c = 0; c < 3; ++c) { r0[c] = r[c]; v0[c] = v[c]; }
+#pragma unroll 1
+            for (int s = 0; s < kStages; ++s) {
+                double *Fs = F + (size_t)s * kPF * kPThreads;
+                for (int c = 0; c < 3; ++c) {
+                    Fs[(size_t)c * kPThreads] = v[c].hi;
+                    Fs[(size_t)(3 + c) * kPThreads] = v[c].lo;
+                }
+                Fs[(size_t)6 * kPThreads] = fa.x;
+                Fs[(size_t)7 * kPThreads] = fa.y;
+                Fs[(size_t)8 * kPThreads] = fa.z;
+                // state of stage k: sum_j a_kj f_j in ascending j, zero coefficients skipped
+                const int k = s + 1, ci0 = k * (k - 1) / 2;
+                dd sv[3] = {dd_make(0), dd_make(0), dd_make(0)};
+                double sa[3] = {0.0, 0.0, 0.0};
+#pragma unroll 4
+                for (int j = 0; j < k; ++j) {
+                    const dd a = dd{p_rk_hi[ci0 + j], p_rk_lo[ci0 + j]};
+                    if (a.hi == 0) continue;
+                    const double fac = dd_val(a);
+                    const double *Fj = F + (size_t)j * kPF * kPThreads;
+                    for (int c = 0; c < 3; ++c) {
+                        sv[c] = dd_add(sv[c], dd_mul(a, dd{Fj[(size_t)c * kPThreads], Fj[(size_t)(3 + c) * kPThreads]}));
+                        sa[c] = __dadd_rn(sa[c], __dmul_rn(fac, Fj[(size_t)(6 + c) * kPThreads]));
+                    }
+                }
+                for (int c = 0; c < 3; ++c) {
+                    r[c] = dd_add(r0[c], dd_mul(ddt, sv[c]));
+                    v[c] = dd_add(v0[c], dd_make(dt * sa[c]));
+                }
+                load_records(A, P, 1 + step * kStages + s);
+                if (live) fa = particle_accel(A, P, r, v);
+            }
+        }
+        if (live) {
+            for (int c = 0; c < 3; ++c) {
+                A.state[(0 + c) * n + ip] = r[c].hi;
+                A.state[(3 + c) * n + ip] = r[c].lo;
+                A.state[(6 + c) * n + ip] = v[c].hi;
+                A.state[(9 + c) * n + ip] = v[c].lo;
+            }
+            A.state[12 * n + ip] = fa.x;
+            A.state[13 * n + ip] = fa.y;
+            A.state[14 * n + ip] = fa.z;
+        }
+    }
+}
+
+bool g_part_ready[64];
+cudaError_t particles_setup(int device) {
+    if (device >= 0 && device < 64 && g_part_ready[device]) return cudaSuccess;
+    double hi[EPH_RK12_NCOEF], lo[EPH_RK12_NCOEF], dtk[kStages + 1];
+    rk12_expand(hi, lo, dtk);
+    cudaError_t e = cudaMemcpyToSymbol(p_rk_hi, hi, sizeof(hi));
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(p_rk_lo, lo, sizeof(lo));
+    if (e == cudaSuccess && device >= 0 && device < 64) g_part_ready[device] = true;
+    return e;
+}
+
+}  // namespace
+}  // namespace eph
+
+using namespace eph;
+
+struct eph_particles {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::mutex mu;
+    char err[512] = {0};
+    eph_ctx *ctx = nullptr;            // the perturbers
+    eph_ctx *ctx0 = nullptr;           // scratch context for the start-state records
+    int64_t n_pert = 0, n_part = 0;
+    std::vector<double> h_pert;        // perturber planes as uploaded (for the start-state records)
+    std::vector<int32_t> gp_nz, gp_nt, ring_nd;
+    std::vector<double> gp_coef, ring_param, ring_disk;
+    bool started = false;              // f_0 of the particles formed
+    double *d_state = nullptr, *d_traj = nullptr, *d_fstore = nullptr;
+    int *d_gp_nz = nullptr, *d_gp_nt = nullptr, *d_ring_nd = nullptr, *d_next = nullptr;
+    double *d_gp_coef = nullptr, *d_ring_disk = nullptr;
+    PertInfo *d_info = nullptr;
+    size_t traj_cap = 0;
+    int grid = 0;
+};
+
+static int pfail(eph_particles *p, int code, const char *what, cudaError_t e = cudaSuccess) {
+    if (p) {
+        if (e != cudaSuccess) snprintf(p->err, sizeof(p->err), "%s: %s", what, cudaGetErrorString(e));
+        else snprintf(p->err, sizeof(p->err), "%s", what);
+    }
+    return code;
+}
+#define PCK(call, what)                                                                                     \
+    do {                                                                                                    \
+        cudaError_t e_ = (call);                                                                            \
+        if (e_ != cudaSuccess) return pfail(p, e_ == cudaErrorMemoryAllocation ? EPH_ERR_OOM : EPH_ERR_CUDA, what, e_); \
+    } while (0)
+
+static void part_free(eph_particles *p) {
+    for (void *q : {(void *)p->d_state, (void *)p->d_traj, (void *)p->d_fstore, (void *)p->d_gp_nz, (void *)p->d_gp_nt,
+                    (void *)p->d_ring_nd, (void *)p->d_next, (void *)p->d_gp_coef, (void *)p->d_ring_disk,
+                    (void *)p->d_info})
+        if (q) cudaFree(q);
+    p->d_state = p->d_traj = p->d_fstore = nullptr;
+    p->d_gp_nz = p->d_gp_nt = p->d_ring_nd = p->d_next = nullptr;
+    p->d_gp_coef = p->d_ring_disk = nullptr;
+    p->d_info = nullptr;
+    p->traj_cap = 0;
+}
+
+// t += d in double-double (mass.cpp:441)
+static void dd_advance(double *hi, double *lo, double d) {
+    const double a = *hi, s = a + d, t = s - a;
+    double e = (a - (s - t)) + (d - t);
+    e = e + (*lo + 0.0);
+    const double h = s + e;
+    *lo = e - (h - s);
+    *hi = h;
+}
+
+extern "C" {
+
+int eph_particles_create(int device, eph_particles **out) {
+    if (!out) return EPH_ERR_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) return EPH_ERR_ARG;
+    eph_particles *p = new eph_particles();
+    p->device = device;
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        particles_setup(device) != cudaSuccess || eph_ctx_create(device, &p->ctx) != EPH_OK ||
+        eph_ctx_create(device, &p->ctx0) != EPH_OK) {
+        if (p->ctx) eph_ctx_destroy(p->ctx);
+        delete p;
+        return EPH_ERR_CUDA;
+    }
+    *out = p;
+    return EPH_OK;
+}
+
+int eph_particles_destroy(eph_particles *p) {
+    if (!p) return EPH_ERR_ARG;
+    cudaSetDevice(p->device);
+    part_free(p);
+    if (p->ctx) eph_ctx_destroy(p->ctx);
+    if (p->ctx0) eph_ctx_destroy(p->ctx0);
+    if (p->stream) cudaStreamDestroy(p->stream);
+    delete p;
+    return EPH_OK;
+}
+
+const char *eph_particles_last_error(const eph_particles *p) { return p ? p->err : "null particle set"; }
+
+int eph_particles_upload(eph_particles *p, int64_t n_pert, const double *pert_planes, const eph_models *models,
+                         int64_t n_part, const double *part_state) {
+    if (!p || n_pert <= 0 || n_pert > kPMaxPert || !pert_planes || n_part <= 0 || n_part > (1ll << 31) / 16 || !part_state)
+        return pfail(p, n_pert > kPMaxPert ? EPH_ERR_LIMIT : EPH_ERR_ARG, "eph_particles_upload: bad arguments");
+    std::lock_guard<std::mutex> lock(p->mu);
+    PCK(cudaSetDevice(p->device), "cudaSetDevice");
+    int rc = eph_upload_system(p->ctx, n_pert, pert_planes, models);
+    if (rc) return pfail(p, rc, eph_last_error(p->ctx));
+    part_free(p);
+    p->n_pert = n_pert;
+    p->n_part = n_part;
+    p->h_pert.assign(pert_planes, pert_planes + (size_t)EPH_NPLANES * n_pert);
+    const int n_gp = models ? models->n_gp : 0, n_ring = models ? models->n_ring : 0;
+    p->gp_nz.assign(n_gp ? models->gp_nz : nullptr, n_gp ? models->gp_nz + n_gp : nullptr);
+    p->gp_nt.assign(n_gp ? models->gp_nt : nullptr, n_gp ? models->gp_nt + n_gp : nullptr);
+    p->gp_coef.assign(n_gp ? models->gp_coef : nullptr, n_gp ? models->gp_coef + (size_t)n_gp * EPH_GP_TABLE_SIZE : nullptr);
+    p->ring_nd.assign(n_ring ? models->ring_ndisk : nullptr, n_ring ? models->ring_ndisk + n_ring : nullptr);
+    p->ring_param.assign(n_ring ? models->ring_param : nullptr, n_ring ? models->ring_param + (size_t)n_ring * 4 : nullptr);
+    p->ring_disk.assign(n_ring ? models->ring_disk : nullptr,
+                        n_ring ? models->ring_disk + (size_t)n_ring * EPH_RING_MAX_DISKS * 3 : nullptr);
+    std::vector<PertInfo> info(n_pert);
+    for (int j = 0; j < n_pert; ++j) {
+        auto P = [&](int q) { return pert_planes[(size_t)q * n_pert + j]; };
+        info[j].gp = (int)P(EPH_P_GP_INDEX);
+        info[j].ring = (int)P(EPH_P_RING_INDEX);
+        bool full = P(EPH_P_K2) != 0 || P(EPH_P_K2R) != 0 || P(EPH_P_DJ2) != 0 || P(EPH_P_LUM) != 0 ||
+                    P(EPH_P_RR2G_4C) != 0 || info[j].gp >= 0 || info[j].ring >= 0;
+        for (int q = 0; q < 9; ++q) full = full || P(EPH_P_C_STATIC + q) != 0;
+        for (int c = 0; c < 3; ++c) full = full || P(EPH_P_W + c) != 0 || P(EPH_P_GL_HI + c) != 0 || P(EPH_P_GL_LO + c) != 0;
+        info[j].full = full;
+        info[j].pad = 0;
+    }
+    // particle state: r hi, r lo, v hi, v lo as given, then f (formed at the first integration)
+    std::vector<double> st((size_t)15 * n_part, 0.0);
+    std::copy(part_state, part_state + (size_t)12 * n_part, st.begin());
+    int per_sm = 0, sms = 0;
+    PCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, particle_kernel, kPThreads, 0), "occupancy");
+    PCK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p->device), "SM count");
+    const int64_t nblk = (n_part + kPThreads - 1) / kPThreads;
+    p->grid = (int)std::max<int64_t>(1, std::min<int64_t>(nblk, (int64_t)per_sm * sms));
+    PCK(cudaMalloc(&p->d_state, st.size() * sizeof(double)), "cudaMalloc(particles)");
+    PCK(cudaMalloc(&p->d_fstore, (size_t)p->grid * kStages * kPF * kPThreads * sizeof(double)), "cudaMalloc(stage store)");
+    PCK(cudaMalloc(&p->d_info, n_pert * sizeof(PertInfo)), "cudaMalloc(perturbers)");
+    PCK(cudaMalloc(&p->d_next, sizeof(int)), "cudaMalloc(queue)");
+    PCK(cudaMalloc(&p->d_gp_nz, std::max(n_gp, 1) * sizeof(int)), "cudaMalloc(gp)");
+    PCK(cudaMalloc(&p->d_gp_nt, std::max(n_gp, 1) * sizeof(int)), "cudaMalloc(gp)");
+    PCK(cudaMalloc(&p->d_gp_coef, (size_t)std::max(n_gp, 1) * EPH_GP_TABLE_SIZE * sizeof(double)), "cudaMalloc(gp)");
+    PCK(cudaMalloc(&p->d_ring_nd, std::max(n_ring, 1) * sizeof(int)), "cudaMalloc(ring)");
+    PCK(cudaMalloc(&p->d_ring_disk, (size_t)std::max(n_ring, 1) * EPH_RING_MAX_DISKS * 3 * sizeof(double)), "cudaMalloc(ring)");
+    PCK(cudaMemcpy(p->d_state, st.data(), st.size() * sizeof(double), cudaMemcpyHostToDevice), "upload particles");
+    PCK(cudaMemcpy(p->d_info, info.data(), n_pert * sizeof(PertInfo), cudaMemcpyHostToDevice), "upload perturbers");
+    if (n_gp) {
+        PCK(cudaMemcpy(p->d_gp_nz, p->gp_nz.data(), n_gp * sizeof(int), cudaMemcpyHostToDevice), "upload gp");
+        PCK(cudaMemcpy(p->d_gp_nt, p->gp_nt.data(), n_gp * sizeof(int), cudaMemcpyHostToDevice), "upload gp");
+        PCK(cudaMemcpy(p->d_gp_coef, p->gp_coef.data(), p->gp_coef.size() * sizeof(double), cudaMemcpyHostToDevice), "upload gp");
+    }
+    if (n_ring) {
+        PCK(cudaMemcpy(p->d_ring_nd, p->ring_nd.data(), n_ring * sizeof(int), cudaMemcpyHostToDevice), "upload ring");
+        PCK(cudaMemcpy(p->d_ring_disk, p->ring_disk.data(), p->ring_disk.size() * sizeof(double), cudaMemcpyHostToDevice),
+            "upload ring");
+    }
+    p->started = false;
+    return EPH_OK;
+}
+
+int eph_particles_integrate(eph_particles *p, double dt, int64_t n_step, double *t_eph_hi, double *t_eph_lo) {
+    if (!p || !t_eph_hi || !t_eph_lo) return pfail(p, EPH_ERR_ARG, "eph_particles_integrate: bad arguments");
+    std::lock_guard<std::mutex> lock(p->mu);
+    if (!p->n_part) return pfail(p, EPH_ERR_STATE, "no particles uploaded");
+    if (n_step == 0) return EPH_OK;
+    if (n_step < 0) {   // mass.cpp:401-404
+        n_step = -n_step;
+        dt = -dt;
+    }
+    PCK(cudaSetDevice(p->device), "cudaSetDevice");
+    const size_t rec = (size_t)p->n_pert * kTrajRec;
+    const size_t need = (size_t)(1 + kStages * std::min<int64_t>(n_step, kPChunk)) * rec;
+    if (need > p->traj_cap) {
+        if (p->d_traj) cudaFree(p->d_traj);
+        p->d_traj = nullptr;
+        PCK(cudaMalloc(&p->d_traj, need * sizeof(double)), "cudaMalloc(stage records)");
+        p->traj_cap = need;
+    }
+    int rc;
+    if (!p->started) {
+        // the perturbers' records at the start state (slot 0), from a scratch copy so that their own
+        // integration starts exactly from the uploaded state
+        eph_models m{};
+        m.n_gp = (int32_t)p->gp_nz.size();
+        m.gp_nz = p->gp_nz.data(); m.gp_nt = p->gp_nt.data(); m.gp_coef = p->gp_coef.data();
+        m.n_ring = (int32_t)p->ring_nd.size();
+        m.ring_ndisk = p->ring_nd.data(); m.ring_param = p->ring_param.data(); m.ring_disk = p->ring_disk.data();
+        rc = eph_upload_system(p->ctx0, p->n_pert, p->h_pert.data(), &m);
+        ctx_record_stages(p->ctx0, p->d_traj, 0);
+        if (!rc) rc = eph_accel(p->ctx0);
+        ctx_record_stages(p->ctx0, nullptr, 0);
+        if (rc) return pfail(p, rc, eph_last_error(p->ctx0));
+    }
+    // msystem::integrate: maxima reset before, min_distance inverted after (mass.cpp:406,436)
+    double *d_pl = nullptr;
+    eph_device_planes(p->ctx, &d_pl);
+    PCK(cudaMemset(d_pl + (size_t)EPH_P_MIN_DISTANCE * p->n_pert, 0, 2 * p->n_pert * sizeof(double)), "reset maxima");
+    for (int64_t done = 0; done < n_step;) {
+        const int64_t c = std::min<int64_t>(n_step - done, kPChunk);
+        ctx_record_stages(p->ctx, p->d_traj, 1);
+        rc = eph_rk12(p->ctx, dt, c, *t_eph_hi, *t_eph_lo);
+        ctx_record_stages(p->ctx, nullptr, 0);
+        if (rc) return pfail(p, rc, eph_last_error(p->ctx));
+        PartArgs A;
+        A.n_part = (int)p->n_part;
+        A.n_pert = (int)p->n_pert;
+        A.n_step = c;
+        A.dt = dt;
+        A.traj = p->d_traj;
+        A.start_accel = p->started ? 0 : 1;
+        A.state = p->d_state;
+        A.fstore = p->d_fstore;
+        A.info = p->d_info;
+        A.gp_nz = p->d_gp_nz; A.gp_nt = p->d_gp_nt; A.gp_coef = p->d_gp_coef;
+        A.ring_nd = p->d_ring_nd; A.ring_disk = p->d_ring_disk;
+        A.next = p->d_next;
+        PCK(cudaMemsetAsync(p->d_next, 0, sizeof(int), p->stream), "reset queue");
+        particle_kernel<<<p->grid, kPThreads, 0, p->stream>>>(A);
+        PCK(cudaGetLastError(), "launch particle kernel");
+        PCK(cudaStreamSynchronize(p->stream), "particle kernel");
+        p->started = true;
+        dd_advance(t_eph_hi, t_eph_lo, dt * (double)c);
+        done += c;
+    }
+    std::vector<double> md(p->n_pert);
+    PCK(cudaMemcpy(md.data(), d_pl + (size_t)EPH_P_MIN_DISTANCE * p->n_pert, p->n_pert * sizeof(double),
+                   cudaMemcpyDeviceToHost), "maxima");
+    for (auto &x : md) x = 1 / x;
+    PCK(cudaMemcpy(d_pl + (size_t)EPH_P_MIN_DISTANCE * p->n_pert, md.data(), p->n_pert * sizeof(double),
+                   cudaMemcpyHostToDevice), "maxima");
+    return EPH_OK;
+}
+
+int eph_particles_download(eph_particles *p, double *pert_planes, double *part_state) {
+    if (!p) return EPH_ERR_ARG;
+    std::lock_guard<std::mutex> lock(p->mu);
+    if (!p->n_part) return pfail(p, EPH_ERR_STATE, "no particles uploaded");
+    PCK(cudaSetDevice(p->device), "cudaSetDevice");
+    if (pert_planes) {
+        const int rc = eph_download_system(p->ctx, pert_planes);
+        if (rc) return pfail(p, rc, eph_last_error(p->ctx));
+    }
+    if (part_state)
+        PCK(cudaMemcpy(part_state, p->d_state, (size_t)12 * p->n_part * sizeof(double), cudaMemcpyDeviceToHost),
+            "download particles");
+    return EPH_OK;
+}
+
+}  // extern "C"

@@ -86,6 +86,7 @@ struct Scratch {
     unsigned long long t_last, t_phase[kPhases];
     unsigned long long mbar;          // mbarrier of the tile copies
     unsigned long long bar_target;    // grid-barrier arrivals that complete the next barrier
+    long long traj_slot;              // stage-record slot of the current stage evaluation
     int flag, pad;
 };
 
@@ -862,6 +863,30 @@ __device__ void ext_fields(const SysDev &S, const Own *own, int nb, int buf, Scr
     }
 }
 
+// The stage record of owned body o for massless particles (TrajField layout), in the caller's body order.
+__device__ __noinline__ void record_body(const SysDev &S, const Own &o, long long slot) {
+    double *t = S.traj + ((size_t)slot * S.n + o.orig) * kTrajRec;
+    for (int c = 0; c < 3; ++c) {
+        t[TR_R_HI + c] = o.r[c].hi;
+        t[TR_R_LO + c] = o.r[c].lo;
+        t[TR_NACC + c] = o.nacc[c];
+        t[TR_BETA + c] = o.beta[c];
+    }
+    t[TR_GM] = o.GM;
+    t[TR_PHI] = o.phi;
+    t[TR_BETA2] = o.beta2;
+    for (int q = 0; q < 9; ++q) t[TR_CPOT + q] = o.C[q];
+    t[TR_R2] = o.R2;
+    const v3 gl = fast3(o.GL);
+    t[TR_GL + 0] = gl.x; t[TR_GL + 1] = gl.y; t[TR_GL + 2] = gl.z;
+    for (int q = 0; q < 9; ++q) t[TR_FRAME + q] = dd_val(o.s[q]);
+    t[TR_RADIUS] = o.R;
+    t[TR_SR2] = o.sR2;
+    double rf[9];
+    stm(rf, ring_frame(gl));
+    for (int q = 0; q < 9; ++q) t[TR_RFRAME + q] = o.ring >= 0 ? rf[q] : 0.0;
+}
+
 __device__ bool pass_a(const SysDev &S, Own *own, int nb, int buf, bool deform_only, Scratch &sc, TileState &ts,
                        double *tile) {
     const int ld = S.ld;
@@ -936,6 +961,7 @@ __device__ bool pass_a(const SysDev &S, Own *own, int nb, int buf, bool deform_o
         for (int q = 0; q < 9; ++q) aux[(AUX_CPOT + q) * ld + i] = o.C[q];
         // a non-finite G*L was replaced by GI*w: republish it for pass B
         if (o.gl_fixed) publish_body(S, o, buf);
+        if (S.traj) record_body(S, o, sc.traj_slot);
     }
     __syncthreads();
     mark(S, sc, PH_A_UPDATE);
@@ -1344,6 +1370,7 @@ __global__ void __launch_bounds__(kThreads, 1) step_kernel(SysDev S, StepParams 
 
     if (P.mode == MODE_DEFORM || P.mode == MODE_ACCEL) {
         if (!sync()) return;
+        if (threadIdx.x == 0) sc.traj_slot = S.traj_base;
         if (!pass_a(S, own, nb, 0, P.mode == MODE_DEFORM, sc, ts, tile)) return;
         if (P.mode == MODE_ACCEL) {
             if (!sync()) return;
@@ -1367,6 +1394,7 @@ __global__ void __launch_bounds__(kThreads, 1) step_kernel(SysDev S, StepParams 
             mark(S, sc, PH_RK);
             buf ^= 1;
             if (!sync()) return;
+            if (threadIdx.x == 0) sc.traj_slot = S.traj_base + step * kStages + s;
             if (!pass_a(S, own, nb, buf, false, sc, ts, tile)) return;
             if (!sync()) return;
             if (!pass_b(S, own, nb, buf, sc, ts, tile)) return;

@@ -78,7 +78,15 @@ struct SysDev {
     unsigned int *bar;        // grid barrier: one 64-bit arrival counter (two words, 8-byte aligned), zeroed per launch
     int *status;              // device status word (0 = ok)
     unsigned long long *timers;   // optional [grid][kPhases] nanoseconds per phase (profiling), or null
+    double *traj;             // optional stage records [slot][n][kTrajRec] (massless-particle integration), or null
+    long long traj_base;      // slot of this launch's first stage evaluation
 };
+
+// One stage record of a body (written after pass A, caller's body order): what a massless particle's
+// stage evaluation reads of the massive bodies.
+enum TrajField { TR_R_HI = 0, TR_R_LO = 3, TR_GM = 6, TR_PHI = 7, TR_NACC = 8, TR_BETA = 11, TR_BETA2 = 14,
+                 TR_CPOT = 15, TR_R2 = 24, TR_GL = 25, TR_FRAME = 28, TR_RADIUS = 37, TR_SR2 = 38, TR_RFRAME = 39,
+                 kTrajRec = 48 };
 
 // phases of a stage evaluation, for the optional per-CTA phase timers
 enum Phase { PH_IO = 0, PH_RK = 1, PH_BARRIER = 2, PH_A_SWEEP = 3, PH_A_UPDATE = 4, PH_B_SWEEP = 5,

@@ -195,6 +195,55 @@ class Batch:
         return k.value, l.value
 
 
+class Particles:
+    """Massless test particles against perturbers (eph_particles_* of include/eph_b200.h)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load_library()
+        h = ctypes.c_void_p()
+        check(self.lib.eph_particles_create(device, ctypes.byref(h)), None, "eph_particles_create")
+        self.h = h
+        self.n_pert = self.n_part = 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.eph_particles_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def _check(self, rc, what):
+        if rc:
+            from ._lib import EphError
+            raise EphError(rc, f"{what}: {self.lib.eph_particles_last_error(self.h).decode()}")
+
+    def upload(self, pert_planes: np.ndarray, models, particles: np.ndarray):
+        """particles: [12][n] (position hi, lo; velocity hi, lo) or [6][n] (position, velocity)."""
+        pl = np.ascontiguousarray(pert_planes, np.float64)
+        pa = np.asarray(particles, np.float64)
+        if pa.shape[0] == 6:
+            z = np.zeros((3, pa.shape[1]))
+            pa = np.concatenate([pa[0:3], z, pa[3:6], z])
+        pa = np.ascontiguousarray(pa)
+        self._models = models or Models.empty()
+        st = self._models.struct()
+        self._check(self.lib.eph_particles_upload(self.h, pl.shape[1], _dptr(pl), ctypes.byref(st), pa.shape[1], _dptr(pa)),
+                    "particles upload")
+        self.n_pert, self.n_part = pl.shape[1], pa.shape[1]
+
+    def integrate(self, dt: float, n_step: int, t_eph=(0.0, 0.0)):
+        hi, lo = ctypes.c_double(t_eph[0]), ctypes.c_double(t_eph[1])
+        self._check(self.lib.eph_particles_integrate(self.h, dt, n_step, ctypes.byref(hi), ctypes.byref(lo)),
+                    "particles integrate")
+        return hi.value, lo.value
+
+    def download(self):
+        pl = np.empty((NPLANES, self.n_pert))
+        pa = np.empty((12, self.n_part))
+        self._check(self.lib.eph_particles_download(self.h, _dptr(pl), _dptr(pa)), "particles download")
+        return pl, pa
+
+
 class MSystem:
     """A system of bodies loaded from the reference's initials files and integrated on the GPU."""
 

@@ -384,6 +384,58 @@ def make_ringed_subsystem(seed: int = 6006, n_moons: int = 4, ring_ratio: float 
     return sysm
 
 
+def make_config5(seed: int = 5005, n_particles: int = 2_000_000, j2: float = 2e-4):
+    """Massless test particles against 9 perturbers: a star with J2 (static) and J3-J4 (zonal geopotential)
+    and 8 planets of the config1 recipe (Newtonian + 1PN). Particles: a ~ U(1.5, 50) AU, e ~ U(0, 0.3),
+    i ~ U(0, 20 deg), angles uniform, on heliocentric Kepler orbits shifted to the perturbers' barycentre.
+    Returns (perturber System, particles [6][n]: x, y, z, vx, vy, vz)."""
+    rng = np.random.default_rng(seed)
+    star = Body(name="Star", sid="S0", GM=GM_SUN, R_km=6.96e5, inertia=0.07)
+    star.j2 = j2
+    star.gp_factor = 1.0
+    bodies = [star]
+    for k in range(8):
+        gm = _loguniform(rng, 1e-9, 1e-3) * GM_SUN
+        a = _loguniform(rng, 0.4, 30.0) * AU
+        r, v = _kepler_state(GM_SUN + gm, a, rng.uniform(0, 0.1), rng.uniform(0, 3 * DEG),
+                             rng.uniform(0, 2 * math.pi), rng.uniform(0, 2 * math.pi), rng.uniform(0, 2 * math.pi))
+        bodies.append(Body(name=f"Planet{k + 1}", sid=f"P{k + 1}", GM=gm, R_km=_radius_km(gm), r=tuple(r), v=tuple(v)))
+    _barycentric(bodies)
+    sysm = System(bodies=bodies, delta_t=43200.0)
+    sysm.geopotentials["S0"] = (4, 0, [(n, 0, rng.normal(0, 1e-6) / n, 0.0) for n in (3, 4)])
+    n = n_particles
+    a = rng.uniform(1.5, 50.0, n) * AU
+    e = rng.uniform(0.0, 0.3, n)
+    inc = rng.uniform(0.0, 20 * DEG, n)
+    node, argp, M = (rng.uniform(0, 2 * math.pi, n) for _ in range(3))
+    # Kepler's equation by Newton iteration, vectorised
+    E = M.copy()
+    for _ in range(30):
+        E = E - (E - e * np.sin(E) - M) / (1 - e * np.cos(E))
+    cE, sE = np.cos(E), np.sin(E)
+    px, py = a * (cE - e), a * np.sqrt(1 - e * e) * sE
+    nmot = np.sqrt(GM_SUN / a ** 3)
+    vx, vy = -a * nmot * sE / (1 - e * cE), a * nmot * np.sqrt(1 - e * e) * cE / (1 - e * cE)
+    cO, sO, cw, sw, ci, si = np.cos(node), np.sin(node), np.cos(argp), np.sin(argp), np.cos(inc), np.sin(inc)
+    P = np.array([cO * cw - sO * sw * ci, sO * cw + cO * sw * ci, sw * si])
+    Q = np.array([-cO * sw - sO * cw * ci, -sO * sw + cO * cw * ci, cw * si])
+    rs, vs = np.asarray(star.r), np.asarray(star.v)
+    pos = px * P + py * Q + rs[:, None]
+    vel = vx * P + vy * Q + vs[:, None]
+    return sysm, np.concatenate([pos, vel]).astype(np.float64)
+
+
+def with_test_bodies(sysm: System, particles: np.ndarray, gm: float = 1e-20) -> System:
+    """The perturbers plus the particles as bodies of negligible mass (the reference's equivalent of
+    massless particles), appended after the perturbers."""
+    bodies = list(sysm.bodies)
+    for k in range(particles.shape[1]):
+        bodies.append(Body(name=f"T{k}", sid=f"T{k}", GM=gm, R_km=1e-3, inertia=0.4,
+                           r=tuple(particles[0:3, k]), v=tuple(particles[3:6, k])))
+    return System(bodies=bodies, extras=sysm.extras, geopotentials=sysm.geopotentials, rings=sysm.rings,
+                  delta_t=sysm.delta_t, tdb=sysm.tdb)
+
+
 def make_small_full(seed: int = 7007, n_bodies: int = 48) -> System:
     """The config2 recipe at reduced counts: every force term present, ~n_bodies bodies."""
     rest = max(n_bodies - 9, 8)

@@ -124,6 +124,23 @@ int eph_batch_set_stream(eph_batch *b, void *stream);
 /* Systems in the shared ensemble launch, and launches issued so far. */
 int eph_batch_info(const eph_batch *b, int32_t *n_ensemble, int64_t *launches);
 
+/* ---- Massless test particles (no counterpart in the reference, which has no massless bodies; bodies of
+ * negligible GM in one msystem with the perturbers are its equivalent). The perturbers (at most 32, any
+ * physics) run with msystem::integrate semantics; each particle feels every perturber's Newtonian, 1PN,
+ * deformation, Lense-Thirring, geopotential and ring terms and acts on nothing. */
+typedef struct eph_particles eph_particles;
+int eph_particles_create(int device, eph_particles **out);
+int eph_particles_destroy(eph_particles *p);
+const char *eph_particles_last_error(const eph_particles *p);
+/* Perturbers: planes [EPH_NPLANES][n_pert] (host) and models; particles: [12][n_part] (host) = position
+ * hi (3), position lo (3), velocity hi (3), velocity lo (3) as double-double, SI units. */
+int eph_particles_upload(eph_particles *p, int64_t n_pert, const double *pert_planes, const eph_models *models,
+                         int64_t n_part, const double *part_state);
+/* n_step steps of dt (negative n_step: backwards) from t_eph = t_eph_hi + t_eph_lo, which advances. */
+int eph_particles_integrate(eph_particles *p, double dt, int64_t n_step, double *t_eph_hi, double *t_eph_lo);
+/* Perturber planes and/or particle states ([12][n_part]); either pointer may be NULL. */
+int eph_particles_download(eph_particles *p, double *pert_planes, double *part_state);
+
 /* Limits of eph_integrate_noalloc's fixed scratch (about 2.5 MB of device memory per GPU). */
 #define EPH_NOALLOC_MAX_BODIES 1024
 #define EPH_NOALLOC_MAX_EXT 16     /* bodies with a geopotential or ring model */
