@@ -405,24 +405,28 @@ def make_config5(seed: int = 5005, n_particles: int = 2_000_000, j2: float = 2e-
     sysm.geopotentials["S0"] = (4, 0, [(n, 0, rng.normal(0, 1e-6) / n, 0.0) for n in (3, 4)])
     n = n_particles
     a = rng.uniform(1.5, 50.0, n) * AU
-    e = rng.uniform(0.0, 0.3, n)
-    inc = rng.uniform(0.0, 20 * DEG, n)
+    return sysm, kepler_cloud(rng, GM_SUN, a, rng.uniform(0.0, 0.3, n), rng.uniform(0.0, 20 * DEG, n), star.r, star.v)
+
+
+def kepler_cloud(rng, gm: float, a, e, inc, center_r, center_v) -> np.ndarray:
+    """Particles on Kepler orbits of semi-major axes a, eccentricities e and inclinations inc (arrays) about
+    a centre of mass gm at (center_r, center_v); node, argument of pericentre and mean anomaly uniform.
+    Returns [6][n]: x, y, z, vx, vy, vz."""
+    n = len(a)
     node, argp, M = (rng.uniform(0, 2 * math.pi, n) for _ in range(3))
-    # Kepler's equation by Newton iteration, vectorised
-    E = M.copy()
+    E = M.copy()   # Kepler's equation by Newton iteration, vectorised
     for _ in range(30):
         E = E - (E - e * np.sin(E) - M) / (1 - e * np.cos(E))
     cE, sE = np.cos(E), np.sin(E)
     px, py = a * (cE - e), a * np.sqrt(1 - e * e) * sE
-    nmot = np.sqrt(GM_SUN / a ** 3)
+    nmot = np.sqrt(gm / a ** 3)
     vx, vy = -a * nmot * sE / (1 - e * cE), a * nmot * np.sqrt(1 - e * e) * cE / (1 - e * cE)
     cO, sO, cw, sw, ci, si = np.cos(node), np.sin(node), np.cos(argp), np.sin(argp), np.cos(inc), np.sin(inc)
     P = np.array([cO * cw - sO * sw * ci, sO * cw + cO * sw * ci, sw * si])
     Q = np.array([-cO * sw - sO * cw * ci, -sO * sw + cO * cw * ci, cw * si])
-    rs, vs = np.asarray(star.r), np.asarray(star.v)
-    pos = px * P + py * Q + rs[:, None]
-    vel = vx * P + vy * Q + vs[:, None]
-    return sysm, np.concatenate([pos, vel]).astype(np.float64)
+    pos = px * P + py * Q + np.asarray(center_r, np.float64)[:, None]
+    vel = vx * P + vy * Q + np.asarray(center_v, np.float64)[:, None]
+    return np.concatenate([pos, vel]).astype(np.float64)
 
 
 def with_test_bodies(sysm: System, particles: np.ndarray, gm: float = 1e-20) -> System:
