@@ -412,6 +412,186 @@ def run_reference_ensemble(args):
         print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- config5: massless test particles
+P_CPU_CHUNK = 64   # particles per reference system (with the perturbers as its first bodies)
+
+
+def particle_flops_per_step(pl, models):
+    """Algorithmic FLOPs of one RK12 step of one particle against the perturbers (same convention as
+    algorithmic_flops_per_step; a particle feels only the perturbers' side of the deformation and
+    Lense-Thirring terms, so those count half)."""
+    from ephemeris_b200.msystem import P
+    m = pl.shape[1]
+    full = 0
+    for j in range(m):
+        f = any(pl[P[k], j] != 0 for k in ("K2", "K2R", "DJ2", "LUM", "RR2G_4C")) or \
+            pl[P["GP_INDEX"], j] >= 0 or pl[P["RING_INDEX"], j] >= 0 or \
+            (pl[P["C_STATIC"]:P["C_STATIC"] + 9, j] != 0).any() or (pl[P["W"]:P["W"] + 3, j] != 0).any() or \
+            (pl[P["GL_HI"]:P["GL_HI"] + 6, j] != 0).any()
+        full += int(bool(f))
+    per_stage = m * (FLOP_PASS_A + FLOP_1PN) + full * (FLOP_DEFORM + FLOP_LT) // 2
+    per_stage += len(models.gp_nz) * FLOP_GP + int(np.sum(models.ring_ndisk)) * FLOP_RING_DISK
+    return 25 * per_stage + FLOP_RK
+
+
+def load_particles(args, tmpdir, rank, device=0):
+    """Perturbers (loaded by the product loader) and this rank's particles [6][n]."""
+    from ephemeris_b200 import MSystem, synth
+    sysm, parts = synth.make_config5(5005, n_particles=args.particles,
+                                     particle_seed=None if rank == 0 else 5005 * 1000 + rank)
+    cfg = synth.write_system(sysm, os.path.join(tmpdir, "perturbers"))
+    ms = MSystem(device)
+    if not ms.load(cfg):
+        raise RuntimeError("perturbers failed to load")
+    out = ms.planes(), ms.models(), ms.delta_t, parts, sysm
+    ms.close()
+    return out
+
+
+def _ref_chunk(args):
+    """One chunk of particles (as GM = 1e-20 bodies) with the perturbers through the reference's serial
+    integrator (a worker process)."""
+    cfg, n_step, n_part = args
+    from oracle.pyoracle import RefSystem
+    ref = RefSystem(cfg)
+    dt = ref.lib().ref_delta_t(ref.h)
+    t0 = time.perf_counter()
+    ref.integrate(dt, n_step)
+    return n_part * n_step, time.perf_counter() - t0
+
+
+def particles_cpu(sysm, parts, n_step, tmpdir):
+    """Reference CPU throughput on massless particles: chunks of P_CPU_CHUNK particles plus the 9
+    perturbers per reference system, one chunk per worker process, all host cores."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+    from ephemeris_b200 import synth
+    cores = os.cpu_count() or 1
+    cfgs = []
+    for c in range(cores):
+        chunk = parts[:, c * P_CPU_CHUNK:(c + 1) * P_CPU_CHUNK]
+        cfgs.append(synth.write_system(synth.with_test_bodies(sysm, chunk), os.path.join(tmpdir, f"chunk{c}")))
+    with cf.ProcessPoolExecutor(max_workers=cores, mp_context=mp.get_context("spawn")) as ex:
+        list(ex.map(_ref_chunk, [(c, 1, P_CPU_CHUNK) for c in cfgs]))   # start the workers
+        t0 = time.perf_counter()
+        done = list(ex.map(_ref_chunk, [(c, n_step, P_CPU_CHUNK) for c in cfgs]))
+        el = time.perf_counter() - t0
+    steps = sum(b for b, _ in done)
+    return {"value": steps / el, "unit": "particle-steps/s", "cores": cores, "kind": "reference",
+            "sample": f"{cores} chunks of {P_CPU_CHUNK} particles (GM=1e-20 bodies) + {len(sysm.bodies)} perturbers, "
+                      f"{n_step} RK12 steps each, reference msystem::integrate(dt,n,0) serial, one chunk per process "
+                      f"on {cores} processes, {el:.1f} s"}
+
+
+def run_b200_particles(args):
+    import torch
+    from ephemeris_b200 import Particles
+    rank, world, local, pg = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    with tempfile.TemporaryDirectory() as td:
+        pl, md, dt, parts, sysm = load_particles(args, td, rank, local)
+        n_part, ks = parts.shape[1], args.p_steps
+        stream = torch.cuda.Stream(dev)
+        torch.cuda.set_stream(stream)
+        p = Particles(local)
+        p.set_stream(stream.cuda_stream)
+        flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+        for _ in range(args.warmup):
+            p.upload(pl, md, parts)
+            p.integrate(dt, min(ks, 20))
+        barrier(pg, dev)
+        torch.cuda.synchronize(dev)
+        clocks = ClockSampler(local)
+        clocks.start()
+        l0, k0 = p.info()
+        dev_ms = 0.0
+        for k in range(args.steps):
+            p.upload(pl, md, parts)                  # inputs in HBM before the timed region
+            flush.fill_(float(k))
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            p.integrate(dt, ks)
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            dev_ms += e0.elapsed_time(e1)
+        clk = clocks.stop()
+        l1, k1 = p.info()
+        part_launches = args.steps                   # one particle-kernel launch per call (all steps fit one round)
+        kern_ms = (k1 - k0) / part_launches
+        dev_ms_max = reduce_max(pg, dev_ms, dev)
+        value = world * n_part * ks * args.steps / (dev_ms_max / 1e3)
+        # end to end through the public API: host particles up, integrate, host particles down
+        pin = torch.from_numpy(np.ascontiguousarray(parts)).pin_memory().numpy()
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            p.upload(pl, md, pin)
+            p.integrate(dt, ks)
+            p.download()
+        e2e_s = reduce_max(pg, time.perf_counter() - t0, dev)
+        e2e = world * n_part * ks * args.steps / e2e_s
+        h2d = int(12 * n_part * 8 + pl.nbytes)
+        d2h = int(12 * n_part * 8 + pl.nbytes)
+        fps = particle_flops_per_step(pl, md)
+        achieved = fps * n_part * ks / (kern_ms / 1e3) / 1e12
+        peak, peak_src = fp64_peak(dev)
+        cpu = None
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            try:
+                cpu = particles_cpu(sysm, parts, args.p_cpu_steps, td)
+            except Exception as exc:
+                cpu = {"value": None, "unit": "particle-steps/s", "cores": 0, "kind": "unavailable", "sample": str(exc)}
+        if rank == 0:
+            line = {
+                "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64 (double-double state)", "data": "synthetic",
+                "config": {"workload": f"config5: {n_part} massless particles per GPU (a 1.5-50 AU, e < 0.3, "
+                                       f"i < 20 deg) against {pl.shape[1]} perturbers (star with J2-J4, 8 planets; "
+                                       f"Newtonian + 1PN), dt=0.5 day, {ks} RK12 steps per bench step",
+                           "particles": n_part, "perturbers": int(pl.shape[1]), "rk_steps_per_step": ks,
+                           "parallelism": f"particles sharded x{world}, perturbers replicated" if world > 1
+                           else "1 GPU",
+                           "l2": "flushed between timed steps (256 MB write); particle state 240 MB > L2"},
+                "e2e": {"value": e2e, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+                "roofline": {"bound": "fp64", "kernel": "particle_kernel", "achieved": achieved, "peak": peak,
+                             "unit": "TFLOP/s", "frac": achieved / peak if peak else None, "traffic": None,
+                             "peak_source": peak_src, "flops_per_launch": fps * n_part * ks,
+                             "kernel_ms": kern_ms},
+                "gpu_launches": l1 - l0,
+                "clocks": clk,
+            }
+            if cpu is not None:
+                line["cpu_baseline"] = cpu
+            print(json.dumps(line), flush=True)
+        p.close()
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+def run_reference_particles(args):
+    """--impl reference --workload config5: the reference CPU integrator on chunks of the particles."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from ephemeris_b200 import synth
+    with tempfile.TemporaryDirectory() as td:
+        sysm, parts = synth.make_config5(5005, n_particles=P_CPU_CHUNK * (os.cpu_count() or 1))
+        vals, cpu = [], None
+        for _ in range(max(1, args.steps)):
+            cpu = particles_cpu(sysm, parts, args.p_cpu_steps, td)
+            vals.append(cpu["value"])
+        value = statistics.median(vals)
+        line = {"metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": args.gpus, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64 (double-double state)", "data": "synthetic", "impl": "reference",
+                "config": {"workload": "config5 particles, reference CPU sample (see cpu_baseline.sample)"},
+                "cpu_baseline": dict(cpu, value=value),
+                "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+
+
 def run_b200(args):
     import torch
     from ephemeris_b200 import Context, MSystem
@@ -567,8 +747,16 @@ def main():
     ap.add_argument("--ens-frac", type=float, default=0.1, help="config3: fraction of each member's drawn duration")
     ap.add_argument("--ens-cpu-members", type=int, default=64, help="config3: members in the CPU sample")
     ap.add_argument("--ens-cpu-steps", type=int, default=200, help="config3: RK12 steps per member in the CPU sample")
+    ap.add_argument("--particles", type=int, default=2_000_000, help="config5: massless particles per GPU")
+    ap.add_argument("--p-steps", type=int, default=100, help="config5: RK12 steps per bench step")
+    ap.add_argument("--p-cpu-steps", type=int, default=300, help="config5: RK12 steps per chunk in the CPU sample")
     args = ap.parse_args()
-    if args.workload == "config3":
+    if args.workload == "config5":
+        if args.impl == "reference":
+            run_reference_particles(args)
+        else:
+            run_b200_particles(args)
+    elif args.workload == "config3":
         if args.impl == "reference":
             run_reference_ensemble(args)
         else:

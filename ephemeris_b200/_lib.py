@@ -63,6 +63,8 @@ SIGNATURES = [
     ("eph_particles_upload", ctypes.c_int, [_VP, ctypes.c_int64, _D, ctypes.POINTER(EphModels), ctypes.c_int64, _D]),
     ("eph_particles_integrate", ctypes.c_int, [_VP, ctypes.c_double, ctypes.c_int64, _D, _D]),
     ("eph_particles_download", ctypes.c_int, [_VP, _D, _D]),
+    ("eph_particles_set_stream", ctypes.c_int, [_VP, _VP]),
+    ("eph_particles_info", ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_double)]),
     ("eph_integrate_noalloc", ctypes.c_int, [ctypes.c_int, _VP, ctypes.c_int64, _VP, ctypes.POINTER(EphModels),
                                              ctypes.c_double, ctypes.c_int64, _D, _D]),
     ("eph_msystem_load", ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(_VP)]),

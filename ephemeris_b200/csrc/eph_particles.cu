@@ -42,12 +42,16 @@ namespace {
 
 constexpr int kPThreads = 256;          // particles per CTA
 constexpr int kPMaxPert = 32;           // perturbers (their stage records live in shared memory)
-constexpr int kPChunk = 400;            // steps per round of perturbers then particles
+constexpr size_t kPRecordBytes = 1ull << 30;   // stage records of one round of perturbers then particles
 constexpr double kCP = 299792458.0;     // src/math/basic_math.h:10,18
 constexpr int kPF = 9;                  // stored values per (particle, stage): velocity dd (hi 3, lo 3), acceleration 3
 
-__constant__ double p_rk_hi[EPH_RK12_NCOEF];
-__constant__ double p_rk_lo[EPH_RK12_NCOEF];
+// the nonzero coefficients of the Feagin table, row by row: entries p_nz_off[k-1] .. p_nz_off[k] - 1 of
+// row k (stage k's state) hold j, a_kj (hi, lo) and hi + lo rounded
+constexpr int kPMaxNZ = EPH_RK12_NCOEF;
+__constant__ int p_nz_off[kStages + 1];
+__constant__ int p_nz_j[kPMaxNZ];
+__constant__ double p_nz_hi[kPMaxNZ], p_nz_lo[kPMaxNZ], p_nz_f[kPMaxNZ];
 
 struct PertInfo {
     int gp, ring;   // model indices, or -1
@@ -71,33 +75,51 @@ struct PartArgs {
     int *next;                  // particle-block queue
 };
 
-// acceleration of particle (r, v) at the stage whose perturber records are in P
-__device__ __forceinline__ v3 particle_accel(const PartArgs &A, const double *P, const dd r[3], const dd v[3]) {
+// gp_sum (eph_models.cuh) for a purely zonal model (Nt = 0) with its degree loop rolled: the zonal
+// recursion of geopotential::sum (src/physics/geopotential.impl:18-60) in a handful of registers, so the
+// particle kernel keeps its occupancy when its only extended perturber is zonal.
+__device__ __forceinline__ v3 gp_zonal(const double *__restrict__ c_table, int Nz, double R, v3 r) {
+    const double rho2 = r.x * r.x + r.y * r.y;
+    const double rr2 = 1.0 / (rho2 + r.z * r.z);
+    const double rho1 = sqrt(rho2);
+    const double rr1 = sqrt(rr2);
+    const double rb1 = R * rr1;
+    const double cphi = rho1 * rr1;
+    const double sphi = r.z * rr1;
+    double cm, sm;
+    if (rho2 < 2.2250738585072014e-308) { cm = 1; sm = 0; }
+    else { cm = r.x / rho1; sm = r.y / rho1; }
+    double rbn = rb1, ppn = 1, pn = 1, pn1 = sphi, zx = 0, zz = 0;
+#pragma unroll 1
+    for (int n = 2; n <= Nz; ++n) {
+        rbn *= rb1;
+        pn = ((double)(2 * n - 1) * sphi * pn1 - (double)(n - 1) * pn) / (double)n;
+        ppn = sphi * ppn + (double)n * pn1;
+        const double z1 = __ldg(c_table + (n * n - 4)) * rbn;
+        zx += (double)(n + 1) * z1 * pn;
+        zz -= z1 * ppn;
+        const double sw = pn; pn = pn1; pn1 = sw;
+    }
+    const double tx = rr2 * zx, tz = rr2 * (zz * cphi);
+    const double g1 = tx * cphi - tz * sphi;
+    return mk(g1 * cm, g1 * sm, cphi * tz + sphi * tx);
+}
+
+// acceleration of particle (r, v) at the stage whose perturber records are in P. One sweep over the
+// perturbers: pass B's 4 phi_i term (mass.impl:90) is sum_j GM_j/r^3 * 4 phi_i * d = 4 phi_i * a_N,i, so it
+// is added once after the sweep instead of waiting for phi_i; the other terms are the reference's.
+// kGeneral = false: the field loop handles zonal geopotentials only (gp_zonal, inline); true: any model
+// (gp_sum, ring_sum: calls, whose register saves cost the kernel some spilling).
+template <bool kGeneral>
+__device__ __forceinline__ v3 particle_accel(const PartArgs &A, const double *P, const PertInfo *info,
+                                             const dd r[3], const dd v[3]) {
     const int np = A.n_pert;
     const double c2 = kCP * kCP;
 #define PR(j, f) P[(j) * kTrajRec + (f)]
-    // pass A
-    double phi = 0;
-    v3 na = mk(0, 0, 0);
-#pragma unroll 1
-    for (int j = 0; j < np; ++j) {
-        const v3 d = mk(sep_diff(PR(j, TR_R_HI + 0), PR(j, TR_R_LO + 0), r[0].hi, r[0].lo),
-                        sep_diff(PR(j, TR_R_HI + 1), PR(j, TR_R_LO + 1), r[1].hi, r[1].lo),
-                        sep_diff(PR(j, TR_R_HI + 2), PR(j, TR_R_LO + 2), r[2].hi, r[2].lo));
-        const double q = dot(d, d), sm = PR(j, TR_SR2);
-        const double rr = rsqrt((q < sm) ? sm : q);
-        const double tp_dphi = rr * PR(j, TR_GM);
-        const double tp_dg = rr * rr * tp_dphi;
-        phi -= tp_dphi;
-        na += tp_dg * d;
-    }
-    // PREPARE_RELATIVITY
-    const v3 bi = vdiv(mk(dd_val(v[0]), dd_val(v[1]), dd_val(v[2])), kCP);
+    const v3 bi = vdiv(mk(dd_val(v[0]), dd_val(v[1]), dd_val(v[2])), kCP);   // PREPARE_RELATIVITY
     const double beta2 = dot(bi, bi);
-    phi = phi / c2;
-    na = vdiv(na, c2);
-    // pass B: 1PN, and the deformation and Lense-Thirring fields of full-class perturbers
-    v3 ga = mk(0, 0, 0), da = mk(0, 0, 0);
+    double phi = 0;
+    v3 na = mk(0, 0, 0), ga = mk(0, 0, 0), da = mk(0, 0, 0);
 #pragma unroll 1
     for (int j = 0; j < np; ++j) {
         const v3 d = mk(sep_diff(PR(j, TR_R_HI + 0), PR(j, TR_R_LO + 0), r[0].hi, r[0].lo),
@@ -106,19 +128,22 @@ __device__ __forceinline__ v3 particle_accel(const PartArgs &A, const double *P,
         const double GMj = PR(j, TR_GM);
         const double q = dot(d, d), sm = PR(j, TR_SR2);
         const double rr = rsqrt((q < sm) ? sm : q);
-        const double rr2 = rr * rr, rr3 = rr * rr2;
+        const double rr2 = rr * rr;
         const double tp_dphi = rr * GMj;
         const double tp_dg = rr2 * tp_dphi;
+        phi -= tp_dphi;                                            // pass A (mass.impl:38-46)
+        na += tp_dg * d;
         const v3 bj = mk(PR(j, TR_BETA + 0), PR(j, TR_BETA + 1), PR(j, TR_BETA + 2));
         const double rbj = dot(d, bj);
         double tp = rbj * rr;
         tp *= tp;
         const v3 naj = mk(PR(j, TR_NACC + 0), PR(j, TR_NACC + 1), PR(j, TR_NACC + 2));
-        const double delta1 = 4 * phi + PR(j, TR_PHI) + beta2 + 2 * PR(j, TR_BETA2) - 4 * dot(bi, bj) +
-                              (dot(d, naj) - 3 * tp) / 2;
+        const double delta1 = PR(j, TR_PHI) + beta2 + 2 * PR(j, TR_BETA2) - 4 * dot(bi, bj) +
+                              (dot(d, naj) - 3 * tp) / 2;                 // mass.impl:82-97 less 4 phi_i
         const v3 b = bj - bi;
         ga += (7 * tp_dphi / 2) * naj + (tp_dg * delta1) * d + (tp_dg * (rbj - dot(d, b) * 4)) * b;
-        if (!A.info[j].full) continue;
+        if (!info[j].full) continue;
+        const double rr3 = rr * rr2;                               // j's deformation and spin (mass.impl:99-125)
         const m3 Cj = m3{mk(PR(j, TR_CPOT + 0), PR(j, TR_CPOT + 1), PR(j, TR_CPOT + 2)),
                          mk(PR(j, TR_CPOT + 3), PR(j, TR_CPOT + 4), PR(j, TR_CPOT + 5)),
                          mk(PR(j, TR_CPOT + 6), PR(j, TR_CPOT + 7), PR(j, TR_CPOT + 8))};
@@ -129,10 +154,13 @@ __device__ __forceinline__ v3 particle_accel(const PartArgs &A, const double *P,
         dj += cross(rcr32 * (GLj - (3 * dot(GLj, d) * rr2) * d), b);
         da += dj;
     }
+    phi = phi / c2;
+    ga += (4 * phi) * na;
+    na = vdiv(na, c2);
     // fields of the extended perturbers, r = r_particle - r_host (mass.cpp:184,198)
 #pragma unroll 1
     for (int j = 0; j < np; ++j) {
-        const int gp = A.info[j].gp, rg = A.info[j].ring;
+        const int gp = info[j].gp, rg = info[j].ring;
         if (gp < 0 && rg < 0) continue;
         const v3 re = mk(dd_diff(r[0].hi, r[0].lo, PR(j, TR_R_HI + 0), PR(j, TR_R_LO + 0)),
                          dd_diff(r[1].hi, r[1].lo, PR(j, TR_R_HI + 1), PR(j, TR_R_LO + 1)),
@@ -141,11 +169,14 @@ __device__ __forceinline__ v3 particle_accel(const PartArgs &A, const double *P,
             const m3 f = m3{mk(PR(j, TR_FRAME + 0), PR(j, TR_FRAME + 1), PR(j, TR_FRAME + 2)),
                             mk(PR(j, TR_FRAME + 3), PR(j, TR_FRAME + 4), PR(j, TR_FRAME + 5)),
                             mk(PR(j, TR_FRAME + 6), PR(j, TR_FRAME + 7), PR(j, TR_FRAME + 8))};
-            const v3 an = toworld(f, gp_sum(A.gp_coef + (size_t)gp * EPH_GP_TABLE_SIZE, A.gp_nz[gp], A.gp_nt[gp],
-                                            PR(j, TR_RADIUS), tolocal(f, re)));
+            const double *tab = A.gp_coef + (size_t)gp * EPH_GP_TABLE_SIZE;
+            const int nz = A.gp_nz[gp], nt = A.gp_nt[gp];
+            const v3 rl = tolocal(f, re);
+            const v3 an = toworld(f, (!kGeneral || nt == 0) ? gp_zonal(tab, nz, PR(j, TR_RADIUS), rl)
+                                                            : gp_sum(tab, nz, nt, PR(j, TR_RADIUS), rl));
             da += PR(j, TR_GM) * an;
         }
-        if (rg >= 0) {
+        if (kGeneral && rg >= 0) {
             const m3 f = m3{mk(PR(j, TR_RFRAME + 0), PR(j, TR_RFRAME + 1), PR(j, TR_RFRAME + 2)),
                             mk(PR(j, TR_RFRAME + 3), PR(j, TR_RFRAME + 4), PR(j, TR_RFRAME + 5)),
                             mk(PR(j, TR_RFRAME + 6), PR(j, TR_RFRAME + 7), PR(j, TR_RFRAME + 8))};
@@ -165,77 +196,114 @@ __device__ __forceinline__ void load_records(const PartArgs &A, double *P, long 
     __syncthreads();
 }
 
+// Per stage, the thread stores (v hi, v lo, f) of its particle to the CTA's slice of the stage store and
+// gathers the earlier stages' values over the nonzero coefficients of the stage's row (p_nz_*). The
+// intermediate stages sum sum_j a_kj v_j and sum_j a_kj f_j in double with fused multiply-adds (v_j by its
+// high part): their rounding reaches the step's result only through the stage accelerations, at about
+// 1e-16 of the stage increment. The last row (the state update) is summed exactly as RungeKutta.impl:
+// 166-186: a_kj v_j in double-double, a_kj f_j rounded term by term.
+template <bool kGeneral>
 __global__ void __launch_bounds__(kPThreads, 2) particle_kernel(PartArgs A) {
     __shared__ double P[kPMaxPert * kTrajRec];
+    __shared__ double X0[12][kPThreads];    // the step's start state: r hi, r lo, v hi, v lo
+    __shared__ PertInfo info[kPMaxPert];
     __shared__ int s_blk;
-    double *F = A.fstore + (size_t)blockIdx.x * kStages * kPF * kPThreads + threadIdx.x;   // [stage][value] stride kPThreads
+    const int t = threadIdx.x;
+    for (int j = t; j < A.n_pert; j += blockDim.x) info[j] = A.info[j];
+    double *F = A.fstore + (size_t)blockIdx.x * kStages * kPF * kPThreads + t;   // [stage][value] stride kPThreads
     const int nb = (A.n_part + kPThreads - 1) / kPThreads;
 #pragma unroll 1
     for (;;) {
-        if (threadIdx.x == 0) s_blk = atomicAdd(A.next, 1);
+        __syncthreads();
+        if (t == 0) s_blk = atomicAdd(A.next, 1);
         __syncthreads();
         const int blk = s_blk;
-        __syncthreads();
         if (blk >= nb) return;
-        const int ip = blk * kPThreads + threadIdx.x;
+        const int ip = blk * kPThreads + t;
         const bool live = ip < A.n_part;
         const int n = A.n_part;
+        // X0: the step's start state; F stage 0: (v, f) of that state. v_k goes to F[k] as soon as it is
+        // formed, so that only r_k stays in registers across the acceleration.
         dd r[3], v[3];
         v3 fa = mk(0, 0, 0);
         for (int c = 0; c < 3; ++c) {
             r[c] = live ? dd{A.state[(0 + c) * n + ip], A.state[(3 + c) * n + ip]} : dd_make(1e30);
             v[c] = live ? dd{A.state[(6 + c) * n + ip], A.state[(9 + c) * n + ip]} : dd_make(0);
+            X0[c][t] = r[c].hi; X0[3 + c][t] = r[c].lo;
+            X0[6 + c][t] = v[c].hi; X0[9 + c][t] = v[c].lo;
+            F[(size_t)c * kPThreads] = v[c].hi;
+            F[(size_t)(3 + c) * kPThreads] = v[c].lo;
         }
         if (live) fa = mk(A.state[12 * n + ip], A.state[13 * n + ip], A.state[14 * n + ip]);
         if (A.start_accel) {   // f_0 at the start state (the reference's loader runs accel(), mass_loader.cpp:555)
             load_records(A, P, 0);
-            if (live) fa = particle_accel(A, P, r, v);
+            if (live) fa = particle_accel<kGeneral>(A, P, info, r, v);
         }
+        F[(size_t)6 * kPThreads] = fa.x;
+        F[(size_t)7 * kPThreads] = fa.y;
+        F[(size_t)8 * kPThreads] = fa.z;
         const double dt = A.dt;
         const dd ddt = dd_make(dt);
 #pragma unroll 1
         for (long long step = 0; step < A.n_step; ++step) {
-            dd r0[3], v0[3];
-            for (int c = 0; c < 3; ++c) { r0[c] = r[c]; v0[c] = v[c]; }
 #pragma unroll 1
             for (int s = 0; s < kStages; ++s) {
-                double *Fs = F + (size_t)s * kPF * kPThreads;
-                for (int c = 0; c < 3; ++c) {
-                    Fs[(size_t)c * kPThreads] = v[c].hi;
-                    Fs[(size_t)(3 + c) * kPThreads] = v[c].lo;
-                }
-                Fs[(size_t)6 * kPThreads] = fa.x;
-                Fs[(size_t)7 * kPThreads] = fa.y;
-                Fs[(size_t)8 * kPThreads] = fa.z;
-                // state of stage k: sum_j a_kj f_j in ascending j, zero coefficients skipped
-                const int k = s + 1, ci0 = k * (k - 1) / 2;
-                dd sv[3] = {dd_make(0), dd_make(0), dd_make(0)};
-                double sa[3] = {0.0, 0.0, 0.0};
-#pragma unroll 4
-                for (int j = 0; j < k; ++j) {
-                    const dd a = dd{p_rk_hi[ci0 + j], p_rk_lo[ci0 + j]};
-                    if (a.hi == 0) continue;
-                    const double fac = dd_val(a);
-                    const double *Fj = F + (size_t)j * kPF * kPThreads;
+                const int e0 = p_nz_off[s], e1 = p_nz_off[s + 1];
+                double *Fk;
+                if (s + 1 < kStages) {
+                    double sv[3] = {0.0, 0.0, 0.0}, sa[3] = {0.0, 0.0, 0.0};
+#pragma unroll 2
+                    for (int e = e0; e < e1; ++e) {
+                        const double fac = p_nz_f[e];
+                        const double *Fj = F + (size_t)p_nz_j[e] * kPF * kPThreads;
+                        for (int c = 0; c < 3; ++c) {
+                            sv[c] = __fma_rn(fac, Fj[(size_t)c * kPThreads], sv[c]);
+                            sa[c] = __fma_rn(fac, Fj[(size_t)(6 + c) * kPThreads], sa[c]);
+                        }
+                    }
+                    Fk = F + (size_t)(s + 1) * kPF * kPThreads;
                     for (int c = 0; c < 3; ++c) {
-                        sv[c] = dd_add(sv[c], dd_mul(a, dd{Fj[(size_t)c * kPThreads], Fj[(size_t)(3 + c) * kPThreads]}));
-                        sa[c] = __dadd_rn(sa[c], __dmul_rn(fac, Fj[(size_t)(6 + c) * kPThreads]));
+                        r[c] = dd_add(dd{X0[c][t], X0[3 + c][t]}, dd_make(dt * sv[c]));
+                        v[c] = dd_add(dd{X0[6 + c][t], X0[9 + c][t]}, dd_make(dt * sa[c]));
+                    }
+                } else {
+                    dd sv[3] = {dd_make(0), dd_make(0), dd_make(0)};
+                    double sa[3] = {0.0, 0.0, 0.0};
+#pragma unroll 1
+                    for (int e = e0; e < e1; ++e) {
+                        const dd a = dd{p_nz_hi[e], p_nz_lo[e]};
+                        const double fac = p_nz_f[e];
+                        const double *Fj = F + (size_t)p_nz_j[e] * kPF * kPThreads;
+                        for (int c = 0; c < 3; ++c) {
+                            sv[c] = dd_add(sv[c], dd_mul(a, dd{Fj[(size_t)c * kPThreads], Fj[(size_t)(3 + c) * kPThreads]}));
+                            sa[c] = __dadd_rn(sa[c], __dmul_rn(fac, Fj[(size_t)(6 + c) * kPThreads]));
+                        }
+                    }
+                    Fk = F;   // the new state is stage 0 of the next step
+                    for (int c = 0; c < 3; ++c) {
+                        r[c] = dd_add(dd{X0[c][t], X0[3 + c][t]}, dd_mul(ddt, sv[c]));
+                        v[c] = dd_add(dd{X0[6 + c][t], X0[9 + c][t]}, dd_make(dt * sa[c]));
+                        X0[c][t] = r[c].hi; X0[3 + c][t] = r[c].lo;
+                        X0[6 + c][t] = v[c].hi; X0[9 + c][t] = v[c].lo;
                     }
                 }
                 for (int c = 0; c < 3; ++c) {
-                    r[c] = dd_add(r0[c], dd_mul(ddt, sv[c]));
-                    v[c] = dd_add(v0[c], dd_make(dt * sa[c]));
+                    Fk[(size_t)c * kPThreads] = v[c].hi;
+                    Fk[(size_t)(3 + c) * kPThreads] = v[c].lo;
                 }
                 load_records(A, P, 1 + step * kStages + s);
-                if (live) fa = particle_accel(A, P, r, v);
+                if (live) fa = particle_accel<kGeneral>(A, P, info, r, v);
+                Fk[(size_t)6 * kPThreads] = fa.x;
+                Fk[(size_t)7 * kPThreads] = fa.y;
+                Fk[(size_t)8 * kPThreads] = fa.z;
             }
         }
         if (live) {
             for (int c = 0; c < 3; ++c) {
-                A.state[(0 + c) * n + ip] = r[c].hi;
-                A.state[(3 + c) * n + ip] = r[c].lo;
-                A.state[(6 + c) * n + ip] = v[c].hi;
-                A.state[(9 + c) * n + ip] = v[c].lo;
+                A.state[(0 + c) * n + ip] = X0[c][t];
+                A.state[(3 + c) * n + ip] = X0[3 + c][t];
+                A.state[(6 + c) * n + ip] = X0[6 + c][t];
+                A.state[(9 + c) * n + ip] = X0[9 + c][t];
             }
             A.state[12 * n + ip] = fa.x;
             A.state[13 * n + ip] = fa.y;
@@ -249,8 +317,24 @@ cudaError_t particles_setup(int device) {
     if (device >= 0 && device < 64 && g_part_ready[device]) return cudaSuccess;
     double hi[EPH_RK12_NCOEF], lo[EPH_RK12_NCOEF], dtk[kStages + 1];
     rk12_expand(hi, lo, dtk);
-    cudaError_t e = cudaMemcpyToSymbol(p_rk_hi, hi, sizeof(hi));
-    if (e == cudaSuccess) e = cudaMemcpyToSymbol(p_rk_lo, lo, sizeof(lo));
+    int off[kStages + 1], nj[kPMaxNZ] = {0};
+    double nh[kPMaxNZ] = {0}, nl[kPMaxNZ] = {0}, nf[kPMaxNZ] = {0};
+    int m = 0;
+    off[0] = 0;
+    for (int k = 1; k <= kStages; ++k) {
+        for (int j = 0; j < k; ++j) {
+            const int ci = k * (k - 1) / 2 + j;
+            if (hi[ci] == 0) continue;   // RungeKutta.impl skips zero coefficients
+            nj[m] = j; nh[m] = hi[ci]; nl[m] = lo[ci]; nf[m] = hi[ci] + lo[ci];
+            ++m;
+        }
+        off[k] = m;
+    }
+    cudaError_t e = cudaMemcpyToSymbol(p_nz_off, off, sizeof(off));
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(p_nz_j, nj, sizeof(nj));
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(p_nz_hi, nh, sizeof(nh));
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(p_nz_lo, nl, sizeof(nl));
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(p_nz_f, nf, sizeof(nf));
     if (e == cudaSuccess && device >= 0 && device < 64) g_part_ready[device] = true;
     return e;
 }
@@ -262,7 +346,11 @@ using namespace eph;
 
 struct eph_particles {
     int device = 0;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;     // work stream (own_stream unless eph_particles_set_stream chose another)
+    cudaStream_t own_stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    int64_t launches = 0;              // kernels launched (step kernel, particle kernel)
+    double kernel_ms = 0;              // particle_kernel device time, summed
     std::mutex mu;
     char err[512] = {0};
     eph_ctx *ctx = nullptr;            // the perturbers
@@ -278,6 +366,7 @@ struct eph_particles {
     PertInfo *d_info = nullptr;
     size_t traj_cap = 0;
     int grid = 0;
+    bool general = false;              // a tesseral geopotential or a ring among the perturbers
 };
 
 static int pfail(eph_particles *p, int code, const char *what, cudaError_t e = cudaSuccess) {
@@ -324,13 +413,14 @@ int eph_particles_create(int device, eph_particles **out) {
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) return EPH_ERR_ARG;
     eph_particles *p = new eph_particles();
     p->device = device;
-    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking) != cudaSuccess ||
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&p->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&p->ev0) != cudaSuccess || cudaEventCreate(&p->ev1) != cudaSuccess ||
         particles_setup(device) != cudaSuccess || eph_ctx_create(device, &p->ctx) != EPH_OK ||
         eph_ctx_create(device, &p->ctx0) != EPH_OK) {
-        if (p->ctx) eph_ctx_destroy(p->ctx);
-        delete p;
+        eph_particles_destroy(p);
         return EPH_ERR_CUDA;
     }
+    p->stream = p->own_stream;
     *out = p;
     return EPH_OK;
 }
@@ -341,12 +431,30 @@ int eph_particles_destroy(eph_particles *p) {
     part_free(p);
     if (p->ctx) eph_ctx_destroy(p->ctx);
     if (p->ctx0) eph_ctx_destroy(p->ctx0);
-    if (p->stream) cudaStreamDestroy(p->stream);
+    if (p->ev0) cudaEventDestroy(p->ev0);
+    if (p->ev1) cudaEventDestroy(p->ev1);
+    if (p->own_stream) cudaStreamDestroy(p->own_stream);
     delete p;
     return EPH_OK;
 }
 
 const char *eph_particles_last_error(const eph_particles *p) { return p ? p->err : "null particle set"; }
+
+int eph_particles_set_stream(eph_particles *p, void *stream) {
+    if (!p) return EPH_ERR_ARG;
+    std::lock_guard<std::mutex> lock(p->mu);
+    p->stream = stream ? (cudaStream_t)stream : p->own_stream;
+    int rc = eph_set_stream(p->ctx, stream);
+    if (!rc) rc = eph_set_stream(p->ctx0, stream);
+    return rc;
+}
+
+int eph_particles_info(const eph_particles *p, int64_t *launches, double *particle_kernel_ms) {
+    if (!p || !launches || !particle_kernel_ms) return EPH_ERR_ARG;
+    *launches = p->launches;
+    *particle_kernel_ms = p->kernel_ms;
+    return EPH_OK;
+}
 
 int eph_particles_upload(eph_particles *p, int64_t n_pert, const double *pert_planes, const eph_models *models,
                          int64_t n_part, const double *part_state) {
@@ -384,7 +492,11 @@ int eph_particles_upload(eph_particles *p, int64_t n_pert, const double *pert_pl
     std::vector<double> st((size_t)15 * n_part, 0.0);
     std::copy(part_state, part_state + (size_t)12 * n_part, st.begin());
     int per_sm = 0, sms = 0;
-    PCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, particle_kernel, kPThreads, 0), "occupancy");
+    p->general = false;
+    for (int j = 0; j < n_pert; ++j)
+        p->general = p->general || info[j].ring >= 0 || (info[j].gp >= 0 && p->gp_nt[info[j].gp] > 0);
+    PCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, p->general ? particle_kernel<true> : particle_kernel<false>,
+                                                      kPThreads, 0), "occupancy");
     PCK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p->device), "SM count");
     const int64_t nblk = (n_part + kPThreads - 1) / kPThreads;
     p->grid = (int)std::max<int64_t>(1, std::min<int64_t>(nblk, (int64_t)per_sm * sms));
@@ -424,7 +536,9 @@ int eph_particles_integrate(eph_particles *p, double dt, int64_t n_step, double 
     }
     PCK(cudaSetDevice(p->device), "cudaSetDevice");
     const size_t rec = (size_t)p->n_pert * kTrajRec;
-    const size_t need = (size_t)(1 + kStages * std::min<int64_t>(n_step, kPChunk)) * rec;
+    // steps per round: all of them while their stage records fit kPRecordBytes
+    const int64_t chunk = std::max<int64_t>(1, (int64_t)(kPRecordBytes / (sizeof(double) * kStages * rec)));
+    const size_t need = (size_t)(1 + kStages * std::min<int64_t>(n_step, chunk)) * rec;
     if (need > p->traj_cap) {
         if (p->d_traj) cudaFree(p->d_traj);
         p->d_traj = nullptr;
@@ -444,6 +558,7 @@ int eph_particles_integrate(eph_particles *p, double dt, int64_t n_step, double 
         ctx_record_stages(p->ctx0, p->d_traj, 0);
         if (!rc) rc = eph_accel(p->ctx0);
         ctx_record_stages(p->ctx0, nullptr, 0);
+        ++p->launches;
         if (rc) return pfail(p, rc, eph_last_error(p->ctx0));
     }
     // msystem::integrate: maxima reset before, min_distance inverted after (mass.cpp:406,436)
@@ -451,10 +566,11 @@ int eph_particles_integrate(eph_particles *p, double dt, int64_t n_step, double 
     eph_device_planes(p->ctx, &d_pl);
     PCK(cudaMemset(d_pl + (size_t)EPH_P_MIN_DISTANCE * p->n_pert, 0, 2 * p->n_pert * sizeof(double)), "reset maxima");
     for (int64_t done = 0; done < n_step;) {
-        const int64_t c = std::min<int64_t>(n_step - done, kPChunk);
+        const int64_t c = std::min<int64_t>(n_step - done, chunk);
         ctx_record_stages(p->ctx, p->d_traj, 1);
         rc = eph_rk12(p->ctx, dt, c, *t_eph_hi, *t_eph_lo);
         ctx_record_stages(p->ctx, nullptr, 0);
+        ++p->launches;
         if (rc) return pfail(p, rc, eph_last_error(p->ctx));
         PartArgs A;
         A.n_part = (int)p->n_part;
@@ -470,9 +586,16 @@ int eph_particles_integrate(eph_particles *p, double dt, int64_t n_step, double 
         A.ring_nd = p->d_ring_nd; A.ring_disk = p->d_ring_disk;
         A.next = p->d_next;
         PCK(cudaMemsetAsync(p->d_next, 0, sizeof(int), p->stream), "reset queue");
-        particle_kernel<<<p->grid, kPThreads, 0, p->stream>>>(A);
+        PCK(cudaEventRecord(p->ev0, p->stream), "event");
+        if (p->general) particle_kernel<true><<<p->grid, kPThreads, 0, p->stream>>>(A);
+        else particle_kernel<false><<<p->grid, kPThreads, 0, p->stream>>>(A);
         PCK(cudaGetLastError(), "launch particle kernel");
+        ++p->launches;
+        PCK(cudaEventRecord(p->ev1, p->stream), "event");
         PCK(cudaStreamSynchronize(p->stream), "particle kernel");
+        float ms = 0;
+        PCK(cudaEventElapsedTime(&ms, p->ev0, p->ev1), "event time");
+        p->kernel_ms += ms;
         p->started = true;
         dd_advance(t_eph_hi, t_eph_lo, dt * (double)c);
         done += c;

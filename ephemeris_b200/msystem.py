@@ -243,6 +243,17 @@ class Particles:
         self._check(self.lib.eph_particles_download(self.h, _dptr(pl), _dptr(pa)), "particles download")
         return pl, pa
 
+    def set_stream(self, stream: int | None):
+        """Issue the work on a cudaStream_t (e.g. torch.cuda.Stream().cuda_stream); None: own stream."""
+        self._check(self.lib.eph_particles_set_stream(self.h, ctypes.c_void_p(stream) if stream else None),
+                    "particles set_stream")
+
+    def info(self):
+        """(kernels launched, summed particle-kernel device time in ms)."""
+        n, ms = ctypes.c_int64(), ctypes.c_double()
+        self._check(self.lib.eph_particles_info(self.h, ctypes.byref(n), ctypes.byref(ms)), "particles info")
+        return n.value, ms.value
+
 
 class MSystem:
     """A system of bodies loaded from the reference's initials files and integrated on the GPU."""

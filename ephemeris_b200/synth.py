@@ -384,11 +384,12 @@ def make_ringed_subsystem(seed: int = 6006, n_moons: int = 4, ring_ratio: float 
     return sysm
 
 
-def make_config5(seed: int = 5005, n_particles: int = 2_000_000, j2: float = 2e-4):
+def make_config5(seed: int = 5005, n_particles: int = 2_000_000, j2: float = 2e-4, particle_seed: int | None = None):
     """Massless test particles against 9 perturbers: a star with J2 (static) and J3-J4 (zonal geopotential)
     and 8 planets of the config1 recipe (Newtonian + 1PN). Particles: a ~ U(1.5, 50) AU, e ~ U(0, 0.3),
     i ~ U(0, 20 deg), angles uniform, on heliocentric Kepler orbits shifted to the perturbers' barycentre.
-    Returns (perturber System, particles [6][n]: x, y, z, vx, vy, vz)."""
+    particle_seed: draw the particles from their own generator (shards of one workload share the
+    perturbers and differ in particles). Returns (perturber System, particles [6][n]: x, y, z, vx, vy, vz)."""
     rng = np.random.default_rng(seed)
     star = Body(name="Star", sid="S0", GM=GM_SUN, R_km=6.96e5, inertia=0.07)
     star.j2 = j2
@@ -404,6 +405,8 @@ def make_config5(seed: int = 5005, n_particles: int = 2_000_000, j2: float = 2e-
     sysm = System(bodies=bodies, delta_t=43200.0)
     sysm.geopotentials["S0"] = (4, 0, [(n, 0, rng.normal(0, 1e-6) / n, 0.0) for n in (3, 4)])
     n = n_particles
+    if particle_seed is not None:
+        rng = np.random.default_rng(particle_seed)
     a = rng.uniform(1.5, 50.0, n) * AU
     return sysm, kepler_cloud(rng, GM_SUN, a, rng.uniform(0.0, 0.3, n), rng.uniform(0.0, 20 * DEG, n), star.r, star.v)
 

@@ -140,6 +140,11 @@ int eph_particles_upload(eph_particles *p, int64_t n_pert, const double *pert_pl
 int eph_particles_integrate(eph_particles *p, double dt, int64_t n_step, double *t_eph_hi, double *t_eph_lo);
 /* Perturber planes and/or particle states ([12][n_part]); either pointer may be NULL. */
 int eph_particles_download(eph_particles *p, double *pert_planes, double *part_state);
+/* Issue the set's device work on `stream` (NULL restores its own stream); calls still return only after
+ * their work has finished. */
+int eph_particles_set_stream(eph_particles *p, void *stream);
+/* Kernels launched so far and the summed device time of the particle kernel (CUDA events, ms). */
+int eph_particles_info(const eph_particles *p, int64_t *launches, double *particle_kernel_ms);
 
 /* Limits of eph_integrate_noalloc's fixed scratch (about 2.5 MB of device memory per GPU). */
 #define EPH_NOALLOC_MAX_BODIES 1024
