@@ -48,6 +48,7 @@ FLOP_DEFORM = 90            # tidal/rotational deformation force of i and j
 FLOP_LT = 80
 FLOP_RAD = 10
 FLOP_GP = 250               # per (body, geopotential host), Nz=6/Nt=4
+FLOP_GP_ZONAL = 80          # per (body, geopotential host), J2-J4 zonal only
 FLOP_RING_DISK = 60         # per (body, ring host, disk)
 FLOP_RK = 3900              # RK12 combination + update per body-step
 
@@ -417,20 +418,22 @@ P_CPU_CHUNK = 64   # particles per reference system (with the perturbers as its 
 
 
 def particle_flops_per_step(pl, models):
-    """Algorithmic FLOPs of one RK12 step of one particle against the perturbers (same convention as
-    algorithmic_flops_per_step; a particle feels only the perturbers' side of the deformation and
-    Lense-Thirring terms, so those count half)."""
+    """Algorithmic FLOPs of one RK12 step of one particle against the perturbers, by the convention of
+    algorithmic_flops_per_step: M perturbers x (pass A + 1PN) per stage; a zonal-only geopotential host
+    (J2-J4: its static J2 included) FLOP_GP_ZONAL, a tesseral one FLOP_GP, each ring disk FLOP_RING_DISK;
+    a tidally deformable or spinning perturber adds its side (half) of the deformation and
+    Lense-Thirring terms; FLOP_RK per step."""
     from ephemeris_b200.msystem import P
     m = pl.shape[1]
-    full = 0
+    per_stage = m * (FLOP_PASS_A + FLOP_1PN)
     for j in range(m):
-        f = any(pl[P[k], j] != 0 for k in ("K2", "K2R", "DJ2", "LUM", "RR2G_4C")) or \
-            pl[P["GP_INDEX"], j] >= 0 or pl[P["RING_INDEX"], j] >= 0 or \
-            (pl[P["C_STATIC"]:P["C_STATIC"] + 9, j] != 0).any() or (pl[P["W"]:P["W"] + 3, j] != 0).any() or \
+        tidal_or_spin = pl[P["K2"], j] != 0 or pl[P["K2R"], j] != 0 or (pl[P["W"]:P["W"] + 3, j] != 0).any() or \
             (pl[P["GL_HI"]:P["GL_HI"] + 6, j] != 0).any()
-        full += int(bool(f))
-    per_stage = m * (FLOP_PASS_A + FLOP_1PN) + full * (FLOP_DEFORM + FLOP_LT) // 2
-    per_stage += len(models.gp_nz) * FLOP_GP + int(np.sum(models.ring_ndisk)) * FLOP_RING_DISK
+        per_stage += (FLOP_DEFORM + FLOP_LT) // 2 if tidal_or_spin else 0
+        g = int(pl[P["GP_INDEX"], j])
+        if g >= 0:
+            per_stage += FLOP_GP_ZONAL if models.gp_nt[g] == 0 else FLOP_GP
+    per_stage += int(np.sum(models.ring_ndisk)) * FLOP_RING_DISK
     return 25 * per_stage + FLOP_RK
 
 
@@ -496,6 +499,7 @@ def run_b200_particles(args):
         torch.cuda.set_stream(stream)
         p = Particles(local)
         p.set_stream(stream.cuda_stream)
+        p.set_precision(args.mixed)
         flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
         for _ in range(args.warmup):
             p.upload(pl, md, parts)
@@ -531,6 +535,17 @@ def run_b200_particles(args):
             p.download()
         e2e_s = reduce_max(pg, time.perf_counter() - t0, dev)
         e2e = world * n_part * ks * args.steps / e2e_s
+        mixed_err = None
+        if args.mixed:   # position error of the mixed run against the FP64 run of the same particles
+            _, part_mixed = p.download()
+            p.set_precision(False)
+            p.upload(pl, md, parts)
+            p.integrate(dt, ks)
+            _, part_fp64 = p.download()
+            r_m, r_d = part_mixed[0:3] + part_mixed[3:6], part_fp64[0:3] + part_fp64[3:6]
+            star = pl[0:3, 0] + pl[3:6, 0]
+            mixed_err = float((np.linalg.norm((part_mixed[0:3] - part_fp64[0:3]) + (part_mixed[3:6] - part_fp64[3:6]),
+                                              axis=0) / np.linalg.norm(r_d - star[:, None], axis=0)).max())
         h2d = int(12 * n_part * 8 + pl.nbytes)
         d2h = int(12 * n_part * 8 + pl.nbytes)
         fps = particle_flops_per_step(pl, md)
@@ -546,14 +561,16 @@ def run_b200_particles(args):
             line = {
                 "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64 (double-double state)", "data": "synthetic",
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64 state, f32 1PN terms" if args.mixed else "f64 (double-double state)", "data": "synthetic",
                 "config": {"workload": f"config5: {n_part} massless particles per GPU (a 1.5-50 AU, e < 0.3, "
                                        f"i < 20 deg) against {pl.shape[1]} perturbers (star with J2-J4, 8 planets; "
                                        f"Newtonian + 1PN), dt=0.5 day, {ks} RK12 steps per bench step",
                            "particles": n_part, "perturbers": int(pl.shape[1]), "rk_steps_per_step": ks,
                            "parallelism": f"particles sharded x{world}, perturbers replicated" if world > 1
                            else "1 GPU",
-                           "l2": "flushed between timed steps (256 MB write); particle state 240 MB > L2"},
+                           "l2": "flushed between timed steps (256 MB write); particle state 240 MB > L2",
+                           "precision": "mixed (EIH 1PN in FP32)" if args.mixed else "fp64"},
                 "e2e": {"value": e2e, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
                 "roofline": {"bound": "fp64", "kernel": "particle_kernel", "achieved": achieved, "peak": peak,
                              "unit": "TFLOP/s", "frac": achieved / peak if peak else None, "traffic": None,
@@ -562,6 +579,8 @@ def run_b200_particles(args):
                 "gpu_launches": l1 - l0,
                 "clocks": clk,
             }
+            if mixed_err is not None:
+                line["mixed_vs_fp64_position_error"] = mixed_err
             if cpu is not None:
                 line["cpu_baseline"] = cpu
             print(json.dumps(line), flush=True)
@@ -750,6 +769,7 @@ def main():
     ap.add_argument("--particles", type=int, default=2_000_000, help="config5: massless particles per GPU")
     ap.add_argument("--p-steps", type=int, default=100, help="config5: RK12 steps per bench step")
     ap.add_argument("--p-cpu-steps", type=int, default=300, help="config5: RK12 steps per chunk in the CPU sample")
+    ap.add_argument("--mixed", action="store_true", help="config5: mixed precision (EIH 1PN in FP32)")
     args = ap.parse_args()
     if args.workload == "config5":
         if args.impl == "reference":

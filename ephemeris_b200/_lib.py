@@ -64,6 +64,7 @@ SIGNATURES = [
     ("eph_particles_integrate", ctypes.c_int, [_VP, ctypes.c_double, ctypes.c_int64, _D, _D]),
     ("eph_particles_download", ctypes.c_int, [_VP, _D, _D]),
     ("eph_particles_set_stream", ctypes.c_int, [_VP, _VP]),
+    ("eph_particles_set_precision", ctypes.c_int, [_VP, ctypes.c_int]),
     ("eph_particles_info", ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_double)]),
     ("eph_integrate_noalloc", ctypes.c_int, [ctypes.c_int, _VP, ctypes.c_int64, _VP, ctypes.POINTER(EphModels),
                                              ctypes.c_double, ctypes.c_int64, _D, _D]),

@@ -44,14 +44,13 @@ constexpr int kPThreads = 256;          // particles per CTA
 constexpr int kPMaxPert = 32;           // perturbers (their stage records live in shared memory)
 constexpr size_t kPRecordBytes = 1ull << 30;   // stage records of one round of perturbers then particles
 constexpr double kCP = 299792458.0;     // src/math/basic_math.h:10,18
-constexpr int kPF = 9;                  // stored values per (particle, stage): velocity dd (hi 3, lo 3), acceleration 3
+constexpr int kPF = 3;                  // stored values per (particle, stage): the acceleration
 
-// the nonzero coefficients of the Feagin table, row by row: entries p_nz_off[k-1] .. p_nz_off[k] - 1 of
-// row k (stage k's state) hold j, a_kj (hi, lo) and hi + lo rounded
-constexpr int kPMaxNZ = EPH_RK12_NCOEF;
-__constant__ int p_nz_off[kStages + 1];
-__constant__ int p_nz_j[kPMaxNZ];
-__constant__ double p_nz_hi[kPMaxNZ], p_nz_lo[kPMaxNZ], p_nz_f[kPMaxNZ];
+// The Feagin table as the particle kernel uses it, rows k = 1..25 at k(k-1)/2: a_kj (hi + lo rounded), the
+// second-order rows Abar = A A, and the nodes c_k.
+__constant__ double p_a[EPH_RK12_NCOEF];
+__constant__ double p_abar[EPH_RK12_NCOEF];
+__constant__ double p_c[kStages + 1];
 
 struct PertInfo {
     int gp, ring;   // model indices, or -1
@@ -66,7 +65,7 @@ struct PartArgs {
     const double *traj;         // [1 + kStages * n_step][n_pert][kTrajRec]
     int start_accel;            // 1: form f_0 from record slot 0 (first round); 0: f_0 is in the state
     double *state;              // [15][n_part]: r hi, r lo, v hi, v lo, f
-    double *fstore;             // [gridDim][kStages][kPF][kPThreads]
+    double *fstore;             // [gridDim][kStages][kPF][kPThreads]: stage accelerations
     const PertInfo *info;
     const int *gp_nz, *gp_nt;
     const double *gp_coef;
@@ -105,14 +104,37 @@ __device__ __forceinline__ v3 gp_zonal(const double *__restrict__ c_table, int N
     return mk(g1 * cm, g1 * sm, cphi * tz + sphi * tx);
 }
 
+// Mixed precision: the perturber fields that the FP32 form reads, as floats, kPF32 per perturber.
+constexpr int kPF32 = 8;
+enum F32Field { F_BETA = 0, F_NACC = 3, F_PHI = 6, F_BETA2 = 7, kF32Used = 8 };
+__device__ __forceinline__ int f32_source(int k) {   // TrajField of float field k
+    return k < 3 ? TR_BETA + k : k < 6 ? TR_NACC + (k - 3) : k == 6 ? TR_PHI : TR_BETA2;
+}
+struct f3 { float x, y, z; };
+__device__ __forceinline__ f3 fk(float x, float y, float z) { return f3{x, y, z}; }
+__device__ __forceinline__ f3 tof(v3 a) { return f3{(float)a.x, (float)a.y, (float)a.z}; }
+__device__ __forceinline__ v3 tod(f3 a) { return v3{(double)a.x, (double)a.y, (double)a.z}; }
+__device__ __forceinline__ f3 operator+(f3 a, f3 b) { return f3{a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ f3 operator-(f3 a, f3 b) { return f3{a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ f3 operator*(float s, f3 a) { return f3{s * a.x, s * a.y, s * a.z}; }
+__device__ __forceinline__ f3 &operator+=(f3 &a, f3 b) { a.x += b.x; a.y += b.y; a.z += b.z; return a; }
+__device__ __forceinline__ float dot(f3 a, f3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ f3 cross(f3 a, f3 b) {
+    return f3{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+
 // acceleration of particle (r, v) at the stage whose perturber records are in P. One sweep over the
 // perturbers: pass B's 4 phi_i term (mass.impl:90) is sum_j GM_j/r^3 * 4 phi_i * d = 4 phi_i * a_N,i, so it
 // is added once after the sweep instead of waiting for phi_i; the other terms are the reference's.
 // kGeneral = false: the field loop handles zonal geopotentials only (gp_zonal, inline); true: any model
 // (gp_sum, ring_sum: calls, whose register saves cost the kernel some spilling).
-template <bool kGeneral>
-__device__ __forceinline__ v3 particle_accel(const PartArgs &A, const double *P, const PertInfo *info,
-                                             const dd r[3], const dd v[3]) {
+// kMixed: the EIH 1PN terms in FP32 from the float records Pf (their sum is ~(v/c)^2 ~ 1e-8 of the
+// Newtonian acceleration for solar-system speeds, so FP32 rounding is ~1e-15 of it); the separations, 1/r,
+// the Newtonian terms and the deformation and Lense-Thirring terms (which can reach 1e-3 of the Newtonian
+// acceleration near an oblate planet) stay FP64.
+template <bool kGeneral, bool kMixed>
+__device__ __forceinline__ v3 particle_accel(const PartArgs &A, const double *P, const float *Pf,
+                                             const PertInfo *info, const dd r[3], const dd v[3]) {
     const int np = A.n_pert;
     const double c2 = kCP * kCP;
 #define PR(j, f) P[(j) * kTrajRec + (f)]
@@ -120,6 +142,9 @@ __device__ __forceinline__ v3 particle_accel(const PartArgs &A, const double *P,
     const double beta2 = dot(bi, bi);
     double phi = 0;
     v3 na = mk(0, 0, 0), ga = mk(0, 0, 0), da = mk(0, 0, 0);
+    const f3 bif = tof(bi);
+    const float beta2f = (float)beta2;
+    f3 gaf = fk(0, 0, 0);
 #pragma unroll 1
     for (int j = 0; j < np; ++j) {
         const v3 d = mk(sep_diff(PR(j, TR_R_HI + 0), PR(j, TR_R_LO + 0), r[0].hi, r[0].lo),
@@ -133,16 +158,32 @@ __device__ __forceinline__ v3 particle_accel(const PartArgs &A, const double *P,
         const double tp_dg = rr2 * tp_dphi;
         phi -= tp_dphi;                                            // pass A (mass.impl:38-46)
         na += tp_dg * d;
+        if (kMixed) {
+            const float *Q = Pf + j * kPF32;
+            const f3 df = tof(d);
+            const float tpf = (float)tp_dphi, tgf = (float)tp_dg;
+            const f3 bj = fk(Q[F_BETA + 0], Q[F_BETA + 1], Q[F_BETA + 2]);
+            const float rbj = dot(df, bj);
+            float tp = rbj * (float)rr;
+            tp *= tp;
+            const f3 naj = fk(Q[F_NACC + 0], Q[F_NACC + 1], Q[F_NACC + 2]);
+            const float delta1 = Q[F_PHI] + beta2f + 2 * Q[F_BETA2] - 4 * dot(bif, bj) + (dot(df, naj) - 3 * tp) / 2;
+            const f3 b = bj - bif;
+            gaf += (7 * tpf / 2) * naj + (tgf * delta1) * df + (tgf * (rbj - dot(df, b) * 4)) * b;
+            if (!info[j].full) continue;
+        }
         const v3 bj = mk(PR(j, TR_BETA + 0), PR(j, TR_BETA + 1), PR(j, TR_BETA + 2));
-        const double rbj = dot(d, bj);
-        double tp = rbj * rr;
-        tp *= tp;
-        const v3 naj = mk(PR(j, TR_NACC + 0), PR(j, TR_NACC + 1), PR(j, TR_NACC + 2));
-        const double delta1 = PR(j, TR_PHI) + beta2 + 2 * PR(j, TR_BETA2) - 4 * dot(bi, bj) +
-                              (dot(d, naj) - 3 * tp) / 2;                 // mass.impl:82-97 less 4 phi_i
         const v3 b = bj - bi;
-        ga += (7 * tp_dphi / 2) * naj + (tp_dg * delta1) * d + (tp_dg * (rbj - dot(d, b) * 4)) * b;
-        if (!info[j].full) continue;
+        if (!kMixed) {
+            const double rbj = dot(d, bj);
+            double tp = rbj * rr;
+            tp *= tp;
+            const v3 naj = mk(PR(j, TR_NACC + 0), PR(j, TR_NACC + 1), PR(j, TR_NACC + 2));
+            const double delta1 = PR(j, TR_PHI) + beta2 + 2 * PR(j, TR_BETA2) - 4 * dot(bi, bj) +
+                                  (dot(d, naj) - 3 * tp) / 2;             // mass.impl:82-97 less 4 phi_i
+            ga += (7 * tp_dphi / 2) * naj + (tp_dg * delta1) * d + (tp_dg * (rbj - dot(d, b) * 4)) * b;
+            if (!info[j].full) continue;
+        }
         const double rr3 = rr * rr2;                               // j's deformation and spin (mass.impl:99-125)
         const m3 Cj = m3{mk(PR(j, TR_CPOT + 0), PR(j, TR_CPOT + 1), PR(j, TR_CPOT + 2)),
                          mk(PR(j, TR_CPOT + 3), PR(j, TR_CPOT + 4), PR(j, TR_CPOT + 5)),
@@ -154,6 +195,7 @@ __device__ __forceinline__ v3 particle_accel(const PartArgs &A, const double *P,
         dj += cross(rcr32 * (GLj - (3 * dot(GLj, d) * rr2) * d), b);
         da += dj;
     }
+    if (kMixed) ga = tod(gaf);
     phi = phi / c2;
     ga += (4 * phi) * na;
     na = vdiv(na, c2);
@@ -189,28 +231,39 @@ __device__ __forceinline__ v3 particle_accel(const PartArgs &A, const double *P,
     return (ga + da) + c2 * na;
 }
 
-__device__ __forceinline__ void load_records(const PartArgs &A, double *P, long long slot) {
+template <bool kMixed>
+__device__ __forceinline__ void load_records(const PartArgs &A, double *P, float *Pf, long long slot) {
     const double *src = A.traj + (size_t)slot * A.n_pert * kTrajRec;
     __syncthreads();   // everyone is done with the previous stage's records
     for (int q = threadIdx.x; q < A.n_pert * kTrajRec; q += blockDim.x) P[q] = src[q];
+    if (kMixed)
+        for (int q = threadIdx.x; q < A.n_pert * kF32Used; q += blockDim.x) {
+            const int j = q / kF32Used, k = q % kF32Used;
+            Pf[j * kPF32 + k] = (float)src[j * kTrajRec + f32_source(k)];
+        }
     __syncthreads();
 }
 
-// Per stage, the thread stores (v hi, v lo, f) of its particle to the CTA's slice of the stage store and
-// gathers the earlier stages' values over the nonzero coefficients of the stage's row (p_nz_*). The
-// intermediate stages sum sum_j a_kj v_j and sum_j a_kj f_j in double with fused multiply-adds (v_j by its
-// high part): their rounding reaches the step's result only through the stage accelerations, at about
-// 1e-16 of the stage increment. The last row (the state update) is summed exactly as RungeKutta.impl:
-// 166-186: a_kj v_j in double-double, a_kj f_j rounded term by term.
-template <bool kGeneral>
+// Stage combination in second-order (Runge-Kutta-Nystrom) form. A particle's stage velocities are
+// themselves combinations of its stage accelerations, v_j = v0 + dt sum_l a_jl f_l, so
+//   sum_j a_kj v_j = c_k v0 + dt sum_l Abar_kl f_l,   Abar = A A (strictly lower triangular),
+// and only f_l (3 doubles per stage) is stored: a third of the velocity-and-acceleration store, small enough
+// to stay in L2. Stage k < 25 (dense rows, fused multiply-adds):
+//   r_k = r0 + dt (c_k v0 + dt sum_l Abar_kl f_l),   v_k = v0 + dt sum_l a_kl f_l.
+// The state update (row 25) keeps RungeKutta.impl:166-186's arithmetic where it sets the result's
+// precision: v = v0 + dt sum_j b_j f_j summed term by term in ascending j over nonzero b_j, and
+// r = r0 + dt (sum_j b_j v_j) in double-double with sum_j b_j v_j = c_25 v0 + dt sum_l Abar_25,l f_l. The
+// rearranged sums differ from the reference's in rounding at ~1e-16 of the stage increment.
+template <bool kGeneral, bool kMixed>
 __global__ void __launch_bounds__(kPThreads, 2) particle_kernel(PartArgs A) {
     __shared__ double P[kPMaxPert * kTrajRec];
+    __shared__ float Pf[kMixed ? kPMaxPert * kPF32 : 1];
     __shared__ double X0[12][kPThreads];    // the step's start state: r hi, r lo, v hi, v lo
     __shared__ PertInfo info[kPMaxPert];
     __shared__ int s_blk;
     const int t = threadIdx.x;
     for (int j = t; j < A.n_pert; j += blockDim.x) info[j] = A.info[j];
-    double *F = A.fstore + (size_t)blockIdx.x * kStages * kPF * kPThreads + t;   // [stage][value] stride kPThreads
+    double *F = A.fstore + (size_t)blockIdx.x * kStages * kPF * kPThreads + t;   // [stage][3] stride kPThreads
     const int nb = (A.n_part + kPThreads - 1) / kPThreads;
 #pragma unroll 1
     for (;;) {
@@ -222,8 +275,6 @@ __global__ void __launch_bounds__(kPThreads, 2) particle_kernel(PartArgs A) {
         const int ip = blk * kPThreads + t;
         const bool live = ip < A.n_part;
         const int n = A.n_part;
-        // X0: the step's start state; F stage 0: (v, f) of that state. v_k goes to F[k] as soon as it is
-        // formed, so that only r_k stays in registers across the acceleration.
         dd r[3], v[3];
         v3 fa = mk(0, 0, 0);
         for (int c = 0; c < 3; ++c) {
@@ -231,71 +282,68 @@ __global__ void __launch_bounds__(kPThreads, 2) particle_kernel(PartArgs A) {
             v[c] = live ? dd{A.state[(6 + c) * n + ip], A.state[(9 + c) * n + ip]} : dd_make(0);
             X0[c][t] = r[c].hi; X0[3 + c][t] = r[c].lo;
             X0[6 + c][t] = v[c].hi; X0[9 + c][t] = v[c].lo;
-            F[(size_t)c * kPThreads] = v[c].hi;
-            F[(size_t)(3 + c) * kPThreads] = v[c].lo;
         }
         if (live) fa = mk(A.state[12 * n + ip], A.state[13 * n + ip], A.state[14 * n + ip]);
         if (A.start_accel) {   // f_0 at the start state (the reference's loader runs accel(), mass_loader.cpp:555)
-            load_records(A, P, 0);
-            if (live) fa = particle_accel<kGeneral>(A, P, info, r, v);
+            load_records<kMixed>(A, P, Pf, 0);
+            if (live) fa = particle_accel<kGeneral, kMixed>(A, P, Pf, info, r, v);
         }
-        F[(size_t)6 * kPThreads] = fa.x;
-        F[(size_t)7 * kPThreads] = fa.y;
-        F[(size_t)8 * kPThreads] = fa.z;
+        F[0] = fa.x;
+        F[kPThreads] = fa.y;
+        F[2 * kPThreads] = fa.z;
         const double dt = A.dt;
         const dd ddt = dd_make(dt);
 #pragma unroll 1
         for (long long step = 0; step < A.n_step; ++step) {
 #pragma unroll 1
             for (int s = 0; s < kStages; ++s) {
-                const int e0 = p_nz_off[s], e1 = p_nz_off[s + 1];
+                const int k = s + 1, row = k * (k - 1) / 2;
+                double s1[3] = {0.0, 0.0, 0.0}, s2[3] = {0.0, 0.0, 0.0};
                 double *Fk;
-                if (s + 1 < kStages) {
-                    double sv[3] = {0.0, 0.0, 0.0}, sa[3] = {0.0, 0.0, 0.0};
-#pragma unroll 2
-                    for (int e = e0; e < e1; ++e) {
-                        const double fac = p_nz_f[e];
-                        const double *Fj = F + (size_t)p_nz_j[e] * kPF * kPThreads;
+                if (k < kStages) {
+#pragma unroll 4
+                    for (int l = 0; l < k; ++l) {
+                        const double ab = p_abar[row + l], a = p_a[row + l];
+                        const double *Fl = F + (size_t)l * kPF * kPThreads;
                         for (int c = 0; c < 3; ++c) {
-                            sv[c] = __fma_rn(fac, Fj[(size_t)c * kPThreads], sv[c]);
-                            sa[c] = __fma_rn(fac, Fj[(size_t)(6 + c) * kPThreads], sa[c]);
+                            const double f = Fl[(size_t)c * kPThreads];
+                            s1[c] = __fma_rn(ab, f, s1[c]);
+                            s2[c] = __fma_rn(a, f, s2[c]);
                         }
                     }
-                    Fk = F + (size_t)(s + 1) * kPF * kPThreads;
+                    const double ck = p_c[k];
                     for (int c = 0; c < 3; ++c) {
-                        r[c] = dd_add(dd{X0[c][t], X0[3 + c][t]}, dd_make(dt * sv[c]));
-                        v[c] = dd_add(dd{X0[6 + c][t], X0[9 + c][t]}, dd_make(dt * sa[c]));
+                        r[c] = dd_add(dd{X0[c][t], X0[3 + c][t]}, dd_make(dt * __fma_rn(ck, X0[6 + c][t], dt * s1[c])));
+                        v[c] = dd_add(dd{X0[6 + c][t], X0[9 + c][t]}, dd_make(dt * s2[c]));
                     }
+                    Fk = F + (size_t)k * kPF * kPThreads;
                 } else {
-                    dd sv[3] = {dd_make(0), dd_make(0), dd_make(0)};
-                    double sa[3] = {0.0, 0.0, 0.0};
 #pragma unroll 1
-                    for (int e = e0; e < e1; ++e) {
-                        const dd a = dd{p_nz_hi[e], p_nz_lo[e]};
-                        const double fac = p_nz_f[e];
-                        const double *Fj = F + (size_t)p_nz_j[e] * kPF * kPThreads;
+                    for (int l = 0; l < k; ++l) {
+                        const double ab = p_abar[row + l], a = p_a[row + l];
+                        const double *Fl = F + (size_t)l * kPF * kPThreads;
                         for (int c = 0; c < 3; ++c) {
-                            sv[c] = dd_add(sv[c], dd_mul(a, dd{Fj[(size_t)c * kPThreads], Fj[(size_t)(3 + c) * kPThreads]}));
-                            sa[c] = __dadd_rn(sa[c], __dmul_rn(fac, Fj[(size_t)(6 + c) * kPThreads]));
+                            const double f = Fl[(size_t)c * kPThreads];
+                            s1[c] = __fma_rn(ab, f, s1[c]);
+                            if (a != 0) s2[c] = __dadd_rn(s2[c], __dmul_rn(a, f));
                         }
                     }
-                    Fk = F;   // the new state is stage 0 of the next step
+                    const dd c25 = dd_make(p_c[k]);
                     for (int c = 0; c < 3; ++c) {
-                        r[c] = dd_add(dd{X0[c][t], X0[3 + c][t]}, dd_mul(ddt, sv[c]));
-                        v[c] = dd_add(dd{X0[6 + c][t], X0[9 + c][t]}, dd_make(dt * sa[c]));
+                        const dd v0 = dd{X0[6 + c][t], X0[9 + c][t]};
+                        const dd sv = dd_add(dd_mul(c25, v0), dd_make(dt * s1[c]));
+                        r[c] = dd_add(dd{X0[c][t], X0[3 + c][t]}, dd_mul(ddt, sv));
+                        v[c] = dd_add(v0, dd_make(dt * s2[c]));
                         X0[c][t] = r[c].hi; X0[3 + c][t] = r[c].lo;
                         X0[6 + c][t] = v[c].hi; X0[9 + c][t] = v[c].lo;
                     }
+                    Fk = F;   // the new state is stage 0 of the next step
                 }
-                for (int c = 0; c < 3; ++c) {
-                    Fk[(size_t)c * kPThreads] = v[c].hi;
-                    Fk[(size_t)(3 + c) * kPThreads] = v[c].lo;
-                }
-                load_records(A, P, 1 + step * kStages + s);
-                if (live) fa = particle_accel<kGeneral>(A, P, info, r, v);
-                Fk[(size_t)6 * kPThreads] = fa.x;
-                Fk[(size_t)7 * kPThreads] = fa.y;
-                Fk[(size_t)8 * kPThreads] = fa.z;
+                load_records<kMixed>(A, P, Pf, 1 + step * kStages + s);
+                if (live) fa = particle_accel<kGeneral, kMixed>(A, P, Pf, info, r, v);
+                Fk[0] = fa.x;
+                Fk[kPThreads] = fa.y;
+                Fk[2 * kPThreads] = fa.z;
             }
         }
         if (live) {
@@ -312,29 +360,31 @@ __global__ void __launch_bounds__(kPThreads, 2) particle_kernel(PartArgs A) {
     }
 }
 
+using PartKernel = void (*)(PartArgs);
+PartKernel kernel_of(bool general, bool mixed) {
+    return general ? (mixed ? particle_kernel<true, true> : particle_kernel<true, false>)
+                   : (mixed ? particle_kernel<false, true> : particle_kernel<false, false>);
+}
+
 bool g_part_ready[64];
 cudaError_t particles_setup(int device) {
     if (device >= 0 && device < 64 && g_part_ready[device]) return cudaSuccess;
     double hi[EPH_RK12_NCOEF], lo[EPH_RK12_NCOEF], dtk[kStages + 1];
     rk12_expand(hi, lo, dtk);
-    int off[kStages + 1], nj[kPMaxNZ] = {0};
-    double nh[kPMaxNZ] = {0}, nl[kPMaxNZ] = {0}, nf[kPMaxNZ] = {0};
-    int m = 0;
-    off[0] = 0;
-    for (int k = 1; k <= kStages; ++k) {
-        for (int j = 0; j < k; ++j) {
-            const int ci = k * (k - 1) / 2 + j;
-            if (hi[ci] == 0) continue;   // RungeKutta.impl skips zero coefficients
-            nj[m] = j; nh[m] = hi[ci]; nl[m] = lo[ci]; nf[m] = hi[ci] + lo[ci];
-            ++m;
+    // Abar_kl = sum_{l<j<k} a_kj a_jl, accumulated in long double from the double-double coefficients
+    double a[EPH_RK12_NCOEF], abar[EPH_RK12_NCOEF] = {0};
+    for (int q = 0; q < EPH_RK12_NCOEF; ++q) a[q] = hi[q] + lo[q];
+    for (int k = 1; k <= kStages; ++k)
+        for (int l = 0; l < k; ++l) {
+            long double acc = 0;
+            for (int j = l + 1; j < k; ++j)
+                acc += ((long double)hi[k * (k - 1) / 2 + j] + lo[k * (k - 1) / 2 + j]) *
+                       ((long double)hi[j * (j - 1) / 2 + l] + lo[j * (j - 1) / 2 + l]);
+            abar[k * (k - 1) / 2 + l] = (double)acc;
         }
-        off[k] = m;
-    }
-    cudaError_t e = cudaMemcpyToSymbol(p_nz_off, off, sizeof(off));
-    if (e == cudaSuccess) e = cudaMemcpyToSymbol(p_nz_j, nj, sizeof(nj));
-    if (e == cudaSuccess) e = cudaMemcpyToSymbol(p_nz_hi, nh, sizeof(nh));
-    if (e == cudaSuccess) e = cudaMemcpyToSymbol(p_nz_lo, nl, sizeof(nl));
-    if (e == cudaSuccess) e = cudaMemcpyToSymbol(p_nz_f, nf, sizeof(nf));
+    cudaError_t e = cudaMemcpyToSymbol(p_a, a, sizeof(a));
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(p_abar, abar, sizeof(abar));
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(p_c, dtk, sizeof(dtk));
     if (e == cudaSuccess && device >= 0 && device < 64) g_part_ready[device] = true;
     return e;
 }
@@ -367,6 +417,7 @@ struct eph_particles {
     size_t traj_cap = 0;
     int grid = 0;
     bool general = false;              // a tesseral geopotential or a ring among the perturbers
+    bool mixed = false;                // EPH_PREC_MIXED
 };
 
 static int pfail(eph_particles *p, int code, const char *what, cudaError_t e = cudaSuccess) {
@@ -449,6 +500,13 @@ int eph_particles_set_stream(eph_particles *p, void *stream) {
     return rc;
 }
 
+int eph_particles_set_precision(eph_particles *p, int mode) {
+    if (!p || (mode != EPH_PREC_FP64 && mode != EPH_PREC_MIXED)) return pfail(p, EPH_ERR_ARG, "bad precision mode");
+    std::lock_guard<std::mutex> lock(p->mu);
+    p->mixed = mode == EPH_PREC_MIXED;
+    return EPH_OK;
+}
+
 int eph_particles_info(const eph_particles *p, int64_t *launches, double *particle_kernel_ms) {
     if (!p || !launches || !particle_kernel_ms) return EPH_ERR_ARG;
     *launches = p->launches;
@@ -495,8 +553,8 @@ int eph_particles_upload(eph_particles *p, int64_t n_pert, const double *pert_pl
     p->general = false;
     for (int j = 0; j < n_pert; ++j)
         p->general = p->general || info[j].ring >= 0 || (info[j].gp >= 0 && p->gp_nt[info[j].gp] > 0);
-    PCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, p->general ? particle_kernel<true> : particle_kernel<false>,
-                                                      kPThreads, 0), "occupancy");
+    PCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel_of(p->general, p->mixed), kPThreads, 0),
+        "occupancy");
     PCK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p->device), "SM count");
     const int64_t nblk = (n_part + kPThreads - 1) / kPThreads;
     p->grid = (int)std::max<int64_t>(1, std::min<int64_t>(nblk, (int64_t)per_sm * sms));
@@ -587,8 +645,7 @@ int eph_particles_integrate(eph_particles *p, double dt, int64_t n_step, double 
         A.next = p->d_next;
         PCK(cudaMemsetAsync(p->d_next, 0, sizeof(int), p->stream), "reset queue");
         PCK(cudaEventRecord(p->ev0, p->stream), "event");
-        if (p->general) particle_kernel<true><<<p->grid, kPThreads, 0, p->stream>>>(A);
-        else particle_kernel<false><<<p->grid, kPThreads, 0, p->stream>>>(A);
+        kernel_of(p->general, p->mixed)<<<p->grid, kPThreads, 0, p->stream>>>(A);
         PCK(cudaGetLastError(), "launch particle kernel");
         ++p->launches;
         PCK(cudaEventRecord(p->ev1, p->stream), "event");

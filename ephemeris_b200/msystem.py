@@ -248,6 +248,10 @@ class Particles:
         self._check(self.lib.eph_particles_set_stream(self.h, ctypes.c_void_p(stream) if stream else None),
                     "particles set_stream")
 
+    def set_precision(self, mixed: bool):
+        """FP64 (default) or mixed precision (FP32 relativistic/deformation terms) for the particles."""
+        self._check(self.lib.eph_particles_set_precision(self.h, 1 if mixed else 0), "particles set_precision")
+
     def info(self):
         """(kernels launched, summed particle-kernel device time in ms)."""
         n, ms = ctypes.c_int64(), ctypes.c_double()

@@ -17,6 +17,7 @@ Workloads (sizes from the benchmark definitions; no public dataset is involved):
 """
 from __future__ import annotations
 
+import copy
 import math
 import os
 from dataclasses import dataclass, field
@@ -385,28 +386,25 @@ def make_ringed_subsystem(seed: int = 6006, n_moons: int = 4, ring_ratio: float 
 
 
 def make_config5(seed: int = 5005, n_particles: int = 2_000_000, j2: float = 2e-4, particle_seed: int | None = None):
-    """Massless test particles against 9 perturbers: a star with J2 (static) and J3-J4 (zonal geopotential)
-    and 8 planets of the config1 recipe (Newtonian + 1PN). Particles: a ~ U(1.5, 50) AU, e ~ U(0, 0.3),
-    i ~ U(0, 20 deg), angles uniform, on heliocentric Kepler orbits shifted to the perturbers' barycentre.
-    particle_seed: draw the particles from their own generator (shards of one workload share the
-    perturbers and differ in particles). Returns (perturber System, particles [6][n]: x, y, z, vx, vy, vz)."""
-    rng = np.random.default_rng(seed)
-    star = Body(name="Star", sid="S0", GM=GM_SUN, R_km=6.96e5, inertia=0.07)
+    """Massless test particles against 9 perturbers: the star and the 8 planets of make_config1(1001)
+    (its moons left out, the nine re-centred on their barycentre), the star given a static J2 and a zonal
+    J3-J4 geopotential (coefficients N(0, 1e-6) / n drawn from `seed`); Newtonian + 1PN otherwise.
+    Particles: a ~ U(1.5, 50) AU, e ~ U(0, 0.3), i ~ U(0, 20 deg), angles uniform, on heliocentric Kepler
+    orbits about the star (drawn from `seed`, or from `particle_seed` when given: shards of one workload
+    share the perturbers and differ in particles). Returns (perturber System, particles [6][n]:
+    x, y, z, vx, vy, vz)."""
+    base = make_config1(1001)
+    bodies = [copy.deepcopy(b) for b in base.bodies[:9]]
+    star = bodies[0]
     star.j2 = j2
     star.gp_factor = 1.0
-    bodies = [star]
-    for k in range(8):
-        gm = _loguniform(rng, 1e-9, 1e-3) * GM_SUN
-        a = _loguniform(rng, 0.4, 30.0) * AU
-        r, v = _kepler_state(GM_SUN + gm, a, rng.uniform(0, 0.1), rng.uniform(0, 3 * DEG),
-                             rng.uniform(0, 2 * math.pi), rng.uniform(0, 2 * math.pi), rng.uniform(0, 2 * math.pi))
-        bodies.append(Body(name=f"Planet{k + 1}", sid=f"P{k + 1}", GM=gm, R_km=_radius_km(gm), r=tuple(r), v=tuple(v)))
     _barycentric(bodies)
+    rng = np.random.default_rng(seed)
     sysm = System(bodies=bodies, delta_t=43200.0)
     sysm.geopotentials["S0"] = (4, 0, [(n, 0, rng.normal(0, 1e-6) / n, 0.0) for n in (3, 4)])
-    n = n_particles
     if particle_seed is not None:
         rng = np.random.default_rng(particle_seed)
+    n = n_particles
     a = rng.uniform(1.5, 50.0, n) * AU
     return sysm, kepler_cloud(rng, GM_SUN, a, rng.uniform(0.0, 0.3, n), rng.uniform(0.0, 20 * DEG, n), star.r, star.v)
 

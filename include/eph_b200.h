@@ -143,6 +143,12 @@ int eph_particles_download(eph_particles *p, double *pert_planes, double *part_s
 /* Issue the set's device work on `stream` (NULL restores its own stream); calls still return only after
  * their work has finished. */
 int eph_particles_set_stream(eph_particles *p, void *stream);
+/* Arithmetic of the particles' EIH 1PN terms: EPH_PREC_FP64 (default) or EPH_PREC_MIXED (those terms,
+ * ~1e-8 of the Newtonian acceleration, in FP32; state, separations, Newtonian, deformation, field terms
+ * and the RK12 combination stay FP64 / double-double). Applies from the next integrate. */
+#define EPH_PREC_FP64 0
+#define EPH_PREC_MIXED 1
+int eph_particles_set_precision(eph_particles *p, int mode);
 /* Kernels launched so far and the summed device time of the particle kernel (CUDA events, ms). */
 int eph_particles_info(const eph_particles *p, int64_t *launches, double *particle_kernel_ms);
 

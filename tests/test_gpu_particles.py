@@ -103,3 +103,46 @@ def test_particles_backwards_and_repeat(tmp_path, oracle):
     _check(out, ref, n_pert)
     again, _ = _gpu(pl, md, n_pert, [(dt, -5)])
     assert np.array_equal(out[0:12], again[0:12])
+
+
+def test_mixed_precision_particles(tmp_path, oracle):
+    """EPH_PREC_MIXED (EIH 1PN in FP32) on the particle workload's recipe and on the ringed planet (its
+    general field path): within the FP64 tolerance of the oracle, and within 1e-14 of the FP64 GPU path
+    after 20 steps of 0.5 day."""
+    from ephemeris_b200 import Particles, synth
+    sysm, parts = synth.make_config5(5007, n_particles=300)
+    pl, md, dt, n_pert = _combined(tmp_path, sysm, parts, "mixed")
+    ref = oracle.integrate(pl, _omodels(md), dt, 20)[0]
+    outs = []
+    for mixed in (False, True):
+        p = Particles(0)
+        p.set_precision(mixed)
+        p.upload(np.ascontiguousarray(pl[:, :n_pert]), md, np.ascontiguousarray(pl[0:12, n_pert:]))
+        p.integrate(dt, 20)
+        pert, part = p.download()
+        p.close()
+        out = pl.copy()
+        out[:, :n_pert] = pert
+        out[0:12, n_pert:] = part
+        outs.append(out)
+        _check(out, ref, n_pert)
+    both = [np.concatenate([o[:, :1], o[:, n_pert:]], axis=1) for o in outs]
+    assert position_error(both[1], both[0]) <= 1e-14
+
+    sysm = synth.make_ringed_subsystem(ring_ratio=0.05)
+    host = sysm.bodies[0]
+    rng = np.random.default_rng(6017)
+    a = rng.uniform(2.6, 12.0, 64) * host.R_km * 1e3
+    parts = synth.kepler_cloud(rng, host.GM, a, rng.uniform(0, 0.1, 64), rng.uniform(0, 30 * synth.DEG, 64),
+                               host.r, host.v)
+    pl, md, dt, n_pert = _combined(tmp_path, sysm, parts, "ringed_mixed")
+    ref = oracle.integrate(pl, _omodels(md), dt, 8)[0]
+    p = Particles(0)
+    p.set_precision(True)
+    p.upload(np.ascontiguousarray(pl[:, :n_pert]), md, np.ascontiguousarray(pl[0:12, n_pert:]))
+    p.integrate(dt, 8)
+    pert, part = p.download()
+    out = pl.copy()
+    out[:, :n_pert] = pert
+    out[0:12, n_pert:] = part
+    _check(out, ref, n_pert)
