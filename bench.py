@@ -611,6 +611,183 @@ def run_reference_particles(args):
         print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- config4: serving against a B-spline ephemeris
+DAY = 86400.0
+
+
+def build_serving_ephemeris(args, tmpdir, device=0):
+    """The perturber ephemeris of the serving workload: synth.make_config4_system (419 point masses)
+    integrated on the GPU for --serve-years at dt = 0.5 day (eph_record_samples), each body's 10 channels
+    fitted with cubic B-splines at 1-day knots (eph_bspline_fit). Returns (coefs, gm, sr2, samples0, setup_s)."""
+    from ephemeris_b200 import Context, MSystem, bspline_fit, synth
+    t0 = time.perf_counter()
+    sysm = synth.make_config4_system(4004)
+    ms = MSystem(device)
+    if not ms.load(synth.write_system(sysm, os.path.join(tmpdir, "ephemeris"))):
+        raise RuntimeError("serving perturbers failed to load")
+    pl, md = ms.planes(), ms.models()
+    ms.close()
+    days = int(round(args.serve_years * 365.25))
+    c = Context(device)
+    c.upload(pl, md)
+    samples, _ = c.record_samples(DAY / 2, 2 * days, 1)
+    c.close()
+    coefs = np.stack([bspline_fit(samples[:, j, :], days, 3) for j in range(pl.shape[1])])
+    return coefs, pl[39].copy(), pl[54].copy(), samples[0], time.perf_counter() - t0, sysm
+
+
+def serve_flops_per_particle_step(m):
+    """Useful work of one accepted particle-step: 25 stages x M perturbers x (pass A + 1PN) + the RK
+    update (the step-doubling evaluations and rejected steps are not counted)."""
+    return 25 * m * (FLOP_PASS_A + FLOP_1PN) + FLOP_RK
+
+
+def run_serving_window(srv, reqs, rate, rng):
+    """Open-loop Poisson arrivals at `rate` per second: each request is submitted at its arrival time and
+    collected as soon as it is done. Returns (latencies [s], particle_steps, wall_s, h2d, d2h)."""
+    gaps = rng.exponential(1.0 / rate, len(reqs))
+    arrivals = np.cumsum(gaps) - gaps[0]
+    pending = {}
+    lat, steps, h2d, d2h = [], 0, 0, 0
+    t0 = time.perf_counter()
+    nxt = 0
+    while nxt < len(reqs) or pending:
+        now = time.perf_counter() - t0
+        while nxt < len(reqs) and arrivals[nxt] <= now:
+            parts, t_end = reqs[nxt]
+            rid = srv.submit(parts, 0.0, t_end, tol=1e-13, h0=DAY)
+            pending[rid] = arrivals[nxt]
+            h2d += 12 * parts.shape[1] * 8
+            nxt += 1
+        done = [rid for rid in list(pending) if srv.poll(rid) == 2]
+        for rid in done:
+            out, acc, _ = srv.result(rid)
+            lat.append(time.perf_counter() - t0 - pending.pop(rid))
+            steps += acc
+            d2h += out.nbytes
+        if not done:
+            time.sleep(0.0005)
+    return np.array(lat), steps, time.perf_counter() - t0, h2d, d2h
+
+
+def run_b200_serving(args):
+    import torch
+    from ephemeris_b200 import Server, synth
+    rank, world, local, pg = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    with tempfile.TemporaryDirectory() as td:
+        coefs, gm, sr2, s0, setup_s, sysm = build_serving_ephemeris(args, td, local)
+        m = coefs.shape[0]
+        srv = Server(coefs, gm, DAY, 0.0, 3, sr2, device=local)
+        span = srv.span[1]
+        rng = np.random.default_rng(4004 + rank)
+        mk = lambda count: synth.make_requests(rng, count, span, p_max=args.serve_pmax, years=(1.0, args.serve_years),
+                                               star_r=s0[0, 0:3], star_v=s0[0, 3:6])
+        run_serving_window(srv, mk(max(1, args.warmup)), args.serve_rate, rng)    # warm-up
+        reqs = mk(args.serve_requests)
+        launches0 = srv.info()[0]
+        barrier(pg, dev)
+        clocks = ClockSampler(local)
+        clocks.start()
+        lat, psteps, wall, h2d, d2h = run_serving_window(srv, reqs, args.serve_rate, rng)
+        clk = clocks.stop()
+        launches = srv.info()[0] - launches0
+        wall_max = reduce_max(pg, wall, dev)
+        value = world * psteps / wall_max
+        fps = serve_flops_per_particle_step(m)
+        peak, peak_src = fp64_peak(dev)
+        achieved = fps * psteps / wall / 1e12
+        cpu = None
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            try:
+                cpu = serving_cpu(sysm, s0, args.p_cpu_steps // 10, td)
+            except Exception as exc:
+                cpu = {"value": None, "unit": "particle-steps/s", "cores": 0, "kind": "unavailable", "sample": str(exc)}
+        if rank == 0:
+            sizes = [p.shape[1] for p, _ in reqs]
+            line = {
+                "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": 1,
+                "warmup": args.warmup, "ms_per_step": wall_max * 1e3, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64 (double-double state)", "data": "synthetic",
+                "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                              "max": float(lat.max()), "requests": int(len(lat))},
+                "config": {"workload": f"config4: serving against a {m}-body B-spline ephemeris (config2 recipe, moons "
+                                       f"merged into their hosts; cubic, 1-day knots, {args.serve_years:g} yr), "
+                                       f"Poisson {args.serve_rate:g} requests/s, P = log-U(1, {args.serve_pmax}) "
+                                       f"particles (a 0.5-50 AU, e < 0.6), durations log-U(1, {args.serve_years:g}) yr, "
+                                       f"adaptive RK12 (step doubling) tol 1e-13",
+                           "requests": len(reqs), "particles": int(sum(sizes)), "perturbers": m,
+                           "ephemeris_setup_s": setup_s, "parallelism": f"independent servers x{world}" if world > 1
+                           else "1 GPU, 16 streams",
+                           "note": "value = accepted particle-steps over the wall-clock serving window (arrivals, "
+                                   "queueing, H2D/D2H included)"},
+                "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+                "roofline": {"bound": "fp64", "kernel": "serve_kernel", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                             "frac": achieved / peak if peak else None, "traffic": None, "peak_source": peak_src,
+                             "flops_per_particle_step": fps, "basis": "useful flops of accepted steps over the window"},
+                "gpu_launches": launches,
+                "clocks": clk,
+            }
+            if cpu is not None:
+                line["cpu_baseline"] = cpu
+            print(json.dumps(line), flush=True)
+        srv.close()
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+def serving_cpu(sysm, s0, n_step, tmpdir):
+    """The reference CPU integrator on the serving perturbers: chunks of P_CPU_CHUNK particles (GM = 1e-20
+    bodies, a 0.5-50 AU) with all perturbers in one msystem, fixed steps of 0.5 day, one chunk per process on
+    every host core (the reference has neither B-spline perturbers nor adaptive stepping)."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+    from ephemeris_b200 import synth
+    cores = os.cpu_count() or 1
+    rng = np.random.default_rng(4005)
+    cfgs = []
+    for c in range(cores):
+        parts = synth.kepler_cloud(rng, synth.GM_SUN, rng.uniform(0.5, 50, P_CPU_CHUNK) * synth.AU,
+                                   rng.uniform(0, 0.6, P_CPU_CHUNK), rng.uniform(0, 20 * synth.DEG, P_CPU_CHUNK),
+                                   s0[0, 0:3], s0[0, 3:6])
+        cfgs.append(synth.write_system(synth.with_test_bodies(sysm, parts), os.path.join(tmpdir, f"serve_chunk{c}")))
+    with cf.ProcessPoolExecutor(max_workers=cores, mp_context=mp.get_context("spawn")) as ex:
+        list(ex.map(_ref_chunk, [(c, 1, P_CPU_CHUNK) for c in cfgs]))
+        t0 = time.perf_counter()
+        done = list(ex.map(_ref_chunk, [(c, n_step, P_CPU_CHUNK) for c in cfgs]))
+        el = time.perf_counter() - t0
+    steps = sum(b for b, _ in done)
+    return {"value": steps / el, "unit": "particle-steps/s", "cores": cores, "kind": "reference",
+            "sample": f"{cores} chunks of {P_CPU_CHUNK} particles (GM=1e-20 bodies) + {len(sysm.bodies)} perturbers, "
+                      f"{n_step} fixed RK12 steps of 0.5 day each, reference msystem::integrate(dt,n,0) serial, one chunk "
+                      f"per process on {cores} processes, {el:.1f} s"}
+
+
+def run_reference_serving(args):
+    """--impl reference --workload config4: the reference CPU integrator on chunks of serving particles."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from ephemeris_b200 import synth
+    with tempfile.TemporaryDirectory() as td:
+        sysm = synth.make_config4_system(4004)
+        s0 = np.zeros((len(sysm.bodies), 10))
+        s0[0, 0:3], s0[0, 3:6] = sysm.bodies[0].r, sysm.bodies[0].v
+        vals, cpu = [], None
+        for _ in range(max(1, args.steps)):
+            cpu = serving_cpu(sysm, s0, args.p_cpu_steps // 10, td)
+            vals.append(cpu["value"])
+        value = statistics.median(vals)
+        line = {"metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": args.gpus, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64 (double-double state)", "data": "synthetic", "impl": "reference",
+                "config": {"workload": "config4 serving particles, reference CPU sample (see cpu_baseline.sample)"},
+                "cpu_baseline": dict(cpu, value=value),
+                "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+
+
 def run_b200(args):
     import torch
     from ephemeris_b200 import Context, MSystem
@@ -770,8 +947,17 @@ def main():
     ap.add_argument("--p-steps", type=int, default=100, help="config5: RK12 steps per bench step")
     ap.add_argument("--p-cpu-steps", type=int, default=300, help="config5: RK12 steps per chunk in the CPU sample")
     ap.add_argument("--mixed", action="store_true", help="config5: mixed precision (EIH 1PN in FP32)")
+    ap.add_argument("--serve-years", type=float, default=10.0, help="config4: ephemeris span and longest request")
+    ap.add_argument("--serve-rate", type=float, default=20.0, help="config4: Poisson request rate per second")
+    ap.add_argument("--serve-requests", type=int, default=200, help="config4: requests in the timed window")
+    ap.add_argument("--serve-pmax", type=int, default=4096, help="config4: most particles in a request")
     args = ap.parse_args()
-    if args.workload == "config5":
+    if args.workload == "config4":
+        if args.impl == "reference":
+            run_reference_serving(args)
+        else:
+            run_b200_serving(args)
+    elif args.workload == "config5":
         if args.impl == "reference":
             run_reference_particles(args)
         else:

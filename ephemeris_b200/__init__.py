@@ -5,10 +5,11 @@ Public entry points (mirroring the reference's msystem for the RK12 path):
     Context   - the lower-level C ABI: upload a plane array, rk12 / integrate / accel, download
     Batch     - many independent systems integrated together (ensembles)
     Particles - massless test particles against perturbers
+    Server    - small-body requests (adaptive RK12) against a device B-spline ephemeris
     synth     - seeded synthetic systems written in the reference's initials formats
 """
-from .msystem import MSystem, Context, Batch, Particles, Models, P as PLANES, set_log_level, CPU_RK12, GPU_RK12, COMBINED_RK12
+from .msystem import MSystem, Context, Batch, Particles, Server, bspline_fit, Models, P as PLANES, set_log_level, CPU_RK12, GPU_RK12, COMBINED_RK12
 from ._lib import load_library, EphError, NPLANES, LIB_PATH
 
-__all__ = ["MSystem", "Context", "Batch", "Particles", "Models", "PLANES", "set_log_level", "load_library", "EphError", "NPLANES",
+__all__ = ["MSystem", "Context", "Batch", "Particles", "Server", "bspline_fit", "Models", "PLANES", "set_log_level", "load_library", "EphError", "NPLANES",
            "LIB_PATH", "CPU_RK12", "GPU_RK12", "COMBINED_RK12"]

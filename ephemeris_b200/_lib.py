@@ -16,7 +16,8 @@ GP_TABLE_SIZE = 77
 RING_MAX_DISKS = 64
 
 STATUS = {0: "EPH_OK", 1: "EPH_ERR_ARG", 2: "EPH_ERR_CUDA", 3: "EPH_ERR_OOM", 4: "EPH_ERR_TIMEOUT",
-          5: "EPH_ERR_STATE", 6: "EPH_ERR_LOAD", 7: "EPH_ERR_UNSUPPORTED", 8: "EPH_ERR_LIMIT"}
+          5: "EPH_ERR_STATE", 6: "EPH_ERR_LOAD", 7: "EPH_ERR_UNSUPPORTED", 8: "EPH_ERR_LIMIT",
+          9: "EPH_ERR_STEP"}
 
 # (name, restype, argtypes) of every exported entry point
 _D = ctypes.POINTER(ctypes.c_double)
@@ -66,6 +67,23 @@ SIGNATURES = [
     ("eph_particles_set_stream", ctypes.c_int, [_VP, _VP]),
     ("eph_particles_set_precision", ctypes.c_int, [_VP, ctypes.c_int]),
     ("eph_particles_info", ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_double)]),
+    ("eph_record_samples", ctypes.c_int, [_VP, ctypes.c_double, ctypes.c_int64, ctypes.c_int64, _D, _D, _D]),
+    ("eph_serve_create", ctypes.c_int, [ctypes.c_int, ctypes.c_int64, _D, _D, ctypes.c_int, ctypes.c_int64,
+                                         ctypes.c_double, ctypes.c_double, _D, ctypes.POINTER(_VP)]),
+    ("eph_serve_destroy", ctypes.c_int, [_VP]),
+    ("eph_serve_last_error", ctypes.c_char_p, [_VP]),
+    ("eph_serve_set_budget", ctypes.c_int, [_VP, ctypes.c_int64]),
+    ("eph_serve_set_step_log", ctypes.c_int, [_VP, ctypes.c_int64]),
+    ("eph_serve_submit", ctypes.c_int, [_VP, ctypes.c_int64, _D, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                         ctypes.c_double, ctypes.POINTER(ctypes.c_int64)]),
+    ("eph_serve_poll", ctypes.c_int, [_VP, ctypes.c_int64, ctypes.POINTER(ctypes.c_int)]),
+    ("eph_serve_result", ctypes.c_int, [_VP, ctypes.c_int64, _D, ctypes.POINTER(ctypes.c_int64),
+                                         ctypes.POINTER(ctypes.c_int64), _D, ctypes.POINTER(ctypes.c_int64)]),
+    ("eph_serve_eval", ctypes.c_int, [_VP, ctypes.c_double, _D]),
+    ("eph_serve_info", ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
+                                       ctypes.POINTER(ctypes.c_int64)]),
+    ("eph_bspline_fit", ctypes.c_int, [ctypes.c_int, ctypes.c_int64, ctypes.c_int64, ctypes.c_int, _D, _D]),
+    ("eph_bspline_cheb_coef", ctypes.c_double, [ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     ("eph_integrate_noalloc", ctypes.c_int, [ctypes.c_int, _VP, ctypes.c_int64, _VP, ctypes.POINTER(EphModels),
                                              ctypes.c_double, ctypes.c_int64, _D, _D]),
     ("eph_msystem_load", ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(_VP)]),

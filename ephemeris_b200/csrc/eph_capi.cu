@@ -57,6 +57,7 @@ void ctx_record_stages(eph_ctx *ctx, double *d_buf, long long base) {
     ctx->d_traj = d_buf;
     ctx->traj_base = base;
 }
+long long ctx_size(const eph_ctx *ctx) { return ctx ? (long long)ctx->n : 0; }
 }  // namespace eph
 
 static int fail(eph_ctx *c, int code, const char *what, cudaError_t e = cudaSuccess) {

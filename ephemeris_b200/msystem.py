@@ -81,6 +81,15 @@ class Context:
         check(self.lib.eph_upload_system(self.h, pl.shape[1], _dptr(pl), ctypes.byref(st)), self.h, "upload")
         self.n = pl.shape[1]
 
+    def record_samples(self, dt: float, n_step: int, stride: int, t_eph=(0.0, 0.0)):
+        """Integrate n_step steps, returning (samples [n_step/stride + 1][n][10], t_eph): position,
+        velocity, Newtonian acceleration / c^2, potential / c^2 at the start and every stride steps."""
+        out = np.empty((n_step // stride + 1, self.n, 10))
+        hi, lo = ctypes.c_double(t_eph[0]), ctypes.c_double(t_eph[1])
+        check(self.lib.eph_record_samples(self.h, dt, n_step, stride, ctypes.byref(hi), ctypes.byref(lo), _dptr(out)),
+              self.h, "record_samples")
+        return out, (hi.value, lo.value)
+
     def upload_device(self, d_ptr: int):
         check(self.lib.eph_upload_planes_device(self.h, ctypes.c_void_p(d_ptr)), self.h, "upload_device")
 
@@ -257,6 +266,97 @@ class Particles:
         n, ms = ctypes.c_int64(), ctypes.c_double()
         self._check(self.lib.eph_particles_info(self.h, ctypes.byref(n), ctypes.byref(ms)), "particles info")
         return n.value, ms.value
+
+
+def bspline_fit(samples: np.ndarray, n: int, degree: int = 3) -> np.ndarray:
+    """eph_bspline_fit: samples [mn + 1][channels] at uniform positions -> coefficients [n + degree][channels]."""
+    sm = np.ascontiguousarray(samples, np.float64)
+    if sm.ndim == 1:
+        sm = sm[:, None]
+    out = np.empty((n + degree, sm.shape[1]))
+    check(load_library().eph_bspline_fit(degree, n, sm.shape[0] - 1, sm.shape[1], _dptr(sm), _dptr(out)), None,
+          "bspline_fit")
+    return out
+
+
+class Server:
+    """Small-body serving against a device B-spline ephemeris (eph_serve_* of include/eph_b200.h)."""
+
+    def __init__(self, coefs: np.ndarray, gm, knot: float, t0: float = 0.0, degree: int = 3, sr2=None,
+                 device: int = 0):
+        """coefs: [n_pert][n_intervals + degree][10] (bspline_fit per body of record_samples' channels)."""
+        self.lib = load_library()
+        c = np.ascontiguousarray(coefs, np.float64)
+        g = np.ascontiguousarray(gm, np.float64)
+        s2 = None if sr2 is None else np.ascontiguousarray(sr2, np.float64)
+        self.n_intervals = c.shape[1] - degree
+        self.n_pert = c.shape[0]
+        self.span = (t0, t0 + self.n_intervals * knot)
+        h = ctypes.c_void_p()
+        rc = self.lib.eph_serve_create(device, c.shape[0], _dptr(g), None if s2 is None else _dptr(s2), degree,
+                                       self.n_intervals, t0, knot, _dptr(c), ctypes.byref(h))
+        check(rc, None, "eph_serve_create")
+        self.h = h
+        self.sizes = {}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.eph_serve_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def _check(self, rc, what):
+        if rc:
+            from ._lib import EphError
+            raise EphError(rc, f"{what}: {self.lib.eph_serve_last_error(self.h).decode()}")
+
+    def set_budget(self, nbytes: int):
+        self._check(self.lib.eph_serve_set_budget(self.h, int(nbytes)), "set_budget")
+
+    def set_step_log(self, cap: int):
+        self._check(self.lib.eph_serve_set_step_log(self.h, int(cap)), "set_step_log")
+
+    def submit(self, particles: np.ndarray, t_start: float, t_end: float, tol: float = 1e-13, h0: float = 86400.0) -> int:
+        """particles: [12][n] (position hi, lo; velocity hi, lo) or [6][n]; returns the request id."""
+        pa = np.asarray(particles, np.float64)
+        if pa.shape[0] == 6:
+            z = np.zeros((3, pa.shape[1]))
+            pa = np.concatenate([pa[0:3], z, pa[3:6], z])
+        pa = np.ascontiguousarray(pa)
+        rid = ctypes.c_int64()
+        self._check(self.lib.eph_serve_submit(self.h, pa.shape[1], _dptr(pa), t_start, t_end, tol, h0, ctypes.byref(rid)),
+                    "submit")
+        self.sizes[rid.value] = pa.shape[1]
+        return rid.value
+
+    def poll(self, rid: int) -> int:
+        st = ctypes.c_int()
+        self._check(self.lib.eph_serve_poll(self.h, rid, ctypes.byref(st)), "poll")
+        return st.value
+
+    def result(self, rid: int, log_cap: int = 0):
+        """(particles [12][n], accepted, rejected[, step log]) of a launched request; releases it."""
+        out = np.empty((12, self.sizes.pop(rid)))
+        acc, rej, nl = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        log = np.empty(max(log_cap, 1))
+        rc = self.lib.eph_serve_result(self.h, rid, _dptr(out), ctypes.byref(acc), ctypes.byref(rej),
+                                       _dptr(log) if log_cap else None, ctypes.byref(nl) if log_cap else None)
+        self._check(rc, "result")
+        if log_cap:
+            return out, acc.value, rej.value, log[:nl.value].copy()
+        return out, acc.value, rej.value
+
+    def eval(self, t: float) -> np.ndarray:
+        """The device ephemeris at time t: [n_pert][10]."""
+        out = np.empty((self.n_pert, 10))
+        self._check(self.lib.eph_serve_eval(self.h, t, _dptr(out)), "eval")
+        return out
+
+    def info(self):
+        a, b, c = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        self._check(self.lib.eph_serve_info(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)), "info")
+        return a.value, b.value, c.value
 
 
 class MSystem:

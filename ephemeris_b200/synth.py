@@ -509,3 +509,40 @@ def write_workload(name: str, directory: str, seed: int | None = None, **kw) -> 
     maker = WORKLOADS[name]
     sysm = maker(seed, **kw) if seed is not None else maker(**kw)
     return write_system(sysm, directory)
+
+
+def make_config4_system(seed: int = 4004) -> System:
+    """Perturbers of the serving workload: the config2 recipe (seeded) with every moon merged into its
+    host (GM summed, barycentric position and velocity), all bodies point masses (Newtonian + 1PN).
+    A 1-day-knot B-spline cannot follow a moon's hours-to-days orbit, so the ephemeris carries the
+    planetary (and dwarf) system barycentres, as small-body ephemerides do."""
+    full = make_config2(seed)
+    hosts = [b for b in full.bodies if b.sid[0] in "SPDAKT" and not b.sid.startswith("DM")]
+    moons = [b for b in full.bodies if b.sid.startswith("M") or b.sid.startswith("DM")]
+    groups = {b.sid: [b] for b in hosts}
+    cand = [b for b in hosts if b.sid[0] in "PD"]
+    for m in moons:
+        host = min(cand, key=lambda h: float(np.sum((np.asarray(h.r) - np.asarray(m.r)) ** 2)))
+        groups[host.sid].append(m)
+    bodies = []
+    for h in hosts:
+        g = groups[h.sid]
+        gm = sum(b.GM for b in g)
+        r = sum(b.GM * np.asarray(b.r) for b in g) / gm
+        v = sum(b.GM * np.asarray(b.v) for b in g) / gm
+        bodies.append(Body(name=h.name, sid=h.sid, GM=gm, R_km=h.R_km, inertia=0.4, r=tuple(r), v=tuple(v)))
+    return System(bodies=bodies, delta_t=43200.0)
+
+
+def make_requests(rng, count: int, span: float, p_max: int = 4096, a_range=(0.5, 50.0), e_max: float = 0.6,
+                  inc_max_deg: float = 20.0, years=(1.0, 100.0), star_r=(0.0, 0.0, 0.0), star_v=(0.0, 0.0, 0.0)):
+    """Serving requests: P = round(log-U(1, p_max)) particles with a ~ U(a_range) AU, e ~ U(0, e_max),
+    i ~ U(0, inc_max) on Kepler orbits about the star's state (star_r, star_v) at the ephemeris start, and a
+    duration log-U(years) in years (capped to the span) from that start. Returns [(particles [6][P], t_end)]."""
+    out = []
+    for _ in range(count):
+        p = int(round(_loguniform(rng, 1.0, float(p_max))))
+        a = rng.uniform(*a_range, p) * AU
+        parts = kepler_cloud(rng, GM_SUN, a, rng.uniform(0, e_max, p), rng.uniform(0, inc_max_deg * DEG, p), star_r, star_v)
+        out.append((parts, min(_loguniform(rng, *years) * 365.25 * 86400.0, span)))
+    return out

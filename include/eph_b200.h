@@ -33,7 +33,8 @@ typedef enum eph_status {
     EPH_ERR_STATE = 5,        /* no system uploaded */
     EPH_ERR_LOAD = 6,         /* a config / initials file was missing or malformed */
     EPH_ERR_UNSUPPORTED = 7,  /* requested path is not provided by this library (e.g. a CPU integrator) */
-    EPH_ERR_LIMIT = 8         /* a size beyond the fixed maximum of eph_integrate_noalloc's scratch */
+    EPH_ERR_LIMIT = 8,        /* a size beyond the fixed maximum of eph_integrate_noalloc's scratch */
+    EPH_ERR_STEP = 9          /* adaptive stepping gave up (step below the minimum, or too many attempts) */
 } eph_status;
 
 /* Geopotential and ring tables of a system (layouts in eph_planes.h). Model k of each kind belongs to
@@ -151,6 +152,55 @@ int eph_particles_set_stream(eph_particles *p, void *stream);
 int eph_particles_set_precision(eph_particles *p, int mode);
 /* Kernels launched so far and the summed device time of the particle kernel (CUDA events, ms). */
 int eph_particles_info(const eph_particles *p, int64_t *launches, double *particle_kernel_ms);
+
+/* ---- B-spline ephemeris fit (host; src/math/interp.h:68-150). Fits samples[mn + 1][channels], taken at
+ * uniform positions 0..mn, with n + d degree-d B-splines of unit knot spacing n / mn samples:
+ * coefs[n + d][channels]. Requires 1 <= d <= EPH_BSPLINE_MAX_DEGREE, n >= 1, mn + 1 >= n + d. */
+#define EPH_BSPLINE_MAX_DEGREE 8
+int eph_bspline_fit(int d, int64_t n, int64_t mn, int channels, const double *samples, double *coefs);
+/* c(d, k, j): B[d, x - k] = sum_j c(d,k,j) T_j(2x - 1) on x in [0, 1) (src/math/interp.h:24-30). */
+double eph_bspline_cheb_coef(int d, int k, int j);
+
+/* ---- Ephemeris samples for a B-spline ephemeris (no counterpart in the reference's GPU path; its
+ * generator records states on the host per cadence, src/modules/ephemeris_generator.cpp:128-169).
+ * Integrates n_step steps of dt from t_eph (advanced, msystem::integrate's RK12) and writes the state at
+ * the start and after every `stride` steps (n_step a multiple of stride):
+ * out[n_step / stride + 1][n][EPH_EPHEM_CHANNELS] = position (3), velocity (3), Newtonian acceleration /
+ * c^2 (3), potential / c^2 (1) of every body, in the caller's order, in SI units. */
+#define EPH_EPHEM_CHANNELS 10
+int eph_record_samples(eph_ctx *ctx, double dt, int64_t n_step, int64_t stride, double *t_eph_hi, double *t_eph_lo,
+                       double *out);
+
+/* ---- Serving: massless particles with adaptive RK12 against a device-resident B-spline ephemeris
+ * (no counterpart in the reference). The ephemeris: n_pert bodies (GM, softening sR2 or NULL for none),
+ * each fitted by eph_bspline_fit with degree `degree` on n_intervals knot intervals of `knot` seconds from
+ * t0, EPH_EPHEM_CHANNELS channels: coefs[n_pert][n_intervals + degree][EPH_EPHEM_CHANNELS]. Body 0 is the
+ * central body of the error measure. */
+#define EPH_SERVE_MAX_PERTURBERS 1024
+typedef struct eph_serve eph_serve;
+int eph_serve_create(int device, int64_t n_pert, const double *gm, const double *sr2, int degree, int64_t n_intervals,
+                     double t0, double knot, const double *coefs, eph_serve **out);
+int eph_serve_destroy(eph_serve *s);
+const char *eph_serve_last_error(const eph_serve *s);
+/* Device memory the in-flight requests may hold (default: half the free memory at creation). */
+int eph_serve_set_budget(eph_serve *s, int64_t bytes);
+/* Record up to `cap` accepted step sizes of each later request's first block of particles (0: off). */
+int eph_serve_set_step_log(eph_serve *s, int64_t cap);
+/* Queue a request: part_state[12][n_part] (position hi, lo, velocity hi, lo; copied), integrated from
+ * t_start to t_end (either direction, inside the ephemeris) with tolerance `tol` on the step-doubling
+ * error |r_h - r_h/2| / |r - r_0| and first step h0 > 0 seconds. It launches when its memory fits. */
+int eph_serve_submit(eph_serve *s, int64_t n_part, const double *part_state, double t_start, double t_end, double tol,
+                     double h0, int64_t *id);
+/* state: 0 queued, 1 running, 2 done. Also launches queued requests that now fit. */
+int eph_serve_poll(eph_serve *s, int64_t id, int *state);
+/* Wait for a launched request, copy its particles out ([12][n_part], or NULL), its accepted / rejected
+ * particle-steps and (with a step log) its first block's accepted step sizes; release it. EPH_ERR_STATE if
+ * it is still queued; EPH_ERR_STEP if its stepping gave up (the state is still copied out). */
+int eph_serve_result(eph_serve *s, int64_t id, double *part_state, int64_t *n_accepted, int64_t *n_rejected,
+                     double *step_log, int64_t *n_logged);
+/* The ephemeris on the device at time t: out[n_pert][EPH_EPHEM_CHANNELS] (host). */
+int eph_serve_eval(eph_serve *s, double t, double *out);
+int eph_serve_info(const eph_serve *s, int64_t *launches, int64_t *queued, int64_t *bytes_in_use);
 
 /* Limits of eph_integrate_noalloc's fixed scratch (about 2.5 MB of device memory per GPU). */
 #define EPH_NOALLOC_MAX_BODIES 1024
