@@ -15,6 +15,11 @@ N ranks integrate N independent replicas; value = all ranks' body-steps / max-ov
 
 --impl reference times the reference's own CPU integrator (oracle/_ref, built from the reference
 sources, with its thread pool) on the same workload; without it, the oracle restatement is timed.
+
+Other workloads (--workload): config3 (batched ensemble of 512 systems, eph_batch_*), config4 (serving
+small-body requests against a device B-spline ephemeris, eph_serve_*; Poisson arrivals, p50/p99 latency),
+config5 (2 M massless particles against 9 perturbers, eph_particles_*; --mixed for FP32 1PN terms). Each
+prints the same JSON line with its own unit (body-steps/s or particle-steps/s) and CPU reference arm.
 """
 from __future__ import annotations
 
@@ -719,7 +724,7 @@ def run_b200_serving(args):
                                        f"adaptive RK12 (step doubling) tol 1e-13",
                            "requests": len(reqs), "particles": int(sum(sizes)), "perturbers": m,
                            "ephemeris_setup_s": setup_s, "parallelism": f"independent servers x{world}" if world > 1
-                           else "1 GPU, 16 streams",
+                           else "1 GPU, 128 streams",
                            "note": "value = accepted particle-steps over the wall-clock serving window (arrivals, "
                                    "queueing, H2D/D2H included)"},
                 "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},

@@ -12,8 +12,9 @@
 //   (src/math/interp.h:263-280).
 // * Requests. A request is P particles (double-double position and velocity), a time span and a
 //   tolerance. It runs as one kernel launch of ceil(P G / 256) CTAs on one of the server's streams, G
-//   lanes per particle (G = 32 for P <= 8 down to 1 for P >= 256: small requests split the perturber sweep
-//   over the lanes of a warp, which is what their latency needs). Each CTA integrates its particles with
+//   lanes per particle: the smallest power of two (at most 32) that spreads the request over one block per
+//   SM, so that a request's latency is that of one block's sequential stages (G = 32 below ~1200
+//   particles; 16 at 4096). Each CTA integrates its particles with
 //   a shared adaptive step: one RK12 step of h and two of h/2 (step doubling); the error is the largest
 //   |r_h - r_h/2| / |r_h/2 - r_0| over the CTA's particles (body 0 of the ephemeris is the central star);
 //   a step is accepted when it is at most tol, and the two half steps are kept; the next step is
@@ -437,6 +438,7 @@ struct eph_serve {
     char err[512] = {0};
     cudaStream_t streams[kSStreams] = {};
     int next_stream = 0;
+    int sms = 148;
     int M = 0, Mpad = 0, d = 0;
     long long n = 0;
     double t0 = 0, knot = 0;
@@ -565,6 +567,7 @@ int eph_serve_create(int device, int64_t n_pert, const double *gm, const double 
         (e = cudaMemcpy(s->d_sr2, sr2 ? sr2 : zeros.data(), n_pert * sizeof(double), cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemcpy(s->d_cheb, cheb.data(), cheb.size() * sizeof(double), cudaMemcpyHostToDevice)) != cudaSuccess)
         return bail(EPH_ERR_CUDA, "upload ephemeris", e);
+    cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, device);
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
     s->budget = free_b / 2;
@@ -619,8 +622,10 @@ int eph_serve_submit(eph_serve *s, int64_t n_part, const double *part_state, dou
     SCK(cudaSetDevice(s->device), "cudaSetDevice");
     eph_serve::Req r;
     r.P = (int)n_part;
+    // lanes per particle: split the perturber sweep until the request spans one block per SM (its latency
+    // is one block's sequential stage count), at most a warp per particle
     int G = 1;
-    while (G < 32 && (int64_t)G * 2 * n_part <= kSThreads) G *= 2;
+    while (G < 32 && (n_part * G + kSThreads - 1) / kSThreads < s->sms) G *= 2;
     r.G = G;
     // small requests take a smaller block (whole warps): one warp for a single particle
     r.block = (int)std::min<int64_t>(kSThreads, (n_part * G + 31) / 32 * 32);
