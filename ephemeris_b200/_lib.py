@@ -80,6 +80,8 @@ SIGNATURES = [
     ("eph_serve_result", ctypes.c_int, [_VP, ctypes.c_int64, _D, ctypes.POINTER(ctypes.c_int64),
                                          ctypes.POINTER(ctypes.c_int64), _D, ctypes.POINTER(ctypes.c_int64)]),
     ("eph_serve_eval", ctypes.c_int, [_VP, ctypes.c_double, _D]),
+    ("eph_serve_request_shape", ctypes.c_int, [_VP, ctypes.c_int64, ctypes.POINTER(ctypes.c_int),
+                                                ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     ("eph_serve_info", ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
                                        ctypes.POINTER(ctypes.c_int64)]),
     ("eph_bspline_fit", ctypes.c_int, [ctypes.c_int, ctypes.c_int64, ctypes.c_int64, ctypes.c_int, _D, _D]),

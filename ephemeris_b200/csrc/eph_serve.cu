@@ -731,6 +731,17 @@ int eph_serve_eval(eph_serve *s, double t, double *out) {
     return EPH_OK;
 }
 
+int eph_serve_request_shape(eph_serve *s, int64_t id, int *lanes, int *particles_per_block, int *blocks) {
+    if (!s || !lanes || !particles_per_block || !blocks) return EPH_ERR_ARG;
+    std::lock_guard<std::mutex> lock(s->mu);
+    auto it = s->reqs.find(id);
+    if (it == s->reqs.end()) return sfail(s, EPH_ERR_ARG, "unknown request");
+    *lanes = it->second.G;
+    *particles_per_block = it->second.block / it->second.G;
+    *blocks = it->second.grid;
+    return EPH_OK;
+}
+
 int eph_serve_info(const eph_serve *s, int64_t *launches, int64_t *queued, int64_t *bytes_in_use) {
     if (!s || !launches || !queued || !bytes_in_use) return EPH_ERR_ARG;
     *launches = s->launches;

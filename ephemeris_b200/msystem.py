@@ -347,6 +347,13 @@ class Server:
             return out, acc.value, rej.value, log[:nl.value].copy()
         return out, acc.value, rej.value
 
+    def shape(self, rid: int):
+        """(lanes per particle, particles per block, blocks) of a request."""
+        a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        self._check(self.lib.eph_serve_request_shape(self.h, rid, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)),
+                    "shape")
+        return a.value, b.value, c.value
+
     def eval(self, t: float) -> np.ndarray:
         """The device ephemeris at time t: [n_pert][10]."""
         out = np.empty((self.n_pert, 10))

@@ -198,6 +198,9 @@ int eph_serve_poll(eph_serve *s, int64_t id, int *state);
  * it is still queued; EPH_ERR_STEP if its stepping gave up (the state is still copied out). */
 int eph_serve_result(eph_serve *s, int64_t id, double *part_state, int64_t *n_accepted, int64_t *n_rejected,
                      double *step_log, int64_t *n_logged);
+/* How a request runs: lanes per particle, particles per block (block b holds particles
+ * [b * particles_per_block, ...)), blocks. */
+int eph_serve_request_shape(eph_serve *s, int64_t id, int *lanes, int *particles_per_block, int *blocks);
 /* The ephemeris on the device at time t: out[n_pert][EPH_EPHEM_CHANNELS] (host). */
 int eph_serve_eval(eph_serve *s, double t, double *out);
 int eph_serve_info(const eph_serve *s, int64_t *launches, int64_t *queued, int64_t *bytes_in_use);

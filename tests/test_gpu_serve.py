@@ -7,8 +7,9 @@ eph_bspline_fit. Checks:
 
 * the device evaluation of the ephemeris against the reference's own B-spline sampling
   (src/math/interp.h:263-345, oracle/_ref) at arbitrary times;
-* requests of 5 (32 lanes per particle), 40 (4 lanes) and 300 (one lane, two blocks) particles against the
-  oracle replaying the accepted step sequence (oracle/serve_oracle.py): position within 1e-12 of |r - r_star|.
+* requests of 5 and 300 (32 lanes per particle, 1 and 38 blocks), 4096 (16 lanes) and 40 000 (one lane,
+  157 blocks) particles: the first block's particles against the oracle replaying that block's accepted
+  step sequence (oracle/serve_oracle.py), position within 1e-12 of |r - r_star|; every particle finite.
   A particle that passes within 0.01 AU of a planet (inside its Hill sphere: the 300-particle draw has one
   at 135 000 km from a Jupiter-mass planet) amplifies rounding differences of the two arithmetics by orders
   of magnitude; such particles are held to 1e-9;
@@ -75,18 +76,20 @@ def test_ephemeris_evaluation_matches_reference_sampling(eph):
         assert r_err[1:].max() < 1e-6
 
 
-@pytest.mark.parametrize("n_part", [5, 40, 300])
-def test_request_matches_oracle_replay(eph, oracle, n_part):
+@pytest.mark.parametrize("n_part,lanes", [(5, 32), (300, 32), (4096, 16), (40000, 1)])
+def test_request_matches_oracle_replay(eph, oracle, n_part, lanes):
     from ephemeris_b200 import MSystem, synth
     from oracle.serve_oracle import RefSpline, replay
     parts = _particles(100 + n_part, n_part, eph)
     srv = eph["srv"]
     srv.set_step_log(10000)
     rid = srv.submit(parts, 0.0, 20 * DAY, tol=1e-13, h0=DAY)
+    g, per_block, blocks = srv.shape(rid)
+    assert g == lanes and blocks == -(-n_part // per_block)
     out, acc, rej, steps = srv.result(rid, log_cap=10000)
     srv.set_step_log(0)
-    assert acc >= 3 and len(steps) >= 3 and abs(sum(steps) - 20 * DAY) < 1e-3
-    first = parts[:, :min(n_part, 256)]     # the logged steps are the first block's
+    assert acc >= 3 * n_part and len(steps) >= 3 and abs(sum(steps) - 20 * DAY) < 1e-3
+    first = parts[:, :per_block]            # the logged steps are the first block's
     cfg = synth.write_system(synth.with_test_bodies(eph["sysm"], first), os.path.join(eph["td"], f"comb{n_part}"))
     ms = MSystem(0)
     assert ms.load(cfg)
