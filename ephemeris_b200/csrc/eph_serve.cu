@@ -52,6 +52,7 @@ namespace eph {
 namespace {
 
 constexpr int kSThreads = 256;
+constexpr int kSmemSlots = 64;   // particles per block whose stage store fits shared memory
 constexpr int kSStreams = 128;   // requests in flight at once (the device runs up to 128 kernels concurrently)
 constexpr int kChan = EPH_EPHEM_CHANNELS;   // x y z vx vy vz aN/c^2 (3) phi/c^2
 constexpr double kCS = 299792458.0;         // src/math/basic_math.h:10,18
@@ -80,7 +81,7 @@ struct ServeArgs {
     double t0, knot;
     // request
     double *state;             // [12][P] in place: r hi, r lo, v hi, v lo
-    double *fstore;            // [grid][kStages][3][S]
+    double *fstore;            // [grid][kStages][3][S] (blocks of more than kSmemSlots particles)
     int P, G;
     double t_start, t_end, tol, h0, hmin;
     long long *stats;          // [grid][2]: accepted, rejected
@@ -92,6 +93,49 @@ struct ServeArgs {
 __device__ __forceinline__ double group_sum(double v, int G) {
     for (int o = G >> 1; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
+}
+
+// channel values of all perturbers from the interval's coefficients and the basis values b. D > 0: degree
+// known at compile time, four items per pass with all their coefficient loads issued before any is used
+// (they come from L2); D = 0: any degree, one item at a time.
+template <int D>
+__device__ __forceinline__ void eval_items(const ServeArgs &A, double *PR, const double *b, long long xi) {
+    const int d = D > 0 ? D : A.d;
+    const long long stride = A.n + d;
+    const int total = A.M * kChan;
+    constexpr int U = D > 0 ? 4 : 1;
+    constexpr int NK = D > 0 ? D + 1 : EPH_BSPLINE_MAX_DEGREE + 1;
+#pragma unroll 1
+    for (int item0 = threadIdx.x; item0 < total; item0 += U * blockDim.x) {
+        double cf[U][NK];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int item = item0 + u * blockDim.x;
+            const int it = item < total ? item : total - 1;
+            const double *c = A.coef + ((size_t)(it / kChan) * stride + xi) * kChan + it % kChan;
+            if (D > 0) {
+#pragma unroll
+                for (int k = 0; k < NK; ++k) cf[u][k] = __ldg(c + (size_t)k * kChan);
+            } else {
+                for (int k = 0; k <= d; ++k) cf[u][k] = __ldg(c + (size_t)k * kChan);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int item = item0 + u * blockDim.x;
+            if (item >= total) break;
+            const int body = item / kChan, ch = item % kChan;
+            double v = 0;
+            if (D > 0) {
+#pragma unroll
+                for (int k = 0; k < NK; ++k) v += b[k] * cf[u][k];
+            } else {
+                for (int k = 0; k <= d; ++k) v += b[k] * cf[u][k];
+            }
+            const int row = ch < 3 ? S_RX + ch : ch < 6 ? S_BX + (ch - 3) : ch < 9 ? S_NX + (ch - 6) : S_PHI;
+            PR[row * A.Mpad + body] = (ch >= 3 && ch < 6) ? v / kCS : v;
+        }
+    }
 }
 
 // all perturbers at time t into the shared rows (every thread of the CTA calls it)
@@ -116,19 +160,8 @@ __device__ void eval_perturbers(const ServeArgs &A, double *PR, const double *ch
         }
         b[k] = s;
     }
-    const long long stride = A.n + d;
-    for (int item = threadIdx.x; item < A.M * kChan; item += blockDim.x) {
-        const int body = item / kChan, ch = item % kChan;
-        const double *c = A.coef + ((size_t)body * stride + xi) * kChan + ch;
-        double v = 0;
-#pragma unroll
-        for (int k = 0; k <= EPH_BSPLINE_MAX_DEGREE; ++k) {
-            if (k > d) break;
-            v += b[k] * __ldg(c + (size_t)k * kChan);
-        }
-        const int row = ch < 3 ? S_RX + ch : ch < 6 ? S_BX + (ch - 3) : ch < 9 ? S_NX + (ch - 6) : S_PHI;
-        PR[row * A.Mpad + body] = (ch >= 3 && ch < 6) ? v / kCS : v;
-    }
+    if (d == 3) eval_items<3>(A, PR, b, xi);
+    else eval_items<0>(A, PR, b, xi);
     __syncthreads();
     for (int j = threadIdx.x; j < A.M; j += blockDim.x) {
         const double bx = PR[S_BX * A.Mpad + j], by = PR[S_BY * A.Mpad + j], bz = PR[S_BZ * A.Mpad + j];
@@ -264,7 +297,8 @@ __global__ void __launch_bounds__(kSThreads, 2) serve_kernel(ServeArgs A) {
     double *X0 = PR + kSRows * A.Mpad;        // [12][S]
     double *X1 = X0 + 12 * S;                 // [12][S]
     double *RF = X1 + 12 * S;                 // [6][S]
-    double *F = A.fstore + (size_t)blockIdx.x * kStages * 3 * S + slot;
+    // stage store [kStages][3][S]: shared memory for blocks of up to kSmemSlots particles, else global
+    double *F = (S <= kSmemSlots ? RF + 6 * S : A.fstore + (size_t)blockIdx.x * kStages * 3 * S) + slot;
     const int ip = blockIdx.x * S + slot;
     const bool live = ip < A.P;
     for (int q = threadIdx.x; q < (A.d + 1) * (A.d + 1); q += blockDim.x) cheb[q] = A.cheb[q];
@@ -425,7 +459,9 @@ cudaError_t serve_setup(int device) {
     return e;
 }
 
-size_t serve_smem(int Mpad, int S) { return (size_t)(kSRows * Mpad + 30 * S) * sizeof(double); }
+size_t serve_smem(int Mpad, int S) {
+    return (size_t)(kSRows * Mpad + 30 * S + (S <= kSmemSlots ? kStages * 3 * S : 0)) * sizeof(double);
+}
 
 }  // namespace
 }  // namespace eph
@@ -479,7 +515,7 @@ static int sfail(eph_serve *s, int code, const char *what, cudaError_t e = cudaS
 
 static size_t req_bytes(const eph_serve::Req &r) {
     const int S = r.block / r.G;
-    return (size_t)12 * r.P * sizeof(double) + (size_t)r.grid * kStages * 3 * S * sizeof(double) +
+    return (size_t)12 * r.P * sizeof(double) + (S > kSmemSlots ? (size_t)r.grid * kStages * 3 * S * sizeof(double) : 0) +
            (size_t)r.grid * (2 * sizeof(long long) + sizeof(int)) + (size_t)r.log_cap * sizeof(double);
 }
 
@@ -499,7 +535,9 @@ static int pump(eph_serve *s) {
         cudaStream_t st = s->streams[r.stream];
         SCK(cudaMallocAsync((void **)&r.d_state, (size_t)12 * r.P * sizeof(double), st), "cudaMallocAsync(state)");
         const int S = r.block / r.G;
-        SCK(cudaMallocAsync((void **)&r.d_fstore, (size_t)r.grid * kStages * 3 * S * sizeof(double), st), "cudaMallocAsync(stage store)");
+        if (S > kSmemSlots)
+            SCK(cudaMallocAsync((void **)&r.d_fstore, (size_t)r.grid * kStages * 3 * S * sizeof(double), st),
+                "cudaMallocAsync(stage store)");
         SCK(cudaMallocAsync((void **)&r.d_stats, (size_t)r.grid * 2 * sizeof(long long), st), "cudaMallocAsync(stats)");
         SCK(cudaMallocAsync((void **)&r.d_status, (size_t)r.grid * sizeof(int), st), "cudaMallocAsync(status)");
         if (r.log_cap > 0) SCK(cudaMallocAsync((void **)&r.d_hlog, (size_t)r.log_cap * sizeof(double), st), "cudaMallocAsync(log)");
