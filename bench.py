@@ -623,8 +623,8 @@ DAY = 86400.0
 def build_serving_ephemeris(args, tmpdir, device=0):
     """The perturber ephemeris of the serving workload: synth.make_config4_system (419 point masses)
     integrated on the GPU for --serve-years at dt = 0.5 day (eph_record_samples), each body's 10 channels
-    fitted with cubic B-splines at 1-day knots (eph_bspline_fit). Returns (coefs, gm, sr2, samples0, setup_s)."""
-    from ephemeris_b200 import Context, MSystem, bspline_fit, synth
+    fitted with cubic B-splines at 1-day knots on the GPU (eph_bspline_fit_batch). Returns (coefs, gm, sr2, samples0, setup_s)."""
+    from ephemeris_b200 import Context, MSystem, bspline_fit_batch, synth
     t0 = time.perf_counter()
     sysm = synth.make_config4_system(4004)
     ms = MSystem(device)
@@ -637,7 +637,7 @@ def build_serving_ephemeris(args, tmpdir, device=0):
     c.upload(pl, md)
     samples, _ = c.record_samples(DAY / 2, 2 * days, 1)
     c.close()
-    coefs = np.stack([bspline_fit(samples[:, j, :], days, 3) for j in range(pl.shape[1])])
+    coefs = bspline_fit_batch(np.ascontiguousarray(samples.transpose(1, 0, 2)), days, 3, device)
     return coefs, pl[39].copy(), pl[54].copy(), samples[0], time.perf_counter() - t0, sysm
 
 

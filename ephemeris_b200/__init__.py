@@ -8,8 +8,8 @@ Public entry points (mirroring the reference's msystem for the RK12 path):
     Server    - small-body requests (adaptive RK12) against a device B-spline ephemeris
     synth     - seeded synthetic systems written in the reference's initials formats
 """
-from .msystem import MSystem, Context, Batch, Particles, Server, bspline_fit, Models, P as PLANES, set_log_level, CPU_RK12, GPU_RK12, COMBINED_RK12
+from .msystem import MSystem, Context, Batch, Particles, Server, bspline_fit, bspline_fit_batch, Models, P as PLANES, set_log_level, CPU_RK12, GPU_RK12, COMBINED_RK12
 from ._lib import load_library, EphError, NPLANES, LIB_PATH
 
-__all__ = ["MSystem", "Context", "Batch", "Particles", "Server", "bspline_fit", "Models", "PLANES", "set_log_level", "load_library", "EphError", "NPLANES",
+__all__ = ["MSystem", "Context", "Batch", "Particles", "Server", "bspline_fit", "bspline_fit_batch", "Models", "PLANES", "set_log_level", "load_library", "EphError", "NPLANES",
            "LIB_PATH", "CPU_RK12", "GPU_RK12", "COMBINED_RK12"]

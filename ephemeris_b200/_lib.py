@@ -86,6 +86,8 @@ SIGNATURES = [
                                        ctypes.POINTER(ctypes.c_int64)]),
     ("eph_bspline_fit", ctypes.c_int, [ctypes.c_int, ctypes.c_int64, ctypes.c_int64, ctypes.c_int, _D, _D]),
     ("eph_bspline_cheb_coef", ctypes.c_double, [ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    ("eph_bspline_fit_batch", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int64, ctypes.c_int64, ctypes.c_int,
+                                              ctypes.c_int64, _D, _D]),
     ("eph_integrate_noalloc", ctypes.c_int, [ctypes.c_int, _VP, ctypes.c_int64, _VP, ctypes.POINTER(EphModels),
                                              ctypes.c_double, ctypes.c_int64, _D, _D]),
     ("eph_msystem_load", ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(_VP)]),

@@ -9,6 +9,8 @@
 // Fit (src/math/interp.h:68-150): n + d basis functions B[d, x - i], i = 0..n+d-1, on the sample grid
 // x_j = j n / mn, j = 0..mn; normal equations sum_j B_i(x_j) B_k(x_j) a_k = sum_j B_i(x_j) y_j, each row
 // scaled by 1 / sum_j B_i(x_j), solved by banded LU without pivoting (bandwidth d), all in double-double.
+// The matrix part depends only on the grid (bspline_factor); each data series then takes its right-hand
+// side and the two substitutions, in the reference's operation order.
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -16,6 +18,7 @@
 #include <vector>
 
 #include "../../include/eph_b200.h"
+#include "eph_bspline.h"
 
 namespace {
 
@@ -134,39 +137,43 @@ inline dd mk(double a) { return dd{a, 0}; }
 
 }  // namespace
 
-extern "C" {
+namespace eph {
 
-double eph_bspline_cheb_coef(int d, int k, int j) {
-    if (d < 0 || d > kMaxDeg || k < 0 || k > d || j < 0 || j > d) return 0;
-    return cheb().c[d][k][j];
-}
-
-int eph_bspline_fit(int d, int64_t n, int64_t mn, int channels, const double *samples, double *coefs) {
-    if (d < 1 || d > kMaxDeg || n < 1 || mn + 1 < n + d || channels < 1 || !samples || !coefs) return EPH_ERR_ARG;
+int bspline_factor(int d, int64_t n, int64_t mn, BsplineFactor &f) {
+    if (d < 1 || d > kMaxDeg || n < 1 || mn < 1 || mn + 1 < n + d) return 1;
     const int64_t m = n + d, w = 2 * d + 1;
+    f.d = d; f.n = n; f.mn = mn; f.m = m;
+    f.jmin.assign(m, 0);
+    f.cnt.assign(m, 0);
+    f.J = 0;
+    for (int64_t i = 0; i < m; ++i) {
+        f.jmin[i] = std::max<int64_t>(0, mn * (i - d) + n) / n;
+        const int64_t jmax = std::min<int64_t>(mn, (mn * (i + 1) - 1) / n);
+        f.cnt[i] = (int)std::max<int64_t>(0, jmax - f.jmin[i] + 1);
+        f.J = std::max(f.J, f.cnt[i]);
+    }
+    f.bval.assign((size_t)m * f.J, 0.0);
     std::vector<dd> band((size_t)m * w, mk(0));          // band[i][j - i + d]
-    std::vector<dd> y((size_t)m * channels, mk(0));
     auto A = [&](int64_t i, int64_t j) -> dd & { return band[(size_t)i * w + (j - i + d)]; };
+    std::vector<dd> rw(m);
     const double rmn = 1.0 / (double)mn;
     for (int64_t i = 0; i < m; ++i) {
-        const int64_t jmin = std::max<int64_t>(0, mn * (i - d) + n) / n;
-        const int64_t jmax = std::min<int64_t>(mn, (mn * (i + 1) - 1) / n);
         dd wsum = mk(0);
-        for (int64_t j = jmin; j <= jmax; ++j) {
+        for (int q = 0; q < f.cnt[i]; ++q) {
+            const int64_t j = f.jmin[i] + q;
             const double xj = (double)(j * n) * rmn;
-            const dd b = mk(basis(d, xj - (double)i));
+            const double bij = basis(d, xj - (double)i);
+            f.bval[(size_t)i * f.J + q] = bij;
+            const dd b = mk(bij);
             const int64_t kmin = j * n / mn, kmax = (j * n + mn - 1) / mn + d - 1;
             for (int64_t k = kmin; k <= kmax; ++k)
                 if (k >= 0 && k < m && std::llabs(k - i) <= d) A(i, k) = add(A(i, k), mul(mk(basis(d, xj - (double)k)), b));
-            for (int c = 0; c < channels; ++c)
-                y[(size_t)i * channels + c] = add(y[(size_t)i * channels + c], mul(mk(samples[(size_t)j * channels + c]), b));
             wsum = add(wsum, b);
         }
-        const dd rw = div(mk(1), wsum);
-        for (int64_t k = std::max<int64_t>(0, i - d); k <= std::min<int64_t>(m - 1, i + d); ++k) A(i, k) = mul(A(i, k), rw);
-        for (int c = 0; c < channels; ++c) y[(size_t)i * channels + c] = mul(y[(size_t)i * channels + c], rw);
+        rw[i] = div(mk(1), wsum);
+        for (int64_t k = std::max<int64_t>(0, i - d); k <= std::min<int64_t>(m - 1, i + d); ++k) A(i, k) = mul(A(i, k), rw[i]);
     }
-    // banded LU without pivoting (Doolittle), forward substitution interleaved
+    // banded LU without pivoting (Doolittle)
     for (int64_t i = 0; i < m; ++i) {
         const int64_t lo = std::max<int64_t>(0, i - d), hi = std::min<int64_t>(m - 1, i + d);
         for (int64_t j = lo; j < i; ++j) {
@@ -179,17 +186,55 @@ int eph_bspline_fit(int d, int64_t n, int64_t mn, int channels, const double *sa
             for (int64_t k = std::max<int64_t>(0, j - d); k < i; ++k) s = add(s, mul(A(i, k), A(k, j)));
             A(i, j) = sub(A(i, j), s);
         }
-        for (int64_t k = lo; k < i; ++k)
-            for (int c = 0; c < channels; ++c)
-                y[(size_t)i * channels + c] = sub(y[(size_t)i * channels + c], mul(A(i, k), y[(size_t)k * channels + c]));
     }
-    for (int64_t i = m - 1; i >= 0; --i) {
-        const int64_t hi = std::min<int64_t>(m - 1, i + d);
-        for (int64_t j = i + 1; j <= hi; ++j)
-            for (int c = 0; c < channels; ++c)
-                y[(size_t)i * channels + c] = sub(y[(size_t)i * channels + c], mul(A(i, j), y[(size_t)j * channels + c]));
+    f.rw_hi.resize(m); f.rw_lo.resize(m); f.rd_hi.resize(m); f.rd_lo.resize(m);
+    f.lu_hi.resize((size_t)m * w); f.lu_lo.resize((size_t)m * w);
+    for (int64_t i = 0; i < m; ++i) {
+        f.rw_hi[i] = rw[i].hi; f.rw_lo[i] = rw[i].lo;
         const dd r = div(mk(1), A(i, i));
-        for (int c = 0; c < channels; ++c) y[(size_t)i * channels + c] = mul(y[(size_t)i * channels + c], r);
+        f.rd_hi[i] = r.hi; f.rd_lo[i] = r.lo;
+    }
+    for (size_t q = 0; q < band.size(); ++q) { f.lu_hi[q] = band[q].hi; f.lu_lo[q] = band[q].lo; }
+    return 0;
+}
+
+}  // namespace eph
+
+extern "C" {
+
+double eph_bspline_cheb_coef(int d, int k, int j) {
+    if (d < 0 || d > kMaxDeg || k < 0 || k > d || j < 0 || j > d) return 0;
+    return cheb().c[d][k][j];
+}
+
+int eph_bspline_fit(int d, int64_t n, int64_t mn, int channels, const double *samples, double *coefs) {
+    if (channels < 1 || !samples || !coefs) return EPH_ERR_ARG;
+    eph::BsplineFactor f;
+    if (eph::bspline_factor(d, n, mn, f)) return EPH_ERR_ARG;
+    const int64_t m = f.m, w = 2 * d + 1;
+    std::vector<dd> y((size_t)m * channels);
+    for (int c = 0; c < channels; ++c) {
+        // right-hand side (rows scaled) and forward substitution with L
+        for (int64_t i = 0; i < m; ++i) {
+            dd yi = mk(0);
+            for (int q = 0; q < f.cnt[i]; ++q)
+                yi = add(yi, mul(mk(samples[(size_t)(f.jmin[i] + q) * channels + c]), mk(f.bval[(size_t)i * f.J + q])));
+            yi = mul(yi, dd{f.rw_hi[i], f.rw_lo[i]});
+            for (int64_t k = std::max<int64_t>(0, i - d); k < i; ++k) {
+                const size_t q = (size_t)i * w + (k - i + d);
+                yi = sub(yi, mul(dd{f.lu_hi[q], f.lu_lo[q]}, y[(size_t)k * channels + c]));
+            }
+            y[(size_t)i * channels + c] = yi;
+        }
+        // back substitution with U
+        for (int64_t i = m - 1; i >= 0; --i) {
+            dd yi = y[(size_t)i * channels + c];
+            for (int64_t j = i + 1; j <= std::min<int64_t>(m - 1, i + d); ++j) {
+                const size_t q = (size_t)i * w + (j - i + d);
+                yi = sub(yi, mul(dd{f.lu_hi[q], f.lu_lo[q]}, y[(size_t)j * channels + c]));
+            }
+            y[(size_t)i * channels + c] = mul(yi, dd{f.rd_hi[i], f.rd_lo[i]});
+        }
     }
     for (int64_t i = 0; i < m; ++i)
         for (int c = 0; c < channels; ++c) coefs[(size_t)i * channels + c] = y[(size_t)i * channels + c].hi + y[(size_t)i * channels + c].lo;

@@ -37,6 +37,7 @@
 #include <mutex>
 #include <vector>
 
+#include "eph_bspline.h"
 #include "eph_math.cuh"
 #include "eph_rk12_host.h"
 #include "eph_system.cuh"
@@ -435,6 +436,54 @@ __global__ void gather_samples(const double *traj, int M, int n_take, long long 
     (void)step0;
 }
 
+// Batch B-spline fit: right-hand side and the two banded substitutions of one (series, channel) per
+// thread, with the grid's factorization from bspline_factor (eph_bspline.h). The double-double operations
+// are those of the host fit (eph_bspline.cpp) in the same order, so the coefficients are bit-identical.
+__global__ void bspline_solve_kernel(int d, long long m, int J, int channels, long long n_series, long long series_stride,
+                                     const double *__restrict__ samples, const long long *__restrict__ jmin,
+                                     const int *__restrict__ cnt, const double *__restrict__ bval,
+                                     const double *__restrict__ rw, const double *__restrict__ lu,
+                                     const double *__restrict__ rd, double *__restrict__ y, double *__restrict__ coefs) {
+    const long long T = n_series * channels;
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= T) return;
+    const long long sidx = t / channels;
+    const int c = (int)(t % channels);
+    const int w = 2 * d + 1;
+    const double *smp = samples + sidx * series_stride + c;
+    // y[i] (hi, lo) at y[(2 i) * T + t], y[(2 i + 1) * T + t]
+#pragma unroll 1
+    for (long long i = 0; i < m; ++i) {
+        dd yi = dd_make(0);
+        const long long j0 = jmin[i];
+#pragma unroll 1
+        for (int q = 0; q < cnt[i]; ++q)
+            yi = dd_add(yi, dd_mul(dd_make(smp[(j0 + q) * channels]), dd_make(bval[i * J + q])));
+        yi = dd_mul(yi, dd{rw[2 * i], rw[2 * i + 1]});
+#pragma unroll 1
+        for (long long k = i - d < 0 ? 0 : i - d; k < i; ++k) {
+            const long long qq = i * w + (k - i + d);
+            yi = dd_sub(yi, dd_mul(dd{lu[2 * qq], lu[2 * qq + 1]}, dd{y[(2 * k) * T + t], y[(2 * k + 1) * T + t]}));
+        }
+        y[(2 * i) * T + t] = yi.hi;
+        y[(2 * i + 1) * T + t] = yi.lo;
+    }
+#pragma unroll 1
+    for (long long i = m - 1; i >= 0; --i) {
+        dd yi = dd{y[(2 * i) * T + t], y[(2 * i + 1) * T + t]};
+        const long long hi = i + d < m - 1 ? i + d : m - 1;
+#pragma unroll 1
+        for (long long j = i + 1; j <= hi; ++j) {
+            const long long qq = i * w + (j - i + d);
+            yi = dd_sub(yi, dd_mul(dd{lu[2 * qq], lu[2 * qq + 1]}, dd{y[(2 * j) * T + t], y[(2 * j + 1) * T + t]}));
+        }
+        yi = dd_mul(yi, dd{rd[2 * i], rd[2 * i + 1]});
+        y[(2 * i) * T + t] = yi.hi;
+        y[(2 * i + 1) * T + t] = yi.lo;
+        coefs[(sidx * m + i) * channels + c] = __dadd_rn(yi.hi, yi.lo);
+    }
+}
+
 bool g_serve_ready[64];
 cudaError_t serve_setup(int device) {
     if (device >= 0 && device < 64 && g_serve_ready[device]) return cudaSuccess;
@@ -786,6 +835,65 @@ int eph_serve_info(const eph_serve *s, int64_t *launches, int64_t *queued, int64
     *queued = (int64_t)s->pending.size();
     *bytes_in_use = (int64_t)s->in_use;
     return EPH_OK;
+}
+
+int eph_bspline_fit_batch(int device, int d, int64_t n, int64_t mn, int channels, int64_t n_series,
+                          const double *samples, double *coefs) {
+    if (channels < 1 || n_series < 1 || !samples || !coefs) return EPH_ERR_ARG;
+    eph::BsplineFactor f;
+    if (eph::bspline_factor(d, n, mn, f)) return EPH_ERR_ARG;
+    if (cudaSetDevice(device) != cudaSuccess) return EPH_ERR_ARG;
+    const long long m = f.m, T = n_series * channels, w = 2 * d + 1;
+    auto pack = [](const std::vector<double> &h, const std::vector<double> &l) {
+        std::vector<double> o(2 * h.size());
+        for (size_t i = 0; i < h.size(); ++i) { o[2 * i] = h[i]; o[2 * i + 1] = l[i]; }
+        return o;
+    };
+    const std::vector<double> rw = pack(f.rw_hi, f.rw_lo), lu = pack(f.lu_hi, f.lu_lo), rd = pack(f.rd_hi, f.rd_lo);
+    const size_t n_smp = (size_t)n_series * (mn + 1) * channels, n_coef = (size_t)n_series * m * channels;
+    double *d_smp = nullptr, *d_coef = nullptr, *d_y = nullptr, *d_bval = nullptr, *d_rw = nullptr, *d_lu = nullptr, *d_rd = nullptr;
+    long long *d_jmin = nullptr;
+    int *d_cnt = nullptr;
+    int rc = EPH_OK;
+    cudaError_t e = cudaSuccess;
+    auto alloc = [&](void **p, size_t bytes) {
+        if (e == cudaSuccess) e = cudaMalloc(p, bytes);
+    };
+    alloc((void **)&d_smp, n_smp * sizeof(double));
+    alloc((void **)&d_coef, n_coef * sizeof(double));
+    alloc((void **)&d_y, (size_t)2 * m * T * sizeof(double));
+    alloc((void **)&d_bval, f.bval.size() * sizeof(double));
+    alloc((void **)&d_rw, rw.size() * sizeof(double));
+    alloc((void **)&d_lu, lu.size() * sizeof(double));
+    alloc((void **)&d_rd, rd.size() * sizeof(double));
+    alloc((void **)&d_jmin, f.jmin.size() * sizeof(long long));
+    alloc((void **)&d_cnt, f.cnt.size() * sizeof(int));
+    if (e != cudaSuccess) rc = e == cudaErrorMemoryAllocation ? EPH_ERR_OOM : EPH_ERR_CUDA;
+    if (!rc) {
+        std::vector<long long> jm(f.jmin.begin(), f.jmin.end());
+        if ((e = cudaMemcpy(d_smp, samples, n_smp * sizeof(double), cudaMemcpyHostToDevice)) != cudaSuccess ||
+            (e = cudaMemcpy(d_bval, f.bval.data(), f.bval.size() * sizeof(double), cudaMemcpyHostToDevice)) != cudaSuccess ||
+            (e = cudaMemcpy(d_rw, rw.data(), rw.size() * sizeof(double), cudaMemcpyHostToDevice)) != cudaSuccess ||
+            (e = cudaMemcpy(d_lu, lu.data(), lu.size() * sizeof(double), cudaMemcpyHostToDevice)) != cudaSuccess ||
+            (e = cudaMemcpy(d_rd, rd.data(), rd.size() * sizeof(double), cudaMemcpyHostToDevice)) != cudaSuccess ||
+            (e = cudaMemcpy(d_jmin, jm.data(), jm.size() * sizeof(long long), cudaMemcpyHostToDevice)) != cudaSuccess ||
+            (e = cudaMemcpy(d_cnt, f.cnt.data(), f.cnt.size() * sizeof(int), cudaMemcpyHostToDevice)) != cudaSuccess)
+            rc = EPH_ERR_CUDA;
+    }
+    if (!rc) {
+        const int threads = 128;
+        bspline_solve_kernel<<<(unsigned)((T + threads - 1) / threads), threads>>>(
+            d, m, f.J, channels, n_series, (long long)(mn + 1) * channels, d_smp, d_jmin, d_cnt, d_bval, d_rw, d_lu, d_rd,
+            d_y, d_coef);
+        if ((e = cudaGetLastError()) != cudaSuccess ||
+            (e = cudaMemcpy(coefs, d_coef, n_coef * sizeof(double), cudaMemcpyDeviceToHost)) != cudaSuccess)
+            rc = EPH_ERR_CUDA;
+    }
+    for (void *p : {(void *)d_smp, (void *)d_coef, (void *)d_y, (void *)d_bval, (void *)d_rw, (void *)d_lu, (void *)d_rd,
+                    (void *)d_jmin, (void *)d_cnt})
+        if (p) cudaFree(p);
+    (void)w;
+    return rc;
 }
 
 // Ephemeris samples from a context: integrates n_step steps of dt from t_eph (advanced), and writes the

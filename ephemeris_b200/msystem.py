@@ -279,6 +279,16 @@ def bspline_fit(samples: np.ndarray, n: int, degree: int = 3) -> np.ndarray:
     return out
 
 
+def bspline_fit_batch(samples: np.ndarray, n: int, degree: int = 3, device: int = 0) -> np.ndarray:
+    """eph_bspline_fit_batch: samples [series][mn + 1][channels] -> coefficients [series][n + degree][channels],
+    solved on the GPU, bit-identical to bspline_fit per series."""
+    sm = np.ascontiguousarray(samples, np.float64)
+    out = np.empty((sm.shape[0], n + degree, sm.shape[2]))
+    check(load_library().eph_bspline_fit_batch(device, degree, n, sm.shape[1] - 1, sm.shape[2], sm.shape[0], _dptr(sm),
+                                               _dptr(out)), None, "bspline_fit_batch")
+    return out
+
+
 class Server:
     """Small-body serving against a device B-spline ephemeris (eph_serve_* of include/eph_b200.h)."""
 

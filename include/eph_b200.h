@@ -158,6 +158,11 @@ int eph_particles_info(const eph_particles *p, int64_t *launches, double *partic
  * coefs[n + d][channels]. Requires 1 <= d <= EPH_BSPLINE_MAX_DEGREE, n >= 1, mn + 1 >= n + d. */
 #define EPH_BSPLINE_MAX_DEGREE 8
 int eph_bspline_fit(int d, int64_t n, int64_t mn, int channels, const double *samples, double *coefs);
+/* The same fit for n_series series on one sample grid, solved on `device` (one thread per series and
+ * channel; the grid's matrix is factored once on the host): samples[n_series][mn + 1][channels] ->
+ * coefs[n_series][n + d][channels] (host arrays). Bit-identical to eph_bspline_fit series by series. */
+int eph_bspline_fit_batch(int device, int d, int64_t n, int64_t mn, int channels, int64_t n_series,
+                          const double *samples, double *coefs);
 /* c(d, k, j): B[d, x - k] = sum_j c(d,k,j) T_j(2x - 1) on x in [0, 1) (src/math/interp.h:24-30). */
 double eph_bspline_cheb_coef(int d, int k, int j);
 

@@ -155,3 +155,18 @@ def test_backward_request_and_refusals(eph):
         srv.submit(parts, 0.0, (eph["days"] + 1) * DAY)
     with pytest.raises(EphError):
         srv.submit(parts, 0.0, DAY, tol=0.0)
+
+
+@pytest.mark.parametrize("d,n,mn", [(3, 60, 120), (1, 20, 20), (5, 200, 1000), (8, 200, 1000)])
+def test_batch_fit_on_device_is_bit_identical(eph, d, n, mn):
+    """eph_bspline_fit_batch (one GPU thread per series and channel) against eph_bspline_fit (host)."""
+    from ephemeris_b200 import bspline_fit, bspline_fit_batch
+    rng = np.random.default_rng(d * 1000 + n)
+    i = np.arange(mn + 1)
+    series = [np.stack([np.sin(i * 0.1), np.cos(i * 0.1)], 1), rng.normal(0, 1e11, (mn + 1, 2))]
+    if (n, mn) == (60, 120):
+        series += [eph["samples"][:, j, 0:2] for j in range(3)]
+    sm = np.stack(series)
+    got = bspline_fit_batch(sm, n, d)
+    for k in range(len(series)):
+        assert np.array_equal(got[k], bspline_fit(series[k], n, d)), k
