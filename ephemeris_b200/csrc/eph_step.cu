@@ -1264,10 +1264,14 @@ __device__ void rk_stage(const SysDev &S, Own *own, int nb, int s, long long i_s
         __syncwarp();
         if (lane < 9) o.s[lane] = o.s0[lane];
         __syncwarp();
-        const v3 wv = ldv(o.wnew), dwv = ldv(o.dw);
+        const v3 wv = ldv(o.wnew), dwv = ldv(o.dw), eg = ldv(o.Egrad);
+        // A body that does not rotate (w, its stage change and Egrad all exactly zero) has zero rotation
+        // increments R (rotation_matrix of a zero vector), so its frame keeps s0 exactly: skip the passes.
+        const bool still = wv.x == 0 && wv.y == 0 && wv.z == 0 && dwv.x == 0 && dwv.y == 0 && dwv.z == 0 &&
+                           (k != kStages || (eg.x == 0 && eg.y == 0 && eg.z == 0));
         // s += R % fast(s), element (col, row) = sum_m R[m][row] * s[col][m]
         #pragma unroll 1
-        for (int pass = 0; pass < (k == kStages ? 3 : 2); ++pass) {
+        for (int pass = 0; pass < (still ? 0 : (k == kStages ? 3 : 2)); ++pass) {
             m3 R = pass == 0 ? rotation_matrix(wv - dwv, dt * dt_k / 2)
                  : pass == 1 ? rotation_matrix(wv + dwv, dt * dt_k / 2)
                              : rotation_matrix(ldv(o.Egrad), 1.0 / 72);
