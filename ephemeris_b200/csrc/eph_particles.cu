@@ -145,7 +145,7 @@ __device__ __forceinline__ v3 particle_accel(const PartArgs &A, const double *P,
     const f3 bif = tof(bi);
     const float beta2f = (float)beta2;
     f3 gaf = fk(0, 0, 0);
-#pragma unroll 1
+#pragma unroll 2
     for (int j = 0; j < np; ++j) {
         const v3 d = mk(sep_diff(PR(j, TR_R_HI + 0), PR(j, TR_R_LO + 0), r[0].hi, r[0].lo),
                         sep_diff(PR(j, TR_R_HI + 1), PR(j, TR_R_LO + 1), r[1].hi, r[1].lo),
