@@ -415,8 +415,7 @@ __global__ void __launch_bounds__(kSThreads) eval_kernel(ServeArgs A, double t, 
 }
 
 // step-end stage records of sampled steps into [samples][M][kChan]
-__global__ void gather_samples(const double *traj, int M, int n_take, long long first_step, int stride, long long step0,
-                               double *out) {
+__global__ void gather_samples(const double *traj, int M, int n_take, long long first_step, int stride, double *out) {
     // sample q of this chunk is the end of local step (first_step + q * stride); its record slot is
     // 1 + local_step * kStages + (kStages - 1)
     const long long total = (long long)n_take * M;
@@ -433,7 +432,6 @@ __global__ void gather_samples(const double *traj, int M, int n_take, long long 
         }
         o[9] = rec[TR_PHI];
     }
-    (void)step0;
 }
 
 // Batch B-spline fit: right-hand side and the two banded substitutions of one (series, channel) per
@@ -843,7 +841,7 @@ int eph_bspline_fit_batch(int device, int d, int64_t n, int64_t mn, int channels
     eph::BsplineFactor f;
     if (eph::bspline_factor(d, n, mn, f)) return EPH_ERR_ARG;
     if (cudaSetDevice(device) != cudaSuccess) return EPH_ERR_ARG;
-    const long long m = f.m, T = n_series * channels, w = 2 * d + 1;
+    const long long m = f.m, T = n_series * channels;
     auto pack = [](const std::vector<double> &h, const std::vector<double> &l) {
         std::vector<double> o(2 * h.size());
         for (size_t i = 0; i < h.size(); ++i) { o[2 * i] = h[i]; o[2 * i + 1] = l[i]; }
@@ -892,7 +890,6 @@ int eph_bspline_fit_batch(int device, int d, int64_t n, int64_t mn, int channels
     for (void *p : {(void *)d_smp, (void *)d_coef, (void *)d_y, (void *)d_bval, (void *)d_rw, (void *)d_lu, (void *)d_rd,
                     (void *)d_jmin, (void *)d_cnt})
         if (p) cudaFree(p);
-    (void)w;
     return rc;
 }
 
@@ -940,7 +937,7 @@ int eph_record_samples(eph_ctx *ctx, double dt, int64_t n_step, int64_t stride, 
         ctx_record_stages(ctx, nullptr, 0);
         if (rc) break;
         const int take = (int)(c / stride);
-        gather_samples<<<256, 256>>>(d_traj, (int)n, take, stride - 1, (int)stride, done, d_out);
+        gather_samples<<<256, 256>>>(d_traj, (int)n, take, stride - 1, (int)stride, d_out);
         cudaError_t e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaMemcpy(out + (size_t)written * n * kChan, d_out, (size_t)take * n * kChan * sizeof(double),
                                              cudaMemcpyDeviceToHost);
