@@ -119,9 +119,6 @@ __device__ __forceinline__ f3 operator-(f3 a, f3 b) { return f3{a.x - b.x, a.y -
 __device__ __forceinline__ f3 operator*(float s, f3 a) { return f3{s * a.x, s * a.y, s * a.z}; }
 __device__ __forceinline__ f3 &operator+=(f3 &a, f3 b) { a.x += b.x; a.y += b.y; a.z += b.z; return a; }
 __device__ __forceinline__ float dot(f3 a, f3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
-__device__ __forceinline__ f3 cross(f3 a, f3 b) {
-    return f3{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
-}
 
 // acceleration of particle (r, v) at the stage whose perturber records are in P. One sweep over the
 // perturbers: pass B's 4 phi_i term (mass.impl:90) is sum_j GM_j/r^3 * 4 phi_i * d = 4 phi_i * a_N,i, so it
