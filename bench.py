@@ -530,19 +530,23 @@ def run_b200_particles(args):
         kern_ms = (k1 - k0) / part_launches
         dev_ms_max = reduce_max(pg, dev_ms, dev)
         value = world * n_part * ks * args.steps / (dev_ms_max / 1e3)
-        # end to end through the public API: host particles up, integrate, host particles down
-        pin = torch.from_numpy(np.ascontiguousarray(parts)).pin_memory().numpy()
+        # end to end through the public API: host particles up, integrate, host particles down (pinned
+        # host buffers: the state as double-double rows, as the API takes and returns it)
+        z = np.zeros((3, n_part))
+        pin = torch.from_numpy(np.concatenate([parts[0:3], z, parts[3:6], z])).pin_memory().numpy()
+        pin_out = torch.empty((12, n_part), dtype=torch.float64).pin_memory().numpy()
+        pl_out = np.empty_like(pl)
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
         for _ in range(args.steps):
             p.upload(pl, md, pin)
             p.integrate(dt, ks)
-            p.download()
+            p.download(pl_out, pin_out)
         e2e_s = reduce_max(pg, time.perf_counter() - t0, dev)
         e2e = world * n_part * ks * args.steps / e2e_s
         mixed_err = None
         if args.mixed:   # position error of the mixed run against the FP64 run of the same particles
-            _, part_mixed = p.download()
+            part_mixed = pin_out.copy()
             p.set_precision(False)
             p.upload(pl, md, parts)
             p.integrate(dt, ks)

@@ -413,6 +413,8 @@ struct eph_particles {
     PertInfo *d_info = nullptr;
     size_t traj_cap = 0;
     int grid = 0;
+    int64_t cap_part = 0, cap_pert = 0;  // sizes the device buffers hold
+    int cap_grid = 0, cap_gp = 0, cap_ring = 0;
     bool general = false;              // a tesseral geopotential or a ring among the perturbers
     bool mixed = false;                // EPH_PREC_MIXED
 };
@@ -440,6 +442,8 @@ static void part_free(eph_particles *p) {
     p->d_gp_coef = p->d_ring_disk = nullptr;
     p->d_info = nullptr;
     p->traj_cap = 0;
+    p->cap_part = p->cap_pert = 0;
+    p->cap_grid = p->cap_gp = p->cap_ring = 0;
 }
 
 // t += d in double-double (mass.cpp:441)
@@ -519,7 +523,6 @@ int eph_particles_upload(eph_particles *p, int64_t n_pert, const double *pert_pl
     PCK(cudaSetDevice(p->device), "cudaSetDevice");
     int rc = eph_upload_system(p->ctx, n_pert, pert_planes, models);
     if (rc) return pfail(p, rc, eph_last_error(p->ctx));
-    part_free(p);
     p->n_pert = n_pert;
     p->n_part = n_part;
     p->h_pert.assign(pert_planes, pert_planes + (size_t)EPH_NPLANES * n_pert);
@@ -543,9 +546,6 @@ int eph_particles_upload(eph_particles *p, int64_t n_pert, const double *pert_pl
         info[j].full = full;
         info[j].pad = 0;
     }
-    // particle state: r hi, r lo, v hi, v lo as given, then f (formed at the first integration)
-    std::vector<double> st((size_t)15 * n_part, 0.0);
-    std::copy(part_state, part_state + (size_t)12 * n_part, st.begin());
     int per_sm = 0, sms = 0;
     p->general = false;
     for (int j = 0; j < n_pert; ++j)
@@ -555,16 +555,32 @@ int eph_particles_upload(eph_particles *p, int64_t n_pert, const double *pert_pl
     PCK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p->device), "SM count");
     const int64_t nblk = (n_part + kPThreads - 1) / kPThreads;
     p->grid = (int)std::max<int64_t>(1, std::min<int64_t>(nblk, (int64_t)per_sm * sms));
-    PCK(cudaMalloc(&p->d_state, st.size() * sizeof(double)), "cudaMalloc(particles)");
-    PCK(cudaMalloc(&p->d_fstore, (size_t)p->grid * kStages * kPF * kPThreads * sizeof(double)), "cudaMalloc(stage store)");
-    PCK(cudaMalloc(&p->d_info, n_pert * sizeof(PertInfo)), "cudaMalloc(perturbers)");
-    PCK(cudaMalloc(&p->d_next, sizeof(int)), "cudaMalloc(queue)");
-    PCK(cudaMalloc(&p->d_gp_nz, std::max(n_gp, 1) * sizeof(int)), "cudaMalloc(gp)");
-    PCK(cudaMalloc(&p->d_gp_nt, std::max(n_gp, 1) * sizeof(int)), "cudaMalloc(gp)");
-    PCK(cudaMalloc(&p->d_gp_coef, (size_t)std::max(n_gp, 1) * EPH_GP_TABLE_SIZE * sizeof(double)), "cudaMalloc(gp)");
-    PCK(cudaMalloc(&p->d_ring_nd, std::max(n_ring, 1) * sizeof(int)), "cudaMalloc(ring)");
-    PCK(cudaMalloc(&p->d_ring_disk, (size_t)std::max(n_ring, 1) * EPH_RING_MAX_DISKS * 3 * sizeof(double)), "cudaMalloc(ring)");
-    PCK(cudaMemcpy(p->d_state, st.data(), st.size() * sizeof(double), cudaMemcpyHostToDevice), "upload particles");
+    // device buffers are kept across uploads while they are large enough (a repeated upload of the same
+    // sizes allocates nothing)
+    if (n_part > p->cap_part || p->grid > p->cap_grid || n_pert > p->cap_pert || std::max(n_gp, 1) > p->cap_gp ||
+        std::max(n_ring, 1) > p->cap_ring) {
+        part_free(p);
+        p->cap_part = n_part;
+        p->cap_grid = p->grid;
+        p->cap_pert = n_pert;
+        p->cap_gp = std::max(n_gp, 1);
+        p->cap_ring = std::max(n_ring, 1);
+        PCK(cudaMalloc(&p->d_state, (size_t)15 * n_part * sizeof(double)), "cudaMalloc(particles)");
+        PCK(cudaMalloc(&p->d_fstore, (size_t)p->grid * kStages * kPF * kPThreads * sizeof(double)), "cudaMalloc(stage store)");
+        PCK(cudaMalloc(&p->d_info, n_pert * sizeof(PertInfo)), "cudaMalloc(perturbers)");
+        PCK(cudaMalloc(&p->d_next, sizeof(int)), "cudaMalloc(queue)");
+        PCK(cudaMalloc(&p->d_gp_nz, p->cap_gp * sizeof(int)), "cudaMalloc(gp)");
+        PCK(cudaMalloc(&p->d_gp_nt, p->cap_gp * sizeof(int)), "cudaMalloc(gp)");
+        PCK(cudaMalloc(&p->d_gp_coef, (size_t)p->cap_gp * EPH_GP_TABLE_SIZE * sizeof(double)), "cudaMalloc(gp)");
+        PCK(cudaMalloc(&p->d_ring_nd, p->cap_ring * sizeof(int)), "cudaMalloc(ring)");
+        PCK(cudaMalloc(&p->d_ring_disk, (size_t)p->cap_ring * EPH_RING_MAX_DISKS * 3 * sizeof(double)), "cudaMalloc(ring)");
+    }
+    // particle state [15][n_part]: r hi, r lo, v hi, v lo straight from the caller's rows (a pinned caller
+    // buffer is a DMA), then f, formed at the first integration
+    PCK(cudaMemcpyAsync(p->d_state, part_state, (size_t)12 * n_part * sizeof(double), cudaMemcpyHostToDevice, p->stream),
+        "upload particles");
+    PCK(cudaMemsetAsync(p->d_state + (size_t)12 * n_part, 0, (size_t)3 * n_part * sizeof(double), p->stream), "clear f");
+    PCK(cudaStreamSynchronize(p->stream), "upload particles");
     PCK(cudaMemcpy(p->d_info, info.data(), n_pert * sizeof(PertInfo), cudaMemcpyHostToDevice), "upload perturbers");
     if (n_gp) {
         PCK(cudaMemcpy(p->d_gp_nz, p->gp_nz.data(), n_gp * sizeof(int), cudaMemcpyHostToDevice), "upload gp");
@@ -672,9 +688,11 @@ int eph_particles_download(eph_particles *p, double *pert_planes, double *part_s
         const int rc = eph_download_system(p->ctx, pert_planes);
         if (rc) return pfail(p, rc, eph_last_error(p->ctx));
     }
-    if (part_state)
-        PCK(cudaMemcpy(part_state, p->d_state, (size_t)12 * p->n_part * sizeof(double), cudaMemcpyDeviceToHost),
-            "download particles");
+    if (part_state) {
+        PCK(cudaMemcpyAsync(part_state, p->d_state, (size_t)12 * p->n_part * sizeof(double), cudaMemcpyDeviceToHost,
+                            p->stream), "download particles");
+        PCK(cudaStreamSynchronize(p->stream), "download particles");
+    }
     return EPH_OK;
 }
 

@@ -246,9 +246,11 @@ class Particles:
                     "particles integrate")
         return hi.value, lo.value
 
-    def download(self):
-        pl = np.empty((NPLANES, self.n_pert))
-        pa = np.empty((12, self.n_part))
+    def download(self, pert_out: np.ndarray | None = None, part_out: np.ndarray | None = None):
+        """(perturber planes, particles [12][n]); optional output arrays (e.g. pinned buffers) are filled."""
+        pl = np.empty((NPLANES, self.n_pert)) if pert_out is None else pert_out
+        pa = np.empty((12, self.n_part)) if part_out is None else part_out
+        assert pl.flags.c_contiguous and pa.flags.c_contiguous and pa.shape == (12, self.n_part)
         self._check(self.lib.eph_particles_download(self.h, _dptr(pl), _dptr(pa)), "particles download")
         return pl, pa
 
