@@ -661,6 +661,7 @@ def run_serving_window(srv, reqs, rate, rng):
         arrivals = np.cumsum(gaps) - gaps[0]
     pending = {}
     lat, steps, h2d, d2h = [], 0, 0, 0
+    run_serving_window.rejected = 0
     t0 = time.perf_counter()
     nxt = 0
     while nxt < len(reqs) or pending:
@@ -673,9 +674,10 @@ def run_serving_window(srv, reqs, rate, rng):
             nxt += 1
         done = [rid for rid in list(pending) if srv.poll(rid) == 2]
         for rid in done:
-            out, acc, _ = srv.result(rid)
+            out, acc, rej = srv.result(rid)
             lat.append(time.perf_counter() - t0 - pending.pop(rid))
             steps += acc
+            run_serving_window.rejected += rej
             d2h += out.nbytes
         if not done:
             time.sleep(0.0005)
@@ -704,6 +706,7 @@ def run_b200_serving(args):
         clocks = ClockSampler(local)
         clocks.start()
         _, psteps, wall, h2d, d2h = run_serving_window(srv, reqs, float("inf"), rng)
+        rejected = run_serving_window.rejected
         clk = clocks.stop()
         launches = srv.info()[0] - launches0
         wall_max = reduce_max(pg, wall, dev)
@@ -734,6 +737,7 @@ def run_b200_serving(args):
                                        f"particles (a 0.5-50 AU, e < 0.6), durations log-U(1, {args.serve_years:g}) yr, "
                                        f"adaptive RK12 (step doubling) tol 1e-13",
                            "requests": len(reqs), "particles": int(sum(sizes)), "perturbers": m,
+                           "rejected_step_fraction": rejected / max(1, rejected + psteps),
                            "ephemeris_setup_s": setup_s, "parallelism": f"independent servers x{world}" if world > 1
                            else "1 GPU, 128 streams",
                            "note": "value = accepted particle-steps / wall clock with all requests submitted at once "
