@@ -44,6 +44,11 @@ UNIT = "body-steps/s"
 # ncu capture summarised in profiles/step_kernel_config2.md; the system stays in L2, so the traffic of a
 # launch of k steps is taken as k times this figure.
 DRAM_BYTES_PER_RK_STEP = {"config2": 869632}
+# DRAM bytes (read + write) of one particle_kernel launch per particle, from the ncu capture summarised in
+# profiles/particle_kernel_config5.md (1 M particles x 10 steps: 124.4 + 143.5 MB): the particle state is read
+# and written once per launch and the stage store stays in L2, so the traffic scales with the particles and
+# not with the steps of the launch.
+DRAM_BYTES_PER_PARTICLE_LAUNCH = (124.399360e6 + 143.479040e6) / 1e6
 
 # Algorithmic flop convention per ordered pair and stage evaluation ("Roofline"):
 FLOP_PASS_A = 20            # potential + Newtonian acceleration
@@ -582,7 +587,9 @@ def run_b200_particles(args):
                            "precision": "mixed (EIH 1PN in FP32)" if args.mixed else "fp64"},
                 "e2e": {"value": e2e, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
                 "roofline": {"bound": "fp64", "kernel": "particle_kernel", "achieved": achieved, "peak": peak,
-                             "unit": "TFLOP/s", "frac": achieved / peak if peak else None, "traffic": None,
+                             "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
+                             "traffic": DRAM_BYTES_PER_PARTICLE_LAUNCH * n_part,
+                             "traffic_unit": "bytes per launch (ncu, scaled by particles)",
                              "peak_source": peak_src, "flops_per_launch": fps * n_part * ks,
                              "kernel_ms": kern_ms},
                 "gpu_launches": l1 - l0,
