@@ -580,16 +580,19 @@ static int pump(eph_serve *s) {
         auto &r = s->reqs[s->pending.front()];
         if (s->in_use > 0 && s->in_use + r.bytes > s->budget) break;
         cudaStream_t st = s->streams[r.stream];
-        SCK(cudaMallocAsync((void **)&r.d_state, (size_t)12 * r.P * sizeof(double), st), "cudaMallocAsync(state)");
         const int S = r.block / r.G;
-        if (S > kSmemSlots)
-            SCK(cudaMallocAsync((void **)&r.d_fstore, (size_t)r.grid * kStages * 3 * S * sizeof(double), st),
-                "cudaMallocAsync(stage store)");
-        SCK(cudaMallocAsync((void **)&r.d_stats, (size_t)r.grid * 2 * sizeof(long long), st), "cudaMallocAsync(stats)");
-        SCK(cudaMallocAsync((void **)&r.d_status, (size_t)r.grid * sizeof(int), st), "cudaMallocAsync(status)");
-        if (r.log_cap > 0) SCK(cudaMallocAsync((void **)&r.d_hlog, (size_t)r.log_cap * sizeof(double), st), "cudaMallocAsync(log)");
-        SCK(cudaMemcpyAsync(r.d_state, r.host_in.data(), r.host_in.size() * sizeof(double), cudaMemcpyHostToDevice, st),
-            "upload particles");
+        cudaError_t e = cudaMallocAsync((void **)&r.d_state, (size_t)12 * r.P * sizeof(double), st);
+        if (e == cudaSuccess && S > kSmemSlots)
+            e = cudaMallocAsync((void **)&r.d_fstore, (size_t)r.grid * kStages * 3 * S * sizeof(double), st);
+        if (e == cudaSuccess) e = cudaMallocAsync((void **)&r.d_stats, (size_t)r.grid * 2 * sizeof(long long), st);
+        if (e == cudaSuccess) e = cudaMallocAsync((void **)&r.d_status, (size_t)r.grid * sizeof(int), st);
+        if (e == cudaSuccess && r.log_cap > 0) e = cudaMallocAsync((void **)&r.d_hlog, (size_t)r.log_cap * sizeof(double), st);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(r.d_state, r.host_in.data(), r.host_in.size() * sizeof(double), cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) {   // the request stays queued, holding nothing
+            req_free(r, st);
+            return sfail(s, e == cudaErrorMemoryAllocation ? EPH_ERR_OOM : EPH_ERR_CUDA, "admit request", e);
+        }
         ServeArgs A;
         A.coef = s->d_coef; A.gm = s->d_gm; A.sr2 = s->d_sr2; A.cheb = s->d_cheb;
         A.M = s->M; A.Mpad = s->Mpad; A.d = s->d; A.n = s->n; A.t0 = s->t0; A.knot = s->knot;
