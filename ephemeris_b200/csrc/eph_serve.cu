@@ -100,8 +100,25 @@ __device__ __forceinline__ double group_sum(double v, int G) {
 // known at compile time, four items per pass with all their coefficient loads issued before any is used
 // (they come from L2); D = 0: any degree, one item at a time.
 template <int D>
-__device__ __forceinline__ void eval_items(const ServeArgs &A, double *PR, const double *b, long long xi) {
+__device__ __forceinline__ void eval_items(const ServeArgs &A, double *PR, const double *cheb, double u, long long xi) {
     const int d = D > 0 ? D : A.d;
+    // basis values B[d, x - (xi + k)], k = 0..d, at u = 2 (x - xi) - 1 from their Chebyshev form
+    constexpr int NB = D > 0 ? D + 1 : EPH_BSPLINE_MAX_DEGREE + 1;
+    double b[NB];
+    const double u2 = 2 * u;
+#pragma unroll
+    for (int k = 0; k < NB; ++k) {
+        if (k > d) break;
+        const double *c = cheb + k * (d + 1);
+        double sum = c[0] + c[1] * u, tm, tt = 1, tp = u;
+        for (int j = 2; j <= d; ++j) {
+            tm = tt;
+            tt = tp;
+            tp = u2 * tt - tm;
+            sum += c[j] * tp;
+        }
+        b[k] = sum;
+    }
     const long long stride = A.n + d;
     const int total = A.M * kChan;
     constexpr int U = D > 0 ? 4 : 1;
@@ -145,24 +162,9 @@ __device__ void eval_perturbers(const ServeArgs &A, double *PR, const double *ch
     const double x = (t - A.t0) / A.knot;
     long long xi = (long long)floor(x);
     xi = xi < 0 ? 0 : (xi > A.n - 1 ? A.n - 1 : xi);
-    const double u = 2 * (x - (double)xi) - 1, u2 = 2 * u;
-    const int d = A.d;
-    double b[EPH_BSPLINE_MAX_DEGREE + 1];
-#pragma unroll
-    for (int k = 0; k <= EPH_BSPLINE_MAX_DEGREE; ++k) {
-        if (k > d) break;
-        const double *c = cheb + k * (d + 1);
-        double s = c[0] + c[1] * u, tm, tt = 1, tp = u;
-        for (int j = 2; j <= d; ++j) {
-            tm = tt;
-            tt = tp;
-            tp = u2 * tt - tm;
-            s += c[j] * tp;
-        }
-        b[k] = s;
-    }
-    if (d == 3) eval_items<3>(A, PR, b, xi);
-    else eval_items<0>(A, PR, b, xi);
+    const double u = 2 * (x - (double)xi) - 1;
+    if (A.d == 3) eval_items<3>(A, PR, cheb, u, xi);
+    else eval_items<0>(A, PR, cheb, u, xi);
     __syncthreads();
     for (int j = threadIdx.x; j < A.M; j += blockDim.x) {
         const double bx = PR[S_BX * A.Mpad + j], by = PR[S_BY * A.Mpad + j], bz = PR[S_BZ * A.Mpad + j];
@@ -382,7 +384,8 @@ __global__ void __launch_bounds__(kSThreads, 2) serve_kernel(ServeArgs A) {
             ++rejected;
         }
         // next step: 0.8 (tol / err)^(1/13) within [0.25, 2], no growth right after a rejection
-        double fac = (err == 0) ? 2.0 : (err != err) ? 0.25 : 0.8 * pow(A.tol / err, 1.0 / 13.0);
+        // (the factor only steers the step size: single precision is ample)
+        double fac = (err == 0) ? 2.0 : (err != err) ? 0.25 : 0.8 * (double)powf((float)(A.tol / err), 1.0f / 13.0f);
         fac = fac < 0.25 ? 0.25 : (fac > 2.0 ? 2.0 : fac);
         if (just_rejected && fac > 1.0) fac = 1.0;
         just_rejected = !(err <= A.tol);

@@ -349,12 +349,16 @@ class Server:
 
     def result(self, rid: int, log_cap: int = 0):
         """(particles [12][n], accepted, rejected[, step log]) of a launched request; releases it."""
-        out = np.empty((12, self.sizes.pop(rid)))
+        if rid not in self.sizes:
+            from ._lib import EphError
+            raise EphError(1, f"result: unknown request {rid}")
+        out = np.empty((12, self.sizes[rid]))
         acc, rej, nl = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
         log = np.empty(max(log_cap, 1))
         rc = self.lib.eph_serve_result(self.h, rid, _dptr(out), ctypes.byref(acc), ctypes.byref(rej),
                                        _dptr(log) if log_cap else None, ctypes.byref(nl) if log_cap else None)
         self._check(rc, "result")
+        del self.sizes[rid]
         if log_cap:
             return out, acc.value, rej.value, log[:nl.value].copy()
         return out, acc.value, rej.value
