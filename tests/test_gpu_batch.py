@@ -106,3 +106,31 @@ def test_full_physics_system_in_a_batch(golden, tmp_path):
     c.integrate(dt, 3)
     assert np.array_equal(out[0], c.download())
     assert np.array_equal(out[1], mem[0][0])   # zero steps: untouched
+
+
+def test_full_ensemble_members_match_their_own_runs(tmp_path):
+    """The 512-member ensemble at its full size (durations scaled by 0.02 to keep the test short): eight
+    members, integrated again on their own, give bit-identical states (a member's computation does not
+    depend on the rest of the batch), and every member's state is finite."""
+    from ephemeris_b200 import Batch, MSystem, synth
+    ens = synth.make_ensemble(512)
+    pls, mds, dts, ks = [], [], [], []
+    for s_, (m, k) in enumerate(ens):
+        ms = MSystem(0)
+        assert ms.load(synth.write_system(m, os.path.join(str(tmp_path), f"s{s_}")))
+        pls.append(ms.planes())
+        mds.append(ms.models())
+        dts.append(ms.delta_t)
+        ks.append(max(1, int(round(k * 0.02))))
+        ms.close()
+    b = Batch(0)
+    b.upload(pls, mds)
+    b.integrate(dts, ks)
+    outs = b.download()
+    assert all(np.isfinite(o[0:12]).all() for o in outs)
+    rng = np.random.default_rng(12)
+    for s_ in rng.choice(512, 8, replace=False):
+        one = Batch(0)
+        one.upload([pls[s_]], [mds[s_]])
+        one.integrate([dts[s_]], [ks[s_]])
+        assert np.array_equal(one.download()[0], outs[s_]), s_
