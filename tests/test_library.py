@@ -130,3 +130,22 @@ def test_bench_rank_reduction_gloo():
     for p in procs:
         p.join(timeout=60)
     assert res == [(0, 2, 11.0), (1, 2, 11.0)]
+
+
+def test_serving_and_particle_workloads_are_seeded():
+    """The config4/config5 generators: same seed, same bodies and particles; the stated shapes."""
+    from ephemeris_b200 import synth
+    a, b = synth.make_config4_system(4004), synth.make_config4_system(4004)
+    assert len(a.bodies) == 419 and [x.r for x in a.bodies] == [x.r for x in b.bodies]
+    assert all(x.k2 == 0 and x.j2 == 0 and x.gp_factor == 0 for x in a.bodies)   # point masses
+    s1, p1 = synth.make_config5(5005, n_particles=1000)
+    s2, p2 = synth.make_config5(5005, n_particles=1000)
+    assert np.array_equal(p1, p2) and len(s1.bodies) == 9
+    c1 = synth.make_config1(1001)
+    assert [x.r for x in s1.bodies[1:]] != [] and s1.bodies[0].j2 == 2e-4
+    assert [x.GM for x in s1.bodies] == [x.GM for x in c1.bodies[:9]]      # config1's star and planets
+    r = np.linalg.norm(p1[0:3] - np.asarray(s1.bodies[0].r)[:, None], axis=0) / synth.AU
+    assert r.min() > 1.5 * 0.7 - 1e-9 and r.max() < 50 * 1.3 + 1e-9        # a in [1.5, 50] AU, e < 0.3
+    rng = np.random.default_rng(1)
+    reqs = synth.make_requests(rng, 50, 10 * 365.25 * 86400, years=(1, 10))
+    assert all(1 <= q.shape[1] <= 4096 and 365.25 * 86400 * 0.999 <= t <= 10 * 365.25 * 86400 for q, t in reqs)
