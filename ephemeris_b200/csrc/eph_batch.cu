@@ -422,6 +422,9 @@ __device__ void integrate_system(const BatchSys &Y, const BatchView &V, bool coo
             }
             __syncthreads();
             if (coop) {
+                // every CTA of the cluster has finished the previous stage's pass B, which reads these rows
+                // in its own shared memory, before they are overwritten there
+                cg::this_cluster().sync();
                 broadcast_rows(V, BR_R_HI, BR_GM + 1 - BR_R_HI, lo, hi, rank);
                 cg::this_cluster().sync();
             }
