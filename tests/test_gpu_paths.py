@@ -178,3 +178,19 @@ def test_momentum_conservation(tmp_path):
     err_plain = max(np.linalg.norm(d[0:3]) / np.linalg.norm(hi[6:9]), np.linalg.norm(d[3:6]) / np.linalg.norm(hi[9:12]))
     assert err < 1e-12, err
     assert err / err_plain < 2e-8, err / err_plain
+
+
+def test_full_physics_run_repeats_bit_for_bit(tmp_path):
+    """The 504-body full-physics workload, 50 RK12 steps twice from the same upload: identical planes (the
+    persistent kernel's reductions and barriers fix every summation order)."""
+    from ephemeris_b200 import synth
+    cfg = synth.write_system(synth.make_config2(2002), os.path.join(str(tmp_path), "c2"))
+    ms = _load(cfg)
+    pl, md = ms.planes(), ms.models()
+    outs = []
+    for _ in range(2):
+        c = _ctx(pl, md)
+        c.integrate(ms.delta_t, 50)
+        outs.append(c.download())
+    assert np.isfinite(outs[0][0:12]).all()
+    assert np.array_equal(outs[0], outs[1])
