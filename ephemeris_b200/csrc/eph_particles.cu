@@ -13,8 +13,9 @@
 //   fields  geopotential and ring fields of the extended perturbers at i (mass.cpp:358-371; the reaction
 //           on the perturber is GM_i times the field, zero for a massless particle)
 //   final   f_i = (gaccel + daccel) + naccel (mass.cpp:389-396)
-// The RK12 combination and state update are those of RungeKutta.impl:148-186 (gather form: f_j stored per
-// stage, summed in ascending j). The reference has no massless bodies; bodies of negligible mass
+// The RK12 step is RungeKutta.impl:107-194's in second-order form (only the stage accelerations are
+// stored; see particle_kernel), with its state update's arithmetic. The reference has no massless bodies;
+// bodies of negligible mass
 // (GM = 1e-20 m^3/s^2) in one system with the perturbers are its equivalent, and the tests compare with
 // exactly that.
 #include <cuda_runtime.h>
