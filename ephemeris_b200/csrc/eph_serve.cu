@@ -22,7 +22,9 @@
 //   has no embedded pair, RungeKutta.impl:38-104); step doubling with the same 25-stage method is the
 //   estimator.
 // * Admission. Requests queue on the host and launch while their device memory (state, stage store)
-//   fits the server's budget; finished requests release it when their results are collected.
+//   fits: by default while the device's free memory (cudaMemGetInfo at admission) stays above a 1 GiB
+//   reserve, or within a fixed budget set by the caller; finished requests release their memory when their
+//   results are collected.
 // * Particle acceleration: Newtonian + EIH 1PN against every perturber, one sweep (the 4 phi_i term of
 //   mass.impl:90 factored out as 4 phi_i a_N,i), the stage combination in the second-order form of
 //   eph_particles.cu (only stage accelerations stored).
@@ -53,6 +55,7 @@ namespace eph {
 namespace {
 
 constexpr int kSThreads = 256;
+constexpr size_t kFreeReserve = 1ull << 30;   // device memory kept free when admitting by free memory
 constexpr int kSmemSlots = 64;   // particles per block whose stage store fits shared memory
 constexpr int kSStreams = 128;   // requests in flight at once (the device runs up to 128 kernels concurrently)
 constexpr int kChan = EPH_EPHEM_CHANNELS;   // x y z vx vy vz aN/c^2 (3) phi/c^2
@@ -581,7 +584,14 @@ static void req_free(eph_serve::Req &r, cudaStream_t st) {
 static int pump(eph_serve *s) {
     while (!s->pending.empty()) {
         auto &r = s->reqs[s->pending.front()];
-        if (s->in_use > 0 && s->in_use + r.bytes > s->budget) break;
+        if (s->in_use > 0) {
+            if (s->budget > 0) {
+                if (s->in_use + r.bytes > s->budget) break;
+            } else {   // admission by free device memory
+                size_t free_b = 0, total_b = 0;
+                if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess || free_b < r.bytes + kFreeReserve) break;
+            }
+        }
         cudaStream_t st = s->streams[r.stream];
         const int S = r.block / r.G;
         cudaError_t e = cudaMallocAsync((void **)&r.d_state, (size_t)12 * r.P * sizeof(double), st);
@@ -659,9 +669,7 @@ int eph_serve_create(int device, int64_t n_pert, const double *gm, const double 
         (e = cudaMemcpy(s->d_cheb, cheb.data(), cheb.size() * sizeof(double), cudaMemcpyHostToDevice)) != cudaSuccess)
         return bail(EPH_ERR_CUDA, "upload ephemeris", e);
     cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, device);
-    size_t free_b = 0, total_b = 0;
-    cudaMemGetInfo(&free_b, &total_b);
-    s->budget = free_b / 2;
+    s->budget = 0;   // admission by free device memory
     *out = s;
     return EPH_OK;
 }

@@ -187,7 +187,9 @@ int eph_serve_create(int device, int64_t n_pert, const double *gm, const double 
                      double t0, double knot, const double *coefs, eph_serve **out);
 int eph_serve_destroy(eph_serve *s);
 const char *eph_serve_last_error(const eph_serve *s);
-/* Device memory the in-flight requests may hold (default: half the free memory at creation). */
+/* Device memory the in-flight requests may hold: bytes > 0 a fixed budget; 0 (the default) admits requests
+ * while the device's free memory stays above a 1 GiB reserve. The oldest queued request always launches
+ * when nothing is in flight. */
 int eph_serve_set_budget(eph_serve *s, int64_t bytes);
 /* Record up to `cap` accepted step sizes of each later request's first block of particles (0: off). */
 int eph_serve_set_step_log(eph_serve *s, int64_t cap);

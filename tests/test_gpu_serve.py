@@ -139,7 +139,7 @@ def test_many_requests_and_budget(eph):
         while srv.poll(rid) == 0:
             pass
         assert np.array_equal(srv.result(rid)[0], want)
-    srv.set_budget(1 << 34)
+    srv.set_budget(0)                                           # back to admission by free memory
 
 
 def test_backward_request_and_refusals(eph):
