@@ -41,16 +41,16 @@ sys.path.insert(0, ROOT)
 METRIC = "body-steps/s vs plain FP64 at <=1e-12 pos err; small-body p50/p99 latency"
 UNIT = "body-steps/s"
 # DRAM bytes (read + write) of one step_kernel launch of one RK12 step on the config2 workload, from the
-# ncu capture summarised in profiles/step_kernel_config2.md; the system stays in L2, so the traffic of a
+# an ncu capture of one single-step launch (dram__bytes_read.sum + dram__bytes_write.sum); the system stays in L2, so the traffic of a
 # launch of k steps is taken as k times this figure.
 DRAM_BYTES_PER_RK_STEP = {"config2": 869632}
 # DRAM bytes (read + write) of one particle_kernel launch per particle, from the ncu capture summarised in
-# profiles/particle_kernel_config5.md (1 M particles x 10 steps: 124.4 + 143.5 MB): the particle state is read
+# an ncu capture of one launch (1 M particles x 10 steps: 124.4 + 143.5 MB): the particle state is read
 # and written once per launch and the stage store stays in L2, so the traffic scales with the particles and
 # not with the steps of the launch.
 DRAM_BYTES_PER_PARTICLE_LAUNCH = (124.399360e6 + 143.479040e6) / 1e6
 
-# Algorithmic flop convention per ordered pair and stage evaluation ("Roofline"):
+# Algorithmic flop convention per ordered pair and stage evaluation (add, sub, mul, div, sqrt = 1, fma = 2):
 FLOP_PASS_A = 20            # potential + Newtonian acceleration
 FLOP_PASS_A_TIDE = 120      # time-lagged tidal matrix, extra over the Newtonian part
 FLOP_1PN = 80

@@ -8,7 +8,8 @@
  * called from msystem::integrate(dt, n_step, USE_GPU=1) (src/physics/mass.cpp:408-409) and
  * msystem::accel(parallel_option>0) (src/physics/mass.cpp:218-220). A replacement translation unit
  * marshals the `mass` list into the plane layout of eph_planes.h and calls the functions below
- * (see INTEGRATION.md). All functions return an eph_status; none throws, exits or traps.
+ * (ephemeris_b200/bridge/cuda_rk12_bridge.cpp is that unit). All functions return an eph_status; none
+ * throws, exits or traps.
  *
  * Threading: one context per system; calls on one context are serialised by the context (the
  * reference serialises all GPU work on a global mutex, RungeKutta.cu:25,396,410). Different contexts
