@@ -27,7 +27,7 @@
 #include <vector>
 
 // mass.h:213-215 grants friendship to ephemeris_reader; its translation unit is not linked into
-// this library, so the driver uses the name to reach msystem's private members.
+// this library, so this file uses the name to reach msystem's private members.
 class ephemeris_reader {
 public:
     static htl::vector<mass> &bodies(msystem &m) { return m.mlist; }
