@@ -178,3 +178,26 @@ def test_full_size_workload_properties(tmp_path):
     q.integrate(dt, 20)
     _, alone = q.download()
     assert np.array_equal(alone, mid[:, pick])
+
+
+def test_full_size_mixed_precision_error(tmp_path):
+    """Mixed precision at the workload's full size (2 000 000 particles, 20 steps of 0.5 day): every particle
+    within 1e-14 of |r - r_star| of the FP64 run."""
+    from ephemeris_b200 import MSystem, Particles, synth
+    sysm, parts = synth.make_config5(5005, n_particles=2_000_000)
+    ms = MSystem(0)
+    assert ms.load(synth.write_system(sysm, os.path.join(str(tmp_path), "pert")))
+    pl, md, dt = ms.planes(), ms.models(), ms.delta_t
+    runs = []
+    for mixed in (False, True):
+        p = Particles(0)
+        p.set_precision(mixed)
+        p.upload(pl, md, parts)
+        p.integrate(dt, 20)
+        runs.append(p.download()[1])
+        p.close()
+    a, b = runs
+    star = pl[0:3, 0] + pl[3:6, 0]
+    r = b[0:3] + b[3:6]
+    err = np.linalg.norm((a[0:3] - b[0:3]) + (a[3:6] - b[3:6]), axis=0) / np.linalg.norm(r - star[:, None], axis=0)
+    assert np.isfinite(a).all() and err.max() <= 1e-14, err.max()

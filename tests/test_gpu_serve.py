@@ -170,3 +170,29 @@ def test_batch_fit_on_device_is_bit_identical(eph, d, n, mn):
     got = bspline_fit_batch(sm, n, d)
     for k in range(len(series)):
         assert np.array_equal(got[k], bspline_fit(series[k], n, d)), k
+
+
+def test_full_ephemeris_requests(tmp_path):
+    """The serving workload's full perturber set (419 bodies, 2-year ephemeris built and fitted on the GPU):
+    30 requests of log-U(1, 4096) particles in flight at once all finish with finite states, and two of them
+    rerun alone give the same states bit for bit."""
+    from ephemeris_b200 import Context, MSystem, Server, bspline_fit_batch, synth
+    sysm = synth.make_config4_system(4004)
+    ms = MSystem(0)
+    assert ms.load(synth.write_system(sysm, os.path.join(str(tmp_path), "eph419")))
+    pl, md = ms.planes(), ms.models()
+    c = Context(0)
+    c.upload(pl, md)
+    days = 730
+    samples, _ = c.record_samples(DAY / 2, 2 * days, 1)
+    coefs = bspline_fit_batch(np.ascontiguousarray(samples.transpose(1, 0, 2)), days, 3)
+    srv = Server(coefs, pl[39], DAY, 0.0, 3, pl[54])
+    rng = np.random.default_rng(13)
+    reqs = synth.make_requests(rng, 30, days * DAY, years=(0.1, 2.0), star_r=samples[0, 0, 0:3],
+                               star_v=samples[0, 0, 3:6])
+    ids = [srv.submit(p, 0.0, t) for p, t in reqs]
+    outs = [srv.result(i) for i in ids]
+    assert all(np.isfinite(o[0]).all() and o[1] > 0 for o in outs)
+    for k in (0, 17):
+        again = srv.result(srv.submit(reqs[k][0], 0.0, reqs[k][1]))[0]
+        assert np.array_equal(again, outs[k][0])
