@@ -40,10 +40,9 @@ sys.path.insert(0, ROOT)
 
 METRIC = "body-steps/s vs plain FP64 at <=1e-12 pos err; small-body p50/p99 latency"
 UNIT = "body-steps/s"
-# DRAM bytes (read + write) of one step_kernel launch of one RK12 step on the config2 workload, from the
-# an ncu capture of one single-step launch (dram__bytes_read.sum + dram__bytes_write.sum); the system stays in L2, so the traffic of a
-# launch of k steps is taken as k times this figure.
-DRAM_BYTES_PER_RK_STEP = {"config2": 869632}
+# DRAM bytes (read + write) of one step_kernel launch, from an ncu capture of that launch
+# (dram__bytes_read.sum + dram__bytes_write.sum), keyed by (workload, RK12 steps per launch).
+DRAM_BYTES_PER_LAUNCH = {("config2", 100): 1640960 + 948224}
 # DRAM bytes (read + write) of one particle_kernel launch per particle, from the ncu capture summarised in
 # an ncu capture of one launch (1 M particles x 10 steps: 124.4 + 143.5 MB): the particle state is read
 # and written once per launch and the stage store stays in L2, so the traffic scales with the particles and
@@ -63,15 +62,34 @@ FLOP_RING_DISK = 60         # per (body, ring host, disk)
 FLOP_RK = 3900              # RK12 combination + update per body-step
 
 
+def full_class(planes):
+    """Bodies for which a term beyond point-mass Newtonian + 1PN can be nonzero, as source or target (the
+    kernels' body classes): tides, rotational deformation, J2 rate, luminosity, radiation receptance,
+    geopotential, ring, static harmonics or spin. Pair terms between two other bodies are exactly zero and
+    the kernels skip them."""
+    P = planes
+    f = (P[46] != 0) | (P[47] != 0) | (P[43] != 0) | (P[50] != 0) | (P[55] != 0) | (P[102] >= 0) | (P[103] >= 0)
+    return f | (P[56:65] != 0).any(0) | (P[36:39] != 0).any(0) | (P[12:18] != 0).any(0)
+
+
 def algorithmic_flops_per_step(planes, models):
-    """FLOPs of one RK12 step (25 stage evaluations) of the whole system, by the convention above."""
+    """FLOPs of one RK12 step (25 stage evaluations) of the whole system by the convention above, counting
+    only the terms the kernels evaluate: pass A and 1PN for every ordered pair, the time-lagged tide for pairs
+    whose first body has a delayed tide, deformation / Lense-Thirring / radiation for pairs with a full-class
+    body, geopotential per (body, host) by model kind, ring per (body, host, disk)."""
     n = planes.shape[1]
-    k2, td = planes[46], planes[48]
-    delayed = int(((k2 != 0) & (td != 0)).sum())
-    per_stage = (n * (n - 1) * (FLOP_PASS_A + FLOP_1PN + FLOP_DEFORM + FLOP_LT + FLOP_RAD)
+    n_point = n - int(full_class(planes).sum())
+    pairs = n * (n - 1)
+    pairs_full = pairs - n_point * (n_point - 1)
+    delayed = int(((planes[46] != 0) & (planes[48] != 0)).sum())
+    per_stage = (pairs * (FLOP_PASS_A + FLOP_1PN) + pairs_full * (FLOP_DEFORM + FLOP_LT + FLOP_RAD)
                  + delayed * (n - 1) * FLOP_PASS_A_TIDE)
-    per_stage += len(models.gp_nz) * (n - 1) * FLOP_GP
-    per_stage += int(np.sum(models.ring_ndisk)) * (n - 1) * FLOP_RING_DISK
+    for k in range(len(models.gp_nz)):
+        hosts = int((planes[102] == k).sum())
+        per_stage += hosts * (n - 1) * (FLOP_GP if models.gp_nt[k] > 0 else FLOP_GP_ZONAL)
+    for k in range(len(models.ring_ndisk)):
+        hosts = int((planes[103] == k).sum())
+        per_stage += hosts * (n - 1) * int(models.ring_ndisk[k]) * FLOP_RING_DISK
     return 25 * per_stage + n * FLOP_RK
 
 
@@ -366,6 +384,7 @@ def run_b200_ensemble(args):
         flops = _ensemble_flops(pls, ks)
         achieved = flops / (dev_ms / args.steps / 1e3) / 1e12
         peak, peak_src = fp64_peak(dev)
+        pipe = fp64_pipe_peak(local)
         cpu = None
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
             try:
@@ -565,6 +584,7 @@ def run_b200_particles(args):
         fps = particle_flops_per_step(pl, md)
         achieved = fps * n_part * ks / (kern_ms / 1e3) / 1e12
         peak, peak_src = fp64_peak(dev)
+        pipe = fp64_pipe_peak(local)
         cpu = None
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
             try:
@@ -897,6 +917,7 @@ def run_b200(args):
         flops_step = algorithmic_flops_per_step(planes0, models)
         achieved = flops_step * rk / (kern_ms / 1e3) / 1e12
         peak, peak_src = fp64_peak(dev)
+        pipe = fp64_pipe_peak(local)
         cpu = None
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
             try:
@@ -917,10 +938,11 @@ def run_b200(args):
                         "d2h_bytes_per_step": int(planes0.nbytes)},
                 "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                              "frac": achieved / peak if peak else None,
-                             "traffic": (DRAM_BYTES_PER_RK_STEP[args.workload] * rk
-                                         if args.workload in DRAM_BYTES_PER_RK_STEP else None),
-                             "traffic_unit": "bytes per launch (ncu, scaled by RK12 steps per launch)",
-                             "peak_source": peak_src, "flops_per_launch": flops_step * rk},
+                             "traffic": DRAM_BYTES_PER_LAUNCH.get((args.workload, rk)),
+                             "traffic_unit": "DRAM bytes read + written per step_kernel launch (ncu)",
+                             "peak_source": peak_src, "flops_per_launch": flops_step * rk,
+                             "fp64_pipe_peak": pipe, "frac_of_fp64_pipe": achieved / pipe if pipe else None,
+                             "fp64_pipe_peak_source": "eph_fp64_fma_rate: independent FMA chains on every SM"},
                 "gpu_launches": launches,
                 "clocks": clk,
             }
@@ -929,6 +951,14 @@ def run_b200(args):
             print(json.dumps(line), flush=True)
     if pg is not None:
         pg.destroy_process_group()
+
+
+def fp64_pipe_peak(device: int):
+    """Measured throughput of the FP64 CUDA-core pipe (TFLOP/s), the pipe the RK12 kernels run on."""
+    import ctypes
+    from ephemeris_b200 import load_library
+    v = ctypes.c_double(0)
+    return v.value if load_library().eph_fp64_fma_rate(device, ctypes.byref(v)) == 0 else None
 
 
 def fp64_peak(dev):

@@ -1,8 +1,9 @@
 // eph_models.cuh - device evaluation of the extended-body force models.
 //
-//   gp_sum   : spherical-harmonic field of degree 3..8 (zonal up to Nz, tesseral up to Nt) in the
-//              body frame, per unit GM of the extended body. Same recursion and coefficient packing
-//              as geopotential::sum (src/physics/geopotential.impl:18-106).
+//   gp_field : spherical-harmonic field of degree 2..8 (zonal up to Nz, tesseral up to Nt) in the
+//              body frame, per unit GM of the extended body: what geopotential::sum computes
+//              (src/physics/geopotential.impl:26-106), by Cunningham's Cartesian recursion instead of
+//              the reference's spherical-coordinate Legendre recursion (method below).
 //   ring_sum : field of a cylindrical annulus built from signed uniform disks, per unit GM of the
 //              host, in the ring frame. Same Pade series, angle formula and fp32 bicubic correction
 //              table as ring::sum (src/physics/ring.impl:2070-2195).
@@ -13,73 +14,94 @@
 
 namespace eph {
 
-static __device__ __noinline__ v3 gp_sum(const double *__restrict__ c_table, int Nz, int Nt, double R, v3 r) {
-    double rho2 = r.x * r.x + r.y * r.y;
-    double rr2 = 1.0 / (rho2 + r.z * r.z);
-    double rho1 = sqrt(rho2);
-    double rr1 = sqrt(rr2);
-    double rb1 = R * rr1;
-    double rbn = rb1;
-    double cphi = rho1 * rr1;
-    double sphi = r.z * rr1;
-    double cm, sm;
-    if (rho2 < 2.2250738585072014e-308) { cm = 1; sm = 0; }
-    else { cm = r.x / rho1; sm = r.y / rho1; }
-    double pnm[EPH_GP_MAX_DEGREE], pn1m[EPH_GP_MAX_DEGREE];
-#pragma unroll
-    for (int q = 0; q < EPH_GP_MAX_DEGREE; ++q) { pnm[q] = 0; pn1m[q] = 0; }
-    pn1m[0] = 1;
-    double ppn = 1, pn = 1, pn1 = sphi;
-    double zx = 0, zz = 0;
-    v3 t = mk(0, 0, 0);
-#pragma unroll
-    for (int n = 2; n <= EPH_GP_MAX_DEGREE; ++n) {
-        if (n > Nz) break;
-        rbn *= rb1;
-        const double *JCSn = c_table + (n * n - 4);
-        pn = ((double)(2 * n - 1) * sphi * pn1 - (double)(n - 1) * pn) / (double)n;
-        ppn = sphi * ppn + (double)n * pn1;
-        double z1 = __ldg(JCSn) * rbn;
-        zx += (double)(n + 1) * z1 * pn;
-        zz -= z1 * ppn;
-        { double sw = pn; pn = pn1; pn1 = sw; }
-        if (n > Nt) continue;
-        v3 f = mk(0, 0, 0);
-        double m1 = (double)(2 * n - 1) * sphi;
-        double m2 = (double)(-n) * sphi;
-        double smm = 0, cmm = 0, smm1 = 0, cmm1 = 0;
-#pragma unroll
-        for (int m = 1; m <= n; ++m) {
-            if (m == n) {
-                pn1m[m - 1] = 0;
-                pnm[m - 1] = (double)(2 * n - 1) * cphi * pnm[m >= 2 ? m - 2 : 0];
-            } else {
-                pnm[m - 1] = (m1 * pn1m[m - 1] - (double)(n + m - 1) * pnm[m - 1]) / (double)(n - m);
-            }
-            if (m == 1) { smm = sm; cmm = cm; smm1 = 0; cmm1 = 1; }
-            else {
-                smm = 2 * cm * smm1 - smm;
-                cmm = 2 * cm * cmm1 - cmm;
-            }
-            double S = __ldg(JCSn + 2 * m), C = __ldg(JCSn + 2 * m - 1);
-            double t1 = S * smm + C * cmm;
-            double t2 = S * cmm - C * smm;
-            double ppnm = m2 * pnm[m - 1] + (double)(n + m) * pn1m[m - 1];
-            f.x += t1 * pnm[m - 1];
-            f.y += (double)m * t2 * pnm[m - 1];
-            f.z += t1 * ppnm;
-            { double sw = cmm; cmm = cmm1; cmm1 = sw; }
-            { double sw = smm; smm = smm1; smm1 = sw; }
-            { double sw = pnm[m - 1]; pnm[m - 1] = pn1m[m - 1]; pn1m[m - 1] = sw; }
+// 1/k for the degree recursion (k = 1 .. EPH_GP_MAX_DEGREE + 1); index 0 unused.
+__device__ __constant__ const double GP_RCP[EPH_GP_MAX_DEGREE + 2] = {
+    0.0, 1.0, 1.0 / 2, 1.0 / 3, 1.0 / 4, 1.0 / 5, 1.0 / 6, 1.0 / 7, 1.0 / 8, 1.0 / 9};
+
+// Gradient of the spherical-harmonic potential of an extended body, per unit GM of the body, at the
+// body-frame position r = (x, y, z):
+//   U / GM = 1/r sum_{n>=2} (R/r)^n [ -J_n P_n(sin lat) + sum_{m=1..n} P_nm(sin lat) (C_nm cos m lon + S_nm sin m lon) ],
+// with unnormalised associated Legendre functions without the Condon-Shortley phase (the convention of the
+// model files the loader reads; the coefficient of (n, m) sits at n^2-4 (J_n), n^2-4+2m-1 (C_nm),
+// n^2-4+2m (S_nm), geopotential.impl:21-24). Degrees 2..Nz are zonal, tesseral orders only for n <= Nt.
+//
+// Method: Cunningham's Cartesian recursion of the solid harmonics
+//   V_km + i W_km = (R/r)^(k+1) P_km(sin lat) e^(i m lon)
+// (Cunningham 1970; Montenbruck & Gill, Satellite Orbits, 2000, sec. 3.2.4-3.2.5), whose gradient terms
+// are again solid harmonics of one degree higher:
+//   a_x = 1/R^2 sum [ m=0: -C_n0 V_{n+1,1};  m>0: ( -C V_{n+1,m+1} - S W_{n+1,m+1}
+//                     + (n-m+2)(n-m+1) (C V_{n+1,m-1} + S W_{n+1,m-1}) ) / 2 ]
+//   a_y = 1/R^2 sum [ m=0: -C_n0 W_{n+1,1};  m>0: ( -C W_{n+1,m+1} + S V_{n+1,m+1}
+//                     + (n-m+2)(n-m+1) (-C W_{n+1,m-1} + S V_{n+1,m-1}) ) / 2 ]
+//   a_z = 1/R^2 sum (n-m+1) ( -C V_{n+1,m} - S W_{n+1,m} ).
+// No angle, square root of rho or division by cos(lat) is needed, so the poles are regular points. The
+// table of V, W is never stored: column m (orders) is walked upwards in degree k with the three-term
+// recursion, starting from the diagonal V_mm, W_mm, and every value is consumed at once by the (up to)
+// three gradient terms that read it: a_z of (k-1, m), a_x / a_y of (k-1, m-1) and of (k-1, m+1). Column 0
+// and 1 run to degree Nz + 1 (zonal terms), higher columns to Nt + 1; with kZonal only columns 0 and 1
+// run. T is double (plain FP64) or float (mixed precision; the caller scales far fields into range).
+template <typename T, bool kZonal>
+__device__ __forceinline__ void gp_core(const double *__restrict__ tab, int Nz, int Nt, T R, T x, T y, T z, T &ax,
+                                        T &ay, T &az) {
+    ax = 0; ay = 0; az = 0;
+    const T ir2 = T(1) / (x * x + y * y + z * z);
+    const T q = R * ir2;
+    const T xs = x * q, ys = y * q, zs = z * q, rho2 = R * q;   // (x, y, z) R / r^2, (R / r)^2
+    T vd = R * sqrt(ir2), wd = 0;                               // V_00 = R / r, W_00 = 0
+    const int mlast = kZonal ? 1 : max(Nt + 1, 1);
+#pragma unroll 1
+    for (int m = 0; m <= mlast; ++m) {
+        if (m > 0) {   // diagonal step: V_mm + i W_mm = (2m-1) (x + i y) R/r^2 (V + i W)_{m-1,m-1}
+            const T f = T(2 * m - 1);
+            const T nv = f * (xs * vd - ys * wd), nw = f * (xs * wd + ys * vd);
+            vd = nv;
+            wd = nw;
         }
-        f.x *= (double)(n + 1);
-        t += rbn * f;
+        const int klast = m <= 1 ? Nz + 1 : Nt + 1;
+        T v = vd, w = wd, vp = 0, wp = 0;   // (V, W) at degree k and k - 1 of column m
+#pragma unroll 1
+        for (int k = m; k <= klast; ++k) {
+            if (k > m) {   // (k - m) V_km = (2k-1) z R/r^2 V_{k-1,m} - (k+m-1) (R/r)^2 V_{k-2,m}
+                const T a = T(2 * k - 1) * zs, b = T(k + m - 1) * rho2, c = T(GP_RCP[k - m]);
+                const T nv = (a * v - b * vp) * c, nw = (a * w - b * wp) * c;
+                vp = v; wp = w; v = nv; w = nw;
+            }
+            const int n = k - 1;   // degree of the coefficients that read (V, W)_km
+            if (n < 2) continue;
+            const double *cn = tab + (n * n - 4);
+            if (m == 0) {
+                if (n <= Nz) az += T(n + 1) * (T(__ldg(cn)) * v);                 // -C_n0 = J_n, W_k0 = 0
+            } else if (!kZonal && m <= n && n <= Nt) {
+                az -= T(n - m + 1) * (T(__ldg(cn + 2 * m - 1)) * v + T(__ldg(cn + 2 * m)) * w);
+            }
+            if (m == 1) {
+                if (n <= Nz) {
+                    const T J = T(__ldg(cn));
+                    ax += J * v;
+                    ay += J * w;
+                }
+            } else if (!kZonal && m >= 2 && n <= Nt) {                            // order m - 1 >= 1
+                const T C = T(__ldg(cn + 2 * m - 3)), S = T(__ldg(cn + 2 * m - 2));
+                ax -= T(0.5) * (C * v + S * w);
+                ay += T(0.5) * (S * v - C * w);
+            }
+            if (!kZonal && m + 1 <= n && n <= Nt) {                               // order m + 1
+                const T C = T(__ldg(cn + 2 * m + 1)), S = T(__ldg(cn + 2 * m + 2));
+                const T f = T(0.5) * T((k - m) * (k - m - 1));
+                ax += f * (C * v + S * w);
+                ay += f * (S * v - C * w);
+            }
+        }
     }
-    t.x = zx - cphi * t.x;
-    t.z += zz * cphi;
-    t = rr2 * t;
-    double g1 = t.x * cphi - t.z * sphi;
-    return mk(g1 * cm - t.y * sm, g1 * sm + t.y * cm, cphi * t.z + sphi * t.x);
+    const T s = T(1) / (R * R);
+    ax *= s; ay *= s; az *= s;
+}
+
+// FP64 field of a geopotential model (any Nz, Nt), out of line: it sits on a cold path of the step kernel.
+static __device__ __noinline__ v3 gp_field(const double *__restrict__ tab, int Nz, int Nt, double R, v3 r) {
+    v3 a = mk(0, 0, 0);
+    if (Nz >= 2) gp_core<double, false>(tab, Nz, Nt, R, r.x, r.y, r.z, a.x, a.y, a.z);
+    return a;
 }
 
 __device__ __forceinline__ float ring_fzcorr(float x, float y, int kh) {

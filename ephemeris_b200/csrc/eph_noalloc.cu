@@ -60,7 +60,7 @@ constexpr size_t kOffExt = kOffOwn + r32((size_t)kNB * kOwnMax / 2);
 constexpr size_t kOffGpNz = kOffExt + r32(kNE / 2 + 1);
 constexpr size_t kOffGpNt = kOffGpNz + r32(kNGP / 2 + 1);
 constexpr size_t kOffRingNd = kOffGpNt + r32(kNGP / 2 + 1);
-constexpr size_t kOffWords = kOffRingNd + r32(kNRing / 2 + 1);   // barrier {count, generation}, status
+constexpr size_t kOffWords = kOffRingNd + r32(kNRing / 2 + 1);   // 64-bit barrier arrival counter, status
 constexpr size_t kScratchDoubles = kOffWords + 32;
 
 __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
@@ -213,7 +213,9 @@ int body(int device, cudaStream_t stream, int n, double *d_planes, const eph_mod
     int status = 0;
     NA_CK(cudaMemcpyAsync(&status, S.status, sizeof(int), cudaMemcpyDeviceToHost, stream));
     NA_CK(cudaStreamSynchronize(stream));
-    if (status != ST_OK) return EPH_ERR_TIMEOUT;   // a bounded grid-barrier or tile-copy wait gave up
+    // a bounded grid-barrier or tile-copy wait gave up (as the context path maps it); anything else is a fault
+    if (status == ST_BARRIER_TIMEOUT || status == ST_COPY_TIMEOUT) return EPH_ERR_TIMEOUT;
+    if (status != ST_OK) return EPH_ERR_CUDA;
     // t_eph += dt*n_step in double-double (mass.cpp:441)
     double a = *t_eph_hi, b = dt * (double)n_step;
     double s = a + b, t = s - a;

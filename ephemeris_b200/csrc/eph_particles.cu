@@ -75,34 +75,13 @@ struct PartArgs {
     int *next;                  // particle-block queue
 };
 
-// gp_sum (eph_models.cuh) for a purely zonal model (Nt = 0) with its degree loop rolled: the zonal
-// recursion of geopotential::sum (src/physics/geopotential.impl:18-60) in a handful of registers, so the
-// particle kernel keeps its occupancy when its only extended perturber is zonal.
+// Field of a purely zonal geopotential (Nt = 0), inline: gp_core's columns 0 and 1 only, with rolled
+// loops in a handful of registers, so the particle kernel keeps its occupancy when its only extended
+// perturber is zonal.
 __device__ __forceinline__ v3 gp_zonal(const double *__restrict__ c_table, int Nz, double R, v3 r) {
-    const double rho2 = r.x * r.x + r.y * r.y;
-    const double rr2 = 1.0 / (rho2 + r.z * r.z);
-    const double rho1 = sqrt(rho2);
-    const double rr1 = sqrt(rr2);
-    const double rb1 = R * rr1;
-    const double cphi = rho1 * rr1;
-    const double sphi = r.z * rr1;
-    double cm, sm;
-    if (rho2 < 2.2250738585072014e-308) { cm = 1; sm = 0; }
-    else { cm = r.x / rho1; sm = r.y / rho1; }
-    double rbn = rb1, ppn = 1, pn = 1, pn1 = sphi, zx = 0, zz = 0;
-#pragma unroll 1
-    for (int n = 2; n <= Nz; ++n) {
-        rbn *= rb1;
-        pn = ((double)(2 * n - 1) * sphi * pn1 - (double)(n - 1) * pn) / (double)n;
-        ppn = sphi * ppn + (double)n * pn1;
-        const double z1 = __ldg(c_table + (n * n - 4)) * rbn;
-        zx += (double)(n + 1) * z1 * pn;
-        zz -= z1 * ppn;
-        const double sw = pn; pn = pn1; pn1 = sw;
-    }
-    const double tx = rr2 * zx, tz = rr2 * (zz * cphi);
-    const double g1 = tx * cphi - tz * sphi;
-    return mk(g1 * cm, g1 * sm, cphi * tz + sphi * tx);
+    v3 a = mk(0, 0, 0);
+    if (Nz >= 2) gp_core<double, true>(c_table, Nz, 0, R, r.x, r.y, r.z, a.x, a.y, a.z);
+    return a;
 }
 
 // Mixed precision: the perturber fields that the FP32 form reads, as floats, kPF32 per perturber.
@@ -125,7 +104,7 @@ __device__ __forceinline__ float dot(f3 a, f3 b) { return a.x * b.x + a.y * b.y 
 // perturbers: pass B's 4 phi_i term (mass.impl:90) is sum_j GM_j/r^3 * 4 phi_i * d = 4 phi_i * a_N,i, so it
 // is added once after the sweep instead of waiting for phi_i; the other terms are the reference's.
 // kGeneral = false: the field loop handles zonal geopotentials only (gp_zonal, inline); true: any model
-// (gp_sum, ring_sum: calls, whose register saves cost the kernel some spilling).
+// (gp_field, ring_sum: calls, whose register saves cost the kernel some spilling).
 // kMixed: the EIH 1PN terms in FP32 from the float records Pf (their sum is ~(v/c)^2 ~ 1e-8 of the
 // Newtonian acceleration for solar-system speeds, so FP32 rounding is ~1e-15 of it); the separations, 1/r,
 // the Newtonian terms and the deformation and Lense-Thirring terms (which can reach 1e-3 of the Newtonian
@@ -213,7 +192,7 @@ __device__ __forceinline__ v3 particle_accel(const PartArgs &A, const double *P,
             const int nz = A.gp_nz[gp], nt = A.gp_nt[gp];
             const v3 rl = tolocal(f, re);
             const v3 an = toworld(f, (!kGeneral || nt == 0) ? gp_zonal(tab, nz, PR(j, TR_RADIUS), rl)
-                                                            : gp_sum(tab, nz, nt, PR(j, TR_RADIUS), rl));
+                                                            : gp_field(tab, nz, nt, PR(j, TR_RADIUS), rl));
             da += PR(j, TR_GM) * an;
         }
         if (kGeneral && rg >= 0) {

@@ -32,6 +32,9 @@
 #include <stdint.h>
 #include <string.h>
 
+#include <atomic>
+#include <mutex>
+
 #include "eph_math.cuh"
 #include "eph_models.cuh"
 #include "eph_system.cuh"
@@ -778,7 +781,7 @@ __device__ void ext_fields(const SysDev &S, const Own *own, int nb, int buf, Scr
                 r = body_sep(o, E);
                 GME = __ldcg(pub + PUB_GM * ld + E);
                 m3 f = ld9(pub + PUB_FRAME * ld, ld, E);
-                an = toworld(f, gp_sum(S.gp_coef + (size_t)gpE * EPH_GP_TABLE_SIZE, __ldg(S.gp_nz + gpE),
+                an = toworld(f, gp_field(S.gp_coef + (size_t)gpE * EPH_GP_TABLE_SIZE, __ldg(S.gp_nz + gpE),
                                        __ldg(S.gp_nt + gpE), __ldg(S.cst + CST_R * ld + E), tolocal(f, r)));
             }
             put(0, b, e, o, r, an, GME, live);
@@ -1422,17 +1425,22 @@ constexpr int kMaxSmem = 227 * 1024 - 4096;
 // Largest tile (bodies, multiple of kPad) that fits next to the fixed shared-memory state.
 int max_tile() { return (int)((kMaxSmem - step_fixed_smem_bytes()) / (kTileRows * sizeof(double))) / kPad * kPad; }
 
-static bool g_consts_ready[64];
+// Per-device "constants uploaded" flags. Contexts (each under its own lock) and the fixed-scratch entry
+// point (under its own) may set a device up at the same time: one mutex of its own orders the uploads.
+static std::atomic<bool> g_consts_ready[64];
+static std::mutex g_consts_mu;
 
 cudaError_t upload_constants(int device) {
-    if (device >= 0 && device < 64 && g_consts_ready[device]) return cudaSuccess;
+    if (device >= 0 && device < 64 && g_consts_ready[device].load(std::memory_order_acquire)) return cudaSuccess;
+    std::lock_guard<std::mutex> lock(g_consts_mu);
+    if (device >= 0 && device < 64 && g_consts_ready[device].load(std::memory_order_relaxed)) return cudaSuccess;
     double hi[EPH_RK12_NCOEF], lo[EPH_RK12_NCOEF], dtk[kStages + 1];
     rk12_expand(hi, lo, dtk);
     cudaError_t e = cudaMemcpyToSymbol(c_rk_hi, hi, sizeof(hi));
     if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_rk_lo, lo, sizeof(lo));
     if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_dtk, dtk, sizeof(dtk));
     if (e == cudaSuccess) e = cudaFuncSetAttribute(step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
-    if (e == cudaSuccess && device >= 0 && device < 64) g_consts_ready[device] = true;
+    if (e == cudaSuccess && device >= 0 && device < 64) g_consts_ready[device].store(true, std::memory_order_release);
     return e;
 }
 

@@ -213,6 +213,18 @@ int eph_serve_request_shape(eph_serve *s, int64_t id, int *lanes, int *particles
 int eph_serve_eval(eph_serve *s, double t, double *out);
 int eph_serve_info(const eph_serve *s, int64_t *launches, int64_t *queued, int64_t *bytes_in_use);
 
+/* ---- Force models evaluated on their own (geopotential::sum, src/physics/geopotential.h:36): the field
+ * of a geopotential model coef[EPH_GP_TABLE_SIZE] (degrees 2..nz zonal, tesseral up to nt <= nz) of a body
+ * of radius R at `count` body-frame positions r[count][3] (host arrays): out[count][3] = acceleration per
+ * unit GM of the body, computed on `device` by the device function the integration kernels use. */
+int eph_geopotential_field(int device, const double *coef, int nz, int nt, double R, int64_t count, const double *r,
+                           double *out);
+
+/* Measurement aid (no counterpart in the reference): the throughput of the FP64 CUDA-core pipe that the
+ * integration kernels use, measured on `device` with independent FMA chains on every SM (TFLOP/s, an FMA
+ * counted as 2 flops). */
+int eph_fp64_fma_rate(int device, double *tflops);
+
 /* Limits of eph_integrate_noalloc's fixed scratch (about 2.5 MB of device memory per GPU). */
 #define EPH_NOALLOC_MAX_BODIES 1024
 #define EPH_NOALLOC_MAX_EXT 16     /* bodies with a geopotential or ring model */
@@ -227,12 +239,16 @@ int eph_serve_info(const eph_serve *s, int64_t *launches, int64_t *queued, int64
  * integrated in place on `stream` (a cudaStream_t of that device, or NULL for the legacy default stream);
  * the model tables are read from host memory. The kernel's working memory is one fixed array compiled into
  * the library, which every GPU that loads the library holds until the process exits; no call allocates
- * anything, on the device or through any library. Sizes beyond the EPH_NOALLOC_MAX_* limits (or more
- * co-resident CTAs than the GPU offers) return EPH_ERR_LIMIT before any device work. The first call on a
- * device sets that device up (looks up the array's device address, uploads the RK12 tables); make that
- * first call before any stream capture. All calls share the array, and calls that overlapped on the GPU
- * would race on it: a lock inside the library serialises the calls of one process and each call returns
- * only after its work has finished. The caller's current device is restored before returning. */
+ * anything, on the device or through any library. More bodies, geopotential or ring models than the
+ * EPH_NOALLOC_MAX_* limits return EPH_ERR_LIMIT before any device work. The extended-body limit and the
+ * planes' model indices can only be checked once the planes are on the host: each call first copies the
+ * planes from the device on `stream` and waits for that copy, then returns EPH_ERR_LIMIT (too many extended
+ * bodies or more co-resident CTAs than the GPU offers) or EPH_ERR_ARG (a model index out of range) before
+ * any further device work. The first call on a device sets that device up (looks up the array's device
+ * address, uploads the RK12 tables); make that first call before any stream capture. Every call waits on
+ * `stream` for its own work. All calls share the array, and calls that overlapped on the GPU would race on
+ * it: a lock inside the library serialises the calls of one process and each call returns only after its
+ * work has finished. The caller's current device is restored before returning. */
 int eph_integrate_noalloc(int device, void *stream, int64_t n, double *d_planes, const eph_models *models,
                           double dt, int64_t n_step, double *t_eph_hi, double *t_eph_lo);
 

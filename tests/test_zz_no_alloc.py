@@ -15,7 +15,10 @@ POS_TOL = 1e-12
 ACC_TOL = 1e-14
 MAX_BODIES = 1024          # EPH_NOALLOC_MAX_BODIES
 MAX_GP = 16                # EPH_NOALLOC_MAX_GP
+MAX_EXT = 16               # EPH_NOALLOC_MAX_EXT
+EPH_ERR_ARG = 1
 EPH_ERR_LIMIT = 8
+P_GP_INDEX = 102           # EPH_P_GP_INDEX
 
 
 def _lib():
@@ -71,14 +74,43 @@ def test_noalloc_matches_context_path_on_two_calls(golden, name):
     d = torch.from_numpy(np.ascontiguousarray(g["load"])).to("cuda:0")
     torch.cuda.synchronize()
     t_ref = t_na = (0.0, 0.0)
-    for n_step in (3, 2):   # two calls in a row; the second starts from the first's output
+    dev = torch.cuda.current_device()
+    for n_step in (3, 2, -2):   # calls in a row, each from the previous one's output; the last one backwards
         t_ref = ctx.integrate(dt, n_step, t_ref)
         want = ctx.download()
         rc, t_na = _noalloc(lib, d, n, models, dt, n_step, t_na)
         assert rc == 0, rc
+        assert torch.cuda.current_device() == dev
         got = d.cpu().numpy()
         assert np.isfinite(got[0:12]).all()
         assert position_error(got, want) <= POS_TOL
         assert accel_error(got, want) <= ACC_TOL
         assert t_na == t_ref
     ctx.close()
+
+
+@pytest.mark.gpu
+def test_limits_checked_after_reading_the_planes(golden):
+    """The extended-body limit and the model indices are checked once the planes are read from the device:
+    EPH_ERR_LIMIT for more than EPH_NOALLOC_MAX_EXT bodies with a model, EPH_ERR_ARG for an index beyond the
+    models; the caller's planes are left untouched and the caller's device stays current."""
+    import torch
+    g = golden("small_full")
+    lib = _lib()
+    models = _models(g)
+    pl = np.array(g["load"])
+    n = pl.shape[1]
+    assert n > MAX_EXT
+    many = pl.copy()
+    many[P_GP_INDEX, :MAX_EXT + 1] = 0            # 17 bodies share geopotential model 0
+    bad = pl.copy()
+    bad[P_GP_INDEX, 3] = len(models.gp_nz)        # one past the last model
+    dev = torch.cuda.current_device()
+    for planes, want in ((many, EPH_ERR_LIMIT), (bad, EPH_ERR_ARG)):
+        d = torch.from_numpy(np.ascontiguousarray(planes)).to("cuda:0")
+        torch.cuda.synchronize()
+        rc, t = _noalloc(lib, d, n, models, float(g["dt"]), 1, (0.0, 0.0))
+        assert rc == want, rc
+        assert t == (0.0, 0.0)
+        assert np.array_equal(d.cpu().numpy(), planes)
+        assert torch.cuda.current_device() == dev
