@@ -22,6 +22,7 @@ int max_coresident_ctas(int device, int tile, int *out);
 }  // namespace eph
 
 using namespace eph;
+static_assert(kOwnMax == EPH_MAX_BODIES_PER_CTA, "the C ABI states the per-CTA body limit");
 
 struct eph_ctx {
     int device = 0;
@@ -41,7 +42,10 @@ struct eph_ctx {
     unsigned *d_bar = nullptr;
     int *d_gp_nz = nullptr, *d_gp_nt = nullptr, *d_ring_nd = nullptr;
     double *d_gp_coef = nullptr, *d_ring_param = nullptr, *d_ring_disk = nullptr;
-    std::vector<double> h_cost;          // per-body work estimate for the ownership split
+    std::vector<double> h_cost;          // per-body work estimate for the ownership split (device order)
+    std::vector<double> cost_override;   // caller-order work estimates from eph_set_body_costs (empty: built-in)
+    std::vector<int> h_orig;             // device order -> caller order
+    std::vector<int> h_own;              // current ownership [grid][kOwnMax] (device order, -1 padded)
     int grid = 0, per_cta = 0;           // current launch shape
     int req_grid = 0, req_per_cta = 0;   // requested by eph_set_launch (0 = automatic)
     int64_t launches = 0;
@@ -140,6 +144,7 @@ static int choose_shape(eph_ctx *ctx) {
     plan_ownership(ctx->h_cost.data(), n, grid, per, order.data(), load.data(), cnt.data(), own.data());
     cudaError_t e = cudaMemcpy(ctx->d_own, own.data(), own.size() * sizeof(int), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return fail(ctx, EPH_ERR_CUDA, "upload ownership", e);
+    ctx->h_own = own;
     ctx->grid = grid;
     ctx->per_cta = per;
     return EPH_OK;
@@ -171,8 +176,10 @@ static int prepare_constants(eph_ctx *ctx, const double *h_planes) {
         cst[CST_RING * ld + k] = P(EPH_P_RING_INDEX);
         const bool gp = P(EPH_P_GP_INDEX) >= 0, ring = P(EPH_P_RING_INDEX) >= 0;
         if (gp || ring) ext.push_back(k);
-        ctx->h_cost[k] = plan_cost(h_planes, n, i, k < ctx->n_full);
+        ctx->h_cost[k] = (int)ctx->cost_override.size() == n ? ctx->cost_override[i]
+                                                              : plan_cost(h_planes, n, i, k < ctx->n_full);
     }
+    ctx->h_orig = orig;
     if ((int)ext.size() > kMaxExt) return fail(ctx, EPH_ERR_ARG, "too many bodies with geopotential or ring models");
     ctx->n_ext = (int)ext.size();
     cudaError_t e = cudaMemcpy(ctx->d_cst, cst.data(), cst.size() * sizeof(double), cudaMemcpyHostToDevice);
@@ -410,6 +417,37 @@ int eph_set_launch(eph_ctx *ctx, int grid, int bodies_per_cta) {
     if (!ctx->n) return EPH_OK;
     CK(cudaSetDevice(ctx->device), "cudaSetDevice");
     return choose_shape(ctx);
+}
+
+int eph_set_body_costs(eph_ctx *ctx, const double *cost) {
+    if (!ctx) return EPH_ERR_ARG;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    if (!ctx->n) return fail(ctx, EPH_ERR_STATE, "no system uploaded");
+    const int n = ctx->n;
+    if (cost) {
+        for (int i = 0; i < n; ++i)
+            if (!(cost[i] > 0) || !std::isfinite(cost[i])) return fail(ctx, EPH_ERR_ARG, "eph_set_body_costs: costs must be positive");
+        ctx->cost_override.assign(cost, cost + n);
+    } else {
+        ctx->cost_override.clear();
+    }
+    std::vector<double> h_planes((size_t)EPH_NPLANES * n);
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    CK(cudaMemcpy(h_planes.data(), ctx->d_planes, h_planes.size() * sizeof(double), cudaMemcpyDeviceToHost),
+       "read planes");
+    int rc = prepare_constants(ctx, h_planes.data());
+    return rc ? rc : choose_shape(ctx);
+}
+
+int eph_get_ownership(const eph_ctx *ctx, int32_t *bodies, int *grid) {
+    if (!ctx || !bodies || !grid) return EPH_ERR_ARG;
+    if (!ctx->n || ctx->h_own.size() < (size_t)ctx->grid * kOwnMax) return EPH_ERR_STATE;
+    for (size_t q = 0; q < (size_t)ctx->grid * kOwnMax; ++q) {
+        const int k = ctx->h_own[q];
+        bodies[q] = k < 0 ? -1 : ctx->h_orig[k];
+    }
+    *grid = ctx->grid;
+    return EPH_OK;
 }
 
 int eph_get_launch(const eph_ctx *ctx, int *grid, int *bodies_per_cta) {

@@ -164,12 +164,14 @@ __device__ __forceinline__ double normalize2(double &a, double &b) {
 }
 __device__ __forceinline__ double normalize(v3 &v) { return normalize3(v.x, v.y, v.z); }
 
-// (I + R) rotates a vector about w by |w| t (vec_t.h:540-559)
+// (I + R) rotates a vector about w by |w| t (vec_t.h:540-559). sin(wt) and 2 sin^2(wt/2) come from one
+// sincos of the half angle (sin wt = 2 sin(wt/2) cos(wt/2)), one range reduction instead of two.
 __device__ __forceinline__ m3 rotation_matrix(v3 w, double t) {
     double x = w.x, y = w.y, z = w.z;
     double wt = normalize3(x, y, z) * t;
-    double st = sin(wt), st222 = sin(wt / 2);
-    st222 *= 2 * st222;
+    double sh, ch;
+    sincos(wt / 2, &sh, &ch);
+    const double st = 2 * sh * ch, st222 = 2 * sh * sh;
     m3 dr{{x * x - 1, x * y, x * z}, {x * y, y * y - 1, y * z}, {x * z, y * z, z * z - 1}};
     dr = st222 * dr;
     dr.x.y += z * st;

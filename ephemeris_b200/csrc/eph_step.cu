@@ -80,6 +80,7 @@ struct Scratch {
     int split[kOwnMax + 1];           // warp groups of a pass-A re-sweep (equal split of the active bodies)
     int split_a0[kOwnMax + 1];        // warp groups of the first pass-A sweep (all owned bodies, weighted)
     int split_b[kOwnMax + 1];         // warp groups of the pass-B sweep (all owned bodies, weighted)
+    int nw_b;                         // warps of the pass-B sweep (the last one sums host reactions meanwhile)
     double ext[kOwnMax][kMaxExt][3];  // other hosts' fields on the owned bodies (geopotential, or ring)
     double ext2[kOwnMax][kMaxExt][3]; // ring half of a host that has both models
     double react[kOwnMax][6];         // summed reactions of owned hosts
@@ -167,15 +168,18 @@ __device__ __forceinline__ void mbar_init(Scratch &sc) {
     __syncthreads();
 }
 
-// Copy `rows` planes (row r from src[r] + j0, `count` bodies rounded up to kPad) into tile rows of
-// `stride` doubles. Every thread waits for completion (bounded). Returns false on timeout.
+// Copy `rows` planes (row r from src[r] + j0, `count` bodies rounded up to kPad; rows from `tail_from` on
+// `count_tail` bodies; a null src[r] keeps tile row r as it is) into tile rows of `stride` doubles. Every
+// thread waits for completion (bounded). Returns false on timeout.
 __device__ bool load_tile(const SysDev &S, Scratch &sc, TileState &ts, double *tile, int stride,
                           const double *const *src, int rows, int j0, int count, int count_tail, int tail_from) {
     __syncthreads();   // the previous sweep's reads of the tile are done
     const int cpad = (count + kPad - 1) / kPad * kPad;
     const int tpad = (count_tail + kPad - 1) / kPad * kPad;
     const unsigned bytes = (unsigned)cpad * 8u, tbytes = (unsigned)tpad * 8u;
-    const unsigned total = bytes * (unsigned)tail_from + tbytes * (unsigned)(rows - tail_from);
+    unsigned total = 0;
+    for (int r = 0; r < rows; ++r)
+        if (src[r]) total += r < tail_from ? bytes : tbytes;
     const unsigned mb = smem_addr(&sc.mbar);
     if (threadIdx.x == 0) {
         // order the generic-proxy accesses (tile reads, other CTAs' global stores) before the copies
@@ -184,7 +188,7 @@ __device__ bool load_tile(const SysDev &S, Scratch &sc, TileState &ts, double *t
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(total) : "memory");
         for (int r = 0; r < rows; ++r) {
             const unsigned nbytes = r < tail_from ? bytes : tbytes;
-            if (nbytes == 0) continue;
+            if (nbytes == 0 || !src[r]) continue;
             asm volatile(
                 "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
                     smem_addr(tile + (size_t)r * stride)),
@@ -906,41 +910,45 @@ __device__ bool pass_a(const SysDev &S, Own *own, int nb, int buf, bool deform_o
     } else {
         __syncthreads();
     }
-    // the extended bodies' fields run on the last kExtWarps warps alongside the first sweep and the
-    // first angular-velocity update (one tile only: streaming tiles needs every warp)
+    // The extended bodies' fields do not depend on the angular velocity: they run on the last kExtWarps warps
+    // alongside every pass-A sweep and angular-velocity update of the stage (one tile only: streaming tiles
+    // needs every warp, and the fields then run after the first sweep).
     const bool ext_overlap = !deform_only && S.n_ext > 0 && one_tile;
     const int max_iter = deform_only ? 1 : 4;   // MAX_ANGULAR_VELOCITY_ITER (mass.impl:74)
-    #pragma unroll 1
-    for (int it = 0; it < max_iter; ++it) {
-        const int nw = (it == 0 && ext_overlap) ? kWarps - kExtWarps : kWarps;
-        if ((threadIdx.x >> 5) < nw) {
+    const int nw = ext_overlap ? kWarps - kExtWarps : kWarps;
+    if ((threadIdx.x >> 5) < nw) {
+        #pragma unroll 1
+        for (int it = 0; it < max_iter; ++it) {
             unsigned mask = 0;
             for (int b = 0; b < nb; ++b) {
                 // the pair sums depend on the angular velocity only for delayed tides
                 if (it == 0 || (!own[b].converged && own[b].kind == 2)) mask |= 1u << b;
             }
             if (!sweep_a(S, own, nb, mask, buf, sc, ts, tile, one_tile, nw, it == 0 ? sc.split_a0 : nullptr)) return false;
+            if (S.timers && threadIdx.x == 0) sc.t_phase[PH_A_COUNT] += 1;
             mark(S, sc, PH_A_SWEEP);   // thread 0 sits in a sweep warp
             // harmonics and angular velocity of the owned bodies: warp b updates body b
             {
                 const int wb = threadIdx.x >> 5;
                 if (wb < nb && !own[wb].converged) update_warp(own[wb], threadIdx.x & 31, deform_only);
             }
-            if (nw < kWarps) mark(S, sc, PH_A_UPDATE);
-        } else {
-            ext_fields(S, own, nb, buf, sc, kWarps - kExtWarps);
+            part_sync(nw * 32);
+            mark(S, sc, PH_A_UPDATE);
+            if (!deform_only && it == 0 && S.n_ext > 0 && !one_tile) {
+                __syncthreads();   // nw == kWarps here
+                ext_fields(S, own, nb, buf, sc, 0);
+                __syncthreads();
+                mark(S, sc, PH_B_EXT);
+            }
+            int all = 1;
+            for (int b = 0; b < nb; ++b) all &= own[b].converged;
+            if (all) break;
         }
-        if (!deform_only && it == 0 && S.n_ext > 0 && !one_tile) {
-            __syncthreads();
-            ext_fields(S, own, nb, buf, sc, 0);
-        }
-        __syncthreads();
-        // iteration 0 with the extended-body warps: the wait for them beyond sweep + update
-        mark(S, sc, nw == kWarps ? PH_A_UPDATE : PH_B_EXT);
-        int all = 1;
-        for (int b = 0; b < nb; ++b) all &= own[b].converged;
-        if (all) break;
+    } else {
+        ext_fields(S, own, nb, buf, sc, kWarps - kExtWarps);
     }
+    __syncthreads();
+    mark(S, sc, PH_B_EXT);   // the wait for the field warps beyond the sweeps and updates
     if (deform_only) return true;
     // PREPARE_RELATIVITY (mass.impl:76-80) and the pass-A outputs other CTAs read in pass B
     const double c2 = kC * kC;
@@ -1058,6 +1066,8 @@ __device__ bool pass_b(const SysDev &S, Own *own, int nb, int buf, Scratch &sc, 
     const int ld = S.ld, n = S.n, T = S.tile;
     const double *pub = S.pub + (size_t)buf * PUB_NPLANES * ld;
     const double *aux = S.aux, *cst = S.cst;
+    const int nwb = sc.nw_b;
+    const bool sweeper = (threadIdx.x >> 5) < nwb;
     const Group g = group_of(sc.split_b, nb);
     const Own &o = own[g.slot];
     double acc[9];
@@ -1068,13 +1078,17 @@ __device__ bool pass_b(const SysDev &S, Own *own, int nb, int buf, Scratch &sc, 
     for (int j0 = 0; j0 < n; j0 += T) {
         const int cnt = min(T, n - j0);
         const int cnt_full = max(0, min(cnt, S.n_full - j0));
-        // rows every body needs, then rows only full-class bodies need
+        // rows every body needs, then rows only full-class bodies need; with one tile the positions, GM
+        // and sR2 are still in the tile from pass A of this stage (`reuse`)
+        const bool reuse = n <= T;
         const double *src[TB_ROWS] = {
-            pub + (PUB_R_HI + 0) * ld, pub + (PUB_R_HI + 1) * ld, pub + (PUB_R_HI + 2) * ld,
-            pub + (PUB_R_LO + 0) * ld, pub + (PUB_R_LO + 1) * ld, pub + (PUB_R_LO + 2) * ld, pub + PUB_GM * ld,
-            aux + AUX_PHI * ld, aux + (AUX_NACC + 0) * ld, aux + (AUX_NACC + 1) * ld, aux + (AUX_NACC + 2) * ld,
-            aux + (AUX_BETA + 0) * ld, aux + (AUX_BETA + 1) * ld, aux + (AUX_BETA + 2) * ld, aux + AUX_BETA2 * ld,
-            cst + CST_SR2 * ld,
+            reuse ? nullptr : pub + (PUB_R_HI + 0) * ld, reuse ? nullptr : pub + (PUB_R_HI + 1) * ld,
+            reuse ? nullptr : pub + (PUB_R_HI + 2) * ld, reuse ? nullptr : pub + (PUB_R_LO + 0) * ld,
+            reuse ? nullptr : pub + (PUB_R_LO + 1) * ld, reuse ? nullptr : pub + (PUB_R_LO + 2) * ld,
+            aux + (AUX_NACC + 0) * ld, aux + (AUX_NACC + 1) * ld, aux + (AUX_NACC + 2) * ld,
+            aux + (AUX_BETA + 0) * ld, aux + (AUX_BETA + 1) * ld, aux + (AUX_BETA + 2) * ld,
+            reuse ? nullptr : pub + PUB_GM * ld, reuse ? nullptr : cst + CST_SR2 * ld,
+            aux + AUX_PHI * ld, aux + AUX_BETA2 * ld,
             pub + (PUB_GL + 0) * ld, pub + (PUB_GL + 1) * ld, pub + (PUB_GL + 2) * ld,
             aux + (AUX_CPOT + 0) * ld, aux + (AUX_CPOT + 1) * ld, aux + (AUX_CPOT + 2) * ld,
             aux + (AUX_CPOT + 3) * ld, aux + (AUX_CPOT + 4) * ld, aux + (AUX_CPOT + 5) * ld,
@@ -1082,6 +1096,7 @@ __device__ bool pass_b(const SysDev &S, Own *own, int nb, int buf, Scratch &sc, 
             cst + CST_R2 * ld, cst + CST_LUM * ld};
         if (!load_tile(S, sc, ts, tile, T, src, TB_ROWS, j0, cnt, cnt_full, kTileBFullRows)) return false;
         const int self = o.idx - j0;
+        if (!sweeper) continue;
         if (o.full) {
             sweep_b_range<true, true>(o, tile, T, 0, cnt_full, self, g, acc, x);
             sweep_b_range<true, false>(o, tile, T, cnt_full, cnt, self, g, acc, x);
@@ -1090,33 +1105,54 @@ __device__ bool pass_b(const SysDev &S, Own *own, int nb, int buf, Scratch &sc, 
             sweep_b_range<false, false>(o, tile, T, cnt_full, cnt, self, g, acc, x);
         }
     }
-    // exact extremes with the reference's expressions
-    double red_in[11];
-#pragma unroll
-    for (int c = 0; c < 9; ++c) red_in[c] = acc[c];
-    {
-        const double rr2 = 1.0 / x.m_min;
-        red_in[9] = sqrt(rr2);                                // +inf -> 0 when no pair was seen
-        if (x.tq != x.tq) red_in[10] = x.tq;
-        else if (x.tq > 0) {
-            const double r2 = 1.0 / x.tq_m;
-            red_in[10] = r2 * (sqrt(r2) * x.tq_gm);
-        } else red_in[10] = 0.0;
-    }
     __shared__ double red[kOwnMax][16];
-    group_reduce<11>(red_in, sc.split_b, nb, kWarps, sc, red, 9);
-    if (threadIdx.x < nb) {
-        Own &ob = own[threadIdx.x];
-        const double *rr = red[threadIdx.x];
-        for (int c = 0; c < 3; ++c) { ob.gacc[c] = rr[c]; ob.dacc[c] = rr[3 + c]; ob.dtq[c] = rr[6 + c]; }
-        checked_maximize(ob.mind, rr[9]);
-        checked_maximize(ob.maxi, rr[10]);
+    if (sweeper) {
+        // exact extremes with the reference's expressions
+        double red_in[11];
+#pragma unroll
+        for (int c = 0; c < 9; ++c) red_in[c] = acc[c];
+        {
+            const double rr2 = 1.0 / x.m_min;
+            red_in[9] = sqrt(rr2);                                // +inf -> 0 when no pair was seen
+            if (x.tq != x.tq) red_in[10] = x.tq;
+            else if (x.tq > 0) {
+                const double r2 = 1.0 / x.tq_m;
+                red_in[10] = r2 * (sqrt(r2) * x.tq_gm);
+            } else red_in[10] = 0.0;
+        }
+        group_reduce<11>(red_in, sc.split_b, nb, nwb, sc, red, 9);
+        if (threadIdx.x < nb) {
+            Own &ob = own[threadIdx.x];
+            const double *rr = red[threadIdx.x];
+            for (int c = 0; c < 3; ++c) { ob.gacc[c] = rr[c]; ob.dacc[c] = rr[3 + c]; ob.dtq[c] = rr[6 + c]; }
+            checked_maximize(ob.mind, rr[9]);
+            checked_maximize(ob.maxi, rr[10]);
+        }
+    } else {
+        // the last warp: reactions of the owned extended bodies, the sum over all bodies i of the table
+        // written in pass A (lane-strided over i, then a butterfly over the warp)
+        const int lane = threadIdx.x & 31;
+        #pragma unroll 1
+        for (int b = 0; b < nb; ++b) {
+            const int e = own[b].ext_slot;
+            if (e < 0) continue;
+            double part[6] = {0, 0, 0, 0, 0, 0};
+            const double *rc = S.react + (size_t)e * ld * 12;   // [i][geopotential, ring][6]
+            #pragma unroll 1
+            for (int i = lane; i < n; i += 32)
+                for (int c = 0; c < 6; ++c) part[c] += __ldcg(rc + (size_t)i * 12 + c) + __ldcg(rc + (size_t)i * 12 + 6 + c);
+            for (int c = 0; c < 6; ++c) {
+                const double v = warp_sum(part[c]);
+                if (lane == c) sc.react[b][c] = v;
+            }
+        }
     }
     __syncthreads();
     mark(S, sc, PH_B_SWEEP);
-    // reactions of the owned extended bodies: sum over all bodies i of the table written in pass A
+    // reactions of the owned extended bodies, when every warp swept: sum over all bodies i of the table
+    // written in pass A
     #pragma unroll 1
-    for (int b = 0; b < nb; ++b) {
+    for (int b = 0; b < (nwb == kWarps ? nb : 0); ++b) {
         const int e = own[b].ext_slot;
         if (e < 0) continue;   // uniform over the CTA
         double part[6] = {0, 0, 0, 0, 0, 0};
@@ -1272,22 +1308,30 @@ __device__ void rk_stage(const SysDev &S, Own *own, int nb, int s, long long i_s
         // increments R (rotation_matrix of a zero vector), so its frame keeps s0 exactly: skip the passes.
         const bool still = wv.x == 0 && wv.y == 0 && wv.z == 0 && dwv.x == 0 && dwv.y == 0 && dwv.z == 0 &&
                            (k != kStages || (eg.x == 0 && eg.y == 0 && eg.z == 0));
-        // s += R % fast(s), element (col, row) = sum_m R[m][row] * s[col][m]
-        #pragma unroll 1
-        for (int pass = 0; pass < (still ? 0 : (k == kStages ? 3 : 2)); ++pass) {
-            m3 R = pass == 0 ? rotation_matrix(wv - dwv, dt * dt_k / 2)
-                 : pass == 1 ? rotation_matrix(wv + dwv, dt * dt_k / 2)
-                             : rotation_matrix(ldv(o.Egrad), 1.0 / 72);
-            double add = 0;
-            if (lane < 9) {
-                const int col = lane / 3, row = lane % 3;
-                const v3 sc = fast3(o.s + 3 * col);
-                const double *Rr = &R.x.x;   // R column m at Rr[3m]
-                add = (Rr[0 + row] * sc.x + Rr[3 + row] * sc.y) + Rr[6 + row] * sc.z;
+        // s += R % fast(s), element (col, row) = sum_m R[m][row] * s[col][m], for the passes R0 (w - dw),
+        // R1 (w + dw) and, at the last stage, R2 (Egrad). The increment matrices depend only on w, dw and
+        // Egrad, so every lane builds the one of its pass (lanes 9p .. 9p+8 apply pass p) at the same time;
+        // the passes are then applied in order.
+        const int npass = still ? 0 : (k == kStages ? 3 : 2);
+        if (npass) {
+            const int my = min(lane / 9, 2);
+            const m3 R = my == 0 ? rotation_matrix(wv - dwv, dt * dt_k / 2)
+                       : my == 1 ? rotation_matrix(wv + dwv, dt * dt_k / 2)
+                                 : rotation_matrix(eg, 1.0 / 72);
+            const double *Rr = &R.x.x;   // R column m at Rr[3m]
+            const int q = lane - 9 * my, col = q / 3, row = q % 3;
+            #pragma unroll 1
+            for (int pass = 0; pass < npass; ++pass) {
+                const bool mine = my == pass && q < 9;
+                double add = 0;
+                if (mine) {
+                    const v3 sc = fast3(o.s + 3 * col);
+                    add = (Rr[0 + row] * sc.x + Rr[3 + row] * sc.y) + Rr[6 + row] * sc.z;
+                }
+                __syncwarp();
+                if (mine) o.s[q] = dd_add(o.s[q], dd_make(add));
+                __syncwarp();
             }
-            __syncwarp();
-            if (lane < 9) o.s[lane] = dd_add(o.s[lane], dd_make(add));
-            __syncwarp();
         }
         if (k == kStages) {
             // mass::orthogonalize (mass.h:147-150): s += 0.5 fmis % (1 - fmis^T % fmis)
@@ -1359,7 +1403,12 @@ __global__ void __launch_bounds__(kThreads, 1) step_kernel(SysDev S, StepParams 
         for (int b = 0; b < nb; ++b) wt[b] = own[b].kind == 2 ? 8 : 1;
         split_warps(wt, nb, ext_overlap ? kWarps - kExtWarps : kWarps, sc.split_a0);
         for (int b = 0; b < nb; ++b) wt[b] = own[b].full ? 2 : 1;
-        split_warps(wt, nb, kWarps, sc.split_b);
+        // a CTA that owns geopotential / ring hosts sums their reactions on its last warp during the
+        // pass-B sweep (one tile only: streaming tiles needs every warp for the copies)
+        bool host = false;
+        for (int b = 0; b < nb; ++b) host |= own[b].ext_slot >= 0;
+        sc.nw_b = (host && S.n <= S.tile && nb < kWarps) ? kWarps - 1 : kWarps;
+        split_warps(wt, nb, sc.nw_b, sc.split_b);
     }
     auto sync = [&]() {
         bool ok = grid_sync(S, sc);

@@ -24,7 +24,7 @@ namespace eph {
 
 constexpr int kThreads = 512;        // threads per CTA (16 warps; <= 128 registers per thread)
 constexpr int kWarps = kThreads / 32;
-constexpr int kExtWarps = 4;         // warps computing extended-body fields during the first pass-A sweep
+constexpr int kExtWarps = 4;         // warps computing extended-body fields during the pass-A sweeps
 constexpr int kOwnMax = 8;           // bodies owned by one CTA (private state lives in shared memory)
 constexpr int kStages = 25;          // Feagin RK12 stages
 constexpr int kMaxExt = 64;          // extended bodies (geopotential or ring) per system
@@ -46,9 +46,10 @@ enum ConstPlane { CST_SR2 = 0, CST_TDF = 1, CST_R2 = 2, CST_LUM = 3, CST_R = 4, 
 // planes staged into shared memory for the pass-A sweep (tile rows)
 enum TileA { TA_R_HI = 0, TA_R_LO = 3, TA_V_HI = 6, TA_V_LO = 9, TA_GM = 12, TA_SR2 = 13, TA_TDF = 14, TA_ROWS = 15 };
 // planes staged for the pass-B sweep: rows every body needs, then (from kTileBFullRows) rows only
-// bodies of the full class need, staged for the full-class prefix of the tile only
-enum TileB { TB_R_HI = 0, TB_R_LO = 3, TB_GM = 6, TB_PHI = 7, TB_NACC = 8, TB_BETA = 11, TB_BETA2 = 14,
-             TB_SR2 = 15, TB_GL = 16, TB_CPOT = 19, TB_R2 = 28, TB_LUM = 29, TB_ROWS = 30 };
+// bodies of the full class need, staged for the full-class prefix of the tile only. Positions, GM and sR2
+// sit in the rows pass A staged them in: when the whole system fits one tile they are not copied again.
+enum TileB { TB_R_HI = TA_R_HI, TB_R_LO = TA_R_LO, TB_NACC = 6, TB_BETA = 9, TB_GM = TA_GM, TB_SR2 = TA_SR2,
+             TB_PHI = 14, TB_BETA2 = 15, TB_GL = 16, TB_CPOT = 19, TB_R2 = 28, TB_LUM = 29, TB_ROWS = 30 };
 constexpr int kTileBFullRows = TB_GL;
 constexpr int kTileRows = TB_ROWS;
 
@@ -89,8 +90,9 @@ enum TrajField { TR_R_HI = 0, TR_R_LO = 3, TR_GM = 6, TR_PHI = 7, TR_NACC = 8, T
                  kTrajRec = 48 };
 
 // phases of a stage evaluation, for the optional per-CTA phase timers
+// (slot PH_A_COUNT counts the pass-A sweeps instead of nanoseconds)
 enum Phase { PH_IO = 0, PH_RK = 1, PH_BARRIER = 2, PH_A_SWEEP = 3, PH_A_UPDATE = 4, PH_B_SWEEP = 5,
-             PH_B_EXT = 6, PH_B_FINAL = 7, kPhases = 8 };
+             PH_B_EXT = 6, PH_B_FINAL = 7, PH_A_COUNT = 8, kPhases = 9 };
 
 enum Mode { MODE_INTEGRATE = 0, MODE_ACCEL = 1, MODE_DEFORM = 2 };
 

@@ -131,15 +131,33 @@ class Context:
     def launches(self) -> int:
         return int(self.lib.eph_launch_count(self.h))
 
-    PHASES = ("io", "rk", "barrier", "a_sweep", "a_update", "b_sweep", "b_ext", "b_final")
+    def set_body_costs(self, cost=None):
+        """Per-body work estimates (caller order) for the ownership split; None restores the built-in ones."""
+        if cost is None:
+            check(self.lib.eph_set_body_costs(self.h, None), self.h, "set_body_costs")
+            return
+        c = np.ascontiguousarray(cost, dtype=np.float64)
+        check(self.lib.eph_set_body_costs(self.h, c.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), self.h,
+              "set_body_costs")
+
+    def ownership(self) -> np.ndarray:
+        """[grid, 8] caller indices of the bodies each CTA owns (-1 padded)."""
+        out = np.full(1024 * 8, -1, np.int32)
+        g = ctypes.c_int()
+        check(self.lib.eph_get_ownership(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                         ctypes.byref(g)), self.h, "get_ownership")
+        return out[:g.value * 8].reshape(g.value, 8)
+
+    PHASES = ("io", "rk", "barrier", "a_sweep", "a_update", "b_sweep", "b_ext", "b_final", "a_sweeps")
 
     def profile_phases(self, enable: bool = True):
         check(self.lib.eph_profile_phases(self.h, 1 if enable else 0), self.h, "profile_phases")
 
     def phase_times(self) -> np.ndarray:
-        """[grid, 8] nanoseconds per phase of the last launch (profiling must be on)."""
+        """[grid, 9] nanoseconds per phase of the last launch (profiling must be on); the last column counts
+        the pass-A sweeps."""
         g, p = self.launch_shape()
-        out = np.zeros(max(g, 1) * 8, np.uint64)
+        out = np.zeros(max(g, 1) * len(self.PHASES), np.uint64)
         gg, pp = ctypes.c_int(), ctypes.c_int()
         check(self.lib.eph_phase_times(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)),
                                        ctypes.byref(gg), ctypes.byref(pp)), self.h, "phase_times")

@@ -88,17 +88,28 @@ int eph_deform(eph_ctx *ctx);
  * the context's own stream). Calls still return only after their work has finished. */
 int eph_set_stream(eph_ctx *ctx, void *stream);
 
-/* Launch shape: grid = CTAs (0: automatic), bodies_per_cta (0: automatic). Used by the autotuner. */
+/* Launch shape: grid = CTAs (0: automatic), bodies_per_cta (0: automatic, at most EPH_MAX_BODIES_PER_CTA).
+ * The reference fixes its shape in code (RungeKutta.cu:80-88). */
+#define EPH_MAX_BODIES_PER_CTA 8
 int eph_set_launch(eph_ctx *ctx, int grid, int bodies_per_cta);
 /* Current launch shape. */
 int eph_get_launch(const eph_ctx *ctx, int *grid, int *bodies_per_cta);
+/* Work estimates of the uploaded system's bodies (cost[n] > 0, caller order) that the split of bodies over
+ * CTAs balances (longest processing time first); NULL restores the built-in estimate. Re-plans at once; an
+ * upload keeps the override while the body count stays the same. */
+int eph_set_body_costs(eph_ctx *ctx, const double *cost);
+/* Bodies owned by each CTA of the current launch: bodies[grid][EPH_MAX_BODIES_PER_CTA], caller indices,
+ * -1 padded (`bodies` must hold that many entries for the largest grid, i.e. the co-resident CTA count). */
+int eph_get_ownership(const eph_ctx *ctx, int32_t *bodies, int *grid);
 /* Kernel launches issued on this context so far. */
 int64_t eph_launch_count(const eph_ctx *ctx);
 
 /* Profiling aid: with enable != 0 every launch records, per CTA, the nanoseconds spent in each phase
  * of the step (load/store, RK combination, barrier waits, pass-A sweeps, pass-A updates, pass-B sweeps,
- * extended-body forces, finalisation). eph_phase_times copies the last launch's [grid][phases] table
- * (out must hold grid*8 values; grid = CTAs of the current launch shape). */
+ * wait for the extended-body fields, finalisation) and, in the last slot, the number of pass-A sweeps.
+ * eph_phase_times copies the last launch's [grid][EPH_PHASES] table (out must hold grid*EPH_PHASES values;
+ * grid = CTAs of the current launch shape). */
+#define EPH_PHASES 9
 int eph_profile_phases(eph_ctx *ctx, int enable);
 int eph_phase_times(eph_ctx *ctx, uint64_t *out, int *grid, int *phases);
 

@@ -34,8 +34,8 @@ HERE = os.path.join(ROOT, "tests", "golden")
 SYSTEMS = {
     # name: (generator, kwargs, stored text files?, steps to record)
     "config1": ("config1", {}, True, [1, 10, 1000]),
-    "small_full": ("small_full", {}, True, [1, 10]),
-    "config2": ("config2", {}, False, [1]),
+    "small_full": ("small_full", {}, True, [1, 10, 100, 1000]),
+    "config2": ("config2", {}, False, [1, 1000]),
 }
 
 
