@@ -91,7 +91,7 @@ SIGNATURES = [
     ("eph_bspline_fit_batch", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int64, ctypes.c_int64, ctypes.c_int,
                                               ctypes.c_int64, _D, _D]),
     ("eph_geopotential_field", ctypes.c_int, [ctypes.c_int, _D, ctypes.c_int, ctypes.c_int, ctypes.c_double,
-                                               ctypes.c_int64, _D, _D]),
+                                               ctypes.c_int, ctypes.c_int64, _D, _D]),
     ("eph_fp64_fma_rate", ctypes.c_int, [ctypes.c_int, _D]),
     ("eph_integrate_noalloc", ctypes.c_int, [ctypes.c_int, _VP, ctypes.c_int64, _VP, ctypes.POINTER(EphModels),
                                              ctypes.c_double, ctypes.c_int64, _D, _D]),

@@ -218,10 +218,10 @@ int eph_upload_system(eph_ctx *ctx, int64_t n64, const double *planes, const eph
         const int ld = (n + kPad - 1) / kPad * kPad;
         CK(cudaMalloc(&ctx->d_pub, (size_t)2 * PUB_NPLANES * ld * sizeof(double)), "cudaMalloc(public state)");
         CK(cudaMalloc(&ctx->d_aux, (size_t)AUX_NPLANES * ld * sizeof(double)), "cudaMalloc(aux)");
-        CK(cudaMalloc(&ctx->d_react, (size_t)kMaxExt * ld * 12 * sizeof(double)), "cudaMalloc(reactions)");
+        CK(cudaMalloc(&ctx->d_react, (size_t)kMaxExt * ld * 18 * sizeof(double)), "cudaMalloc(reactions)");
         CK(cudaMalloc(&ctx->d_cst, (size_t)CST_NPLANES * ld * sizeof(double)), "cudaMalloc(constants)");
         CK(cudaMemset(ctx->d_aux, 0, (size_t)AUX_NPLANES * ld * sizeof(double)), "cudaMemset");
-        CK(cudaMemset(ctx->d_react, 0, (size_t)kMaxExt * ld * 12 * sizeof(double)), "cudaMemset");
+        CK(cudaMemset(ctx->d_react, 0, (size_t)kMaxExt * ld * 18 * sizeof(double)), "cudaMemset");
         CK(cudaMalloc(&ctx->d_ext, (size_t)kMaxExt * sizeof(int)), "cudaMalloc(ext)");
         CK(cudaMalloc(&ctx->d_own, (size_t)n * kOwnMax * sizeof(int)), "cudaMalloc(ownership)");
         CK(cudaMalloc(&ctx->d_orig, (size_t)n * sizeof(int)), "cudaMalloc(order)");
@@ -314,12 +314,14 @@ static int run(eph_ctx *ctx, const StepParams &P) {
     S.ld = ctx->ld;
     S.tile = ctx->tile;
     S.react = ctx->d_react;
+    S.react_cta = ctx->d_react + (size_t)kMaxExt * ctx->ld * 12;
     S.n_ext = ctx->n_ext;
     S.pub = ctx->d_pub;
     S.aux = ctx->d_aux;
     S.cst = ctx->d_cst;
     S.planes = ctx->d_planes;
     S.ext_body = ctx->d_ext;
+    S.n_gp = ctx->n_gp;
     S.gp_nz = ctx->d_gp_nz;
     S.gp_nt = ctx->d_gp_nt;
     S.gp_coef = ctx->d_gp_coef;

@@ -1,5 +1,5 @@
 // eph_fields.cu - direct evaluation of an extended body's geopotential field on the device, with the same
-// device function the step and particle kernels use (gp_field, eph_models.cuh). It is what
+// device functions the step kernel (gp_field_lanes) and the particle kernels (gp_field) use. It is what
 // geopotential::sum (src/physics/geopotential.h:36) offers the reference's own known-answer test
 // (src/tests/test_geopotential.cpp), so the device evaluation can be held to that test's bound.
 #include <cuda_runtime.h>
@@ -10,6 +10,7 @@
 
 namespace eph {
 
+// one point per thread (gp_field: the massless-particle kernels' evaluation)
 __global__ void gp_field_kernel(const double *__restrict__ coef, int nz, int nt, double R, long long count,
                                 const double *__restrict__ r, double *__restrict__ out) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -20,11 +21,30 @@ __global__ void gp_field_kernel(const double *__restrict__ coef, int nz, int nt,
     out[3 * i + 2] = a.z;
 }
 
+// one point per group of 8 lanes (gp_field_lanes: the single-system step kernel's evaluation)
+__global__ void gp_field_lanes_kernel(const double *__restrict__ coef, int nz, int nt, double R, long long count,
+                                      const double *__restrict__ r, double *__restrict__ out) {
+    __shared__ double X[kGpX];
+    gp_expand(coef, nz, nt, X, threadIdx.x, blockDim.x);
+    __syncthreads();
+    const long long i = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / 8;
+    if (i >= count) return;   // uniform over the group
+    const int lane = threadIdx.x & 31;
+    const v3 a = gp_field_lanes<8>(X, GP_RCP, nz, nt, R, mk(r[3 * i], r[3 * i + 1], r[3 * i + 2]), lane & 7,
+                                   0xffu << (lane & ~7));
+    if ((lane & 7) == 0) {
+        out[3 * i] = a.x;
+        out[3 * i + 1] = a.y;
+        out[3 * i + 2] = a.z;
+    }
+}
+
 }  // namespace eph
 
-extern "C" int eph_geopotential_field(int device, const double *coef, int nz, int nt, double R, int64_t count,
-                                      const double *r, double *out) {
-    if (!coef || !r || !out || count < 0 || nz < 0 || nz > EPH_GP_MAX_DEGREE || nt < 0 || nt > nz)
+extern "C" int eph_geopotential_field(int device, const double *coef, int nz, int nt, double R, int lanes,
+                                      int64_t count, const double *r, double *out) {
+    if (!coef || !r || !out || count < 0 || nz < 0 || nz > EPH_GP_MAX_DEGREE || nt < 0 || nt > nz ||
+        (lanes != 1 && lanes != 8))
         return EPH_ERR_ARG;
     if (count == 0) return EPH_OK;
     int prev = -1;
@@ -44,8 +64,9 @@ extern "C" int eph_geopotential_field(int device, const double *coef, int nz, in
     }
     if (rc == EPH_OK) {
         const int threads = 128;
-        const long long blocks = (count + threads - 1) / threads;
-        eph::gp_field_kernel<<<(unsigned)blocks, threads>>>(d_coef, nz, nt, R, count, d_r, d_out);
+        const long long blocks = (count * lanes + threads - 1) / threads;
+        if (lanes == 1) eph::gp_field_kernel<<<(unsigned)blocks, threads>>>(d_coef, nz, nt, R, count, d_r, d_out);
+        else eph::gp_field_lanes_kernel<<<(unsigned)blocks, threads>>>(d_coef, nz, nt, R, count, d_r, d_out);
         if (cudaGetLastError() != cudaSuccess || cudaMemcpy(out, d_out, vb, cudaMemcpyDeviceToHost) != cudaSuccess)
             rc = EPH_ERR_CUDA;
     }

@@ -14,8 +14,10 @@
 
 namespace eph {
 
-// 1/k for the degree recursion (k = 1 .. EPH_GP_MAX_DEGREE + 1); index 0 unused.
-__device__ __constant__ const double GP_RCP[EPH_GP_MAX_DEGREE + 2] = {
+// 1/k for the degree recursion (k = 1 .. EPH_GP_MAX_DEGREE + 1); index 0 unused. Global memory, not
+// constant memory: the lanes of one evaluation group read different entries. The step kernel keeps a copy
+// in shared memory next to its copies of the coefficient tables (the recursion's loads sit on its chain).
+__device__ const double GP_RCP[EPH_GP_MAX_DEGREE + 2] = {
     0.0, 1.0, 1.0 / 2, 1.0 / 3, 1.0 / 4, 1.0 / 5, 1.0 / 6, 1.0 / 7, 1.0 / 8, 1.0 / 9};
 
 // Gradient of the spherical-harmonic potential of an extended body, per unit GM of the body, at the
@@ -40,14 +42,63 @@ __device__ __constant__ const double GP_RCP[EPH_GP_MAX_DEGREE + 2] = {
 // three gradient terms that read it: a_z of (k-1, m), a_x / a_y of (k-1, m-1) and of (k-1, m+1). Column 0
 // and 1 run to degree Nz + 1 (zonal terms), higher columns to Nt + 1; with kZonal only columns 0 and 1
 // run. T is double (plain FP64) or float (mixed precision; the caller scales far fields into range).
+// Column m of the recursion, from its diagonal value (vd, wd) = (V_mm, W_mm), adding every gradient term
+// that reads a value of the column to (ax, ay, az) (unscaled by 1/R^2).
 template <typename T, bool kZonal>
-__device__ __forceinline__ void gp_core(const double *__restrict__ tab, int Nz, int Nt, T R, T x, T y, T z, T &ax,
-                                        T &ay, T &az) {
-    ax = 0; ay = 0; az = 0;
+__device__ __forceinline__ void gp_column(const double *__restrict__ tab, const double *__restrict__ rcp, int Nz,
+                                          int Nt, int m, T zs, T rho2, T vd, T wd, T &ax, T &ay, T &az) {
+    const int klast = m <= 1 ? Nz + 1 : Nt + 1;
+    T v = vd, w = wd, vp = 0, wp = 0;   // (V, W) at degree k and k - 1 of column m
+#pragma unroll 1
+    for (int k = m; k <= klast; ++k) {
+        if (k > m) {   // (k - m) V_km = (2k-1) z R/r^2 V_{k-1,m} - (k+m-1) (R/r)^2 V_{k-2,m}
+            const T a = T(2 * k - 1) * zs, b = T(k + m - 1) * rho2, c = T(rcp[k - m]);
+            const T nv = (a * v - b * vp) * c, nw = (a * w - b * wp) * c;
+            vp = v; wp = w; v = nv; w = nw;
+        }
+        const int n = k - 1;   // degree of the coefficients that read (V, W)_km
+        if (n < 2) continue;
+        const double *cn = tab + (n * n - 4);
+        if (m == 0) {
+            if (n <= Nz) az += T(n + 1) * (T(cn[0]) * v);                 // -C_n0 = J_n, W_k0 = 0
+        } else if (!kZonal && m <= n && n <= Nt) {
+            az -= T(n - m + 1) * (T(cn[2 * m - 1]) * v + T(cn[2 * m]) * w);
+        }
+        if (m == 1) {
+            if (n <= Nz) {
+                const T J = T(cn[0]);
+                ax += J * v;
+                ay += J * w;
+            }
+        } else if (!kZonal && m >= 2 && n <= Nt) {                            // order m - 1 >= 1
+            const T C = T(cn[2 * m - 3]), S = T(cn[2 * m - 2]);
+            ax -= T(0.5) * (C * v + S * w);
+            ay += T(0.5) * (S * v - C * w);
+        }
+        if (!kZonal && m + 1 <= n && n <= Nt) {                               // order m + 1
+            const T C = T(cn[2 * m + 1]), S = T(cn[2 * m + 2]);
+            const T f = T(0.5) * T((k - m) * (k - m - 1));
+            ax += f * (C * v + S * w);
+            ay += f * (S * v - C * w);
+        }
+    }
+}
+
+// Common set-up of a field evaluation: (x, y, z) R / r^2, (R / r)^2 and V_00 = R / r.
+template <typename T>
+__device__ __forceinline__ void gp_setup(T R, T x, T y, T z, T &xs, T &ys, T &zs, T &rho2, T &v00) {
     const T ir2 = T(1) / (x * x + y * y + z * z);
     const T q = R * ir2;
-    const T xs = x * q, ys = y * q, zs = z * q, rho2 = R * q;   // (x, y, z) R / r^2, (R / r)^2
-    T vd = R * sqrt(ir2), wd = 0;                               // V_00 = R / r, W_00 = 0
+    xs = x * q; ys = y * q; zs = z * q; rho2 = R * q;
+    v00 = R * sqrt(ir2);
+}
+
+template <typename T, bool kZonal>
+__device__ __forceinline__ void gp_core(const double *__restrict__ tab, const double *__restrict__ rcp, int Nz, int Nt,
+                                        T R, T x, T y, T z, T &ax, T &ay, T &az) {
+    ax = 0; ay = 0; az = 0;
+    T xs, ys, zs, rho2, vd, wd = 0;
+    gp_setup(R, x, y, z, xs, ys, zs, rho2, vd);
     const int mlast = kZonal ? 1 : max(Nt + 1, 1);
 #pragma unroll 1
     for (int m = 0; m <= mlast; ++m) {
@@ -57,50 +108,93 @@ __device__ __forceinline__ void gp_core(const double *__restrict__ tab, int Nz, 
             vd = nv;
             wd = nw;
         }
-        const int klast = m <= 1 ? Nz + 1 : Nt + 1;
-        T v = vd, w = wd, vp = 0, wp = 0;   // (V, W) at degree k and k - 1 of column m
-#pragma unroll 1
-        for (int k = m; k <= klast; ++k) {
-            if (k > m) {   // (k - m) V_km = (2k-1) z R/r^2 V_{k-1,m} - (k+m-1) (R/r)^2 V_{k-2,m}
-                const T a = T(2 * k - 1) * zs, b = T(k + m - 1) * rho2, c = T(GP_RCP[k - m]);
-                const T nv = (a * v - b * vp) * c, nw = (a * w - b * wp) * c;
-                vp = v; wp = w; v = nv; w = nw;
-            }
-            const int n = k - 1;   // degree of the coefficients that read (V, W)_km
-            if (n < 2) continue;
-            const double *cn = tab + (n * n - 4);
-            if (m == 0) {
-                if (n <= Nz) az += T(n + 1) * (T(__ldg(cn)) * v);                 // -C_n0 = J_n, W_k0 = 0
-            } else if (!kZonal && m <= n && n <= Nt) {
-                az -= T(n - m + 1) * (T(__ldg(cn + 2 * m - 1)) * v + T(__ldg(cn + 2 * m)) * w);
-            }
-            if (m == 1) {
-                if (n <= Nz) {
-                    const T J = T(__ldg(cn));
-                    ax += J * v;
-                    ay += J * w;
-                }
-            } else if (!kZonal && m >= 2 && n <= Nt) {                            // order m - 1 >= 1
-                const T C = T(__ldg(cn + 2 * m - 3)), S = T(__ldg(cn + 2 * m - 2));
-                ax -= T(0.5) * (C * v + S * w);
-                ay += T(0.5) * (S * v - C * w);
-            }
-            if (!kZonal && m + 1 <= n && n <= Nt) {                               // order m + 1
-                const T C = T(__ldg(cn + 2 * m + 1)), S = T(__ldg(cn + 2 * m + 2));
-                const T f = T(0.5) * T((k - m) * (k - m - 1));
-                ax += f * (C * v + S * w);
-                ay += f * (S * v - C * w);
-            }
-        }
+        gp_column<T, kZonal>(tab, rcp, Nz, Nt, m, zs, rho2, vd, wd, ax, ay, az);
     }
     const T s = T(1) / (R * R);
     ax *= s; ay *= s; az *= s;
 }
 
+// Expanded coefficient table of one model for the lane-parallel evaluation: X[n][m] = (C_nm, S_nm) for
+// n < kGpXN, m < kGpXM, with C_n0 = -J_n, S_n0 = 0, and zero wherever the model has no term (n < 2, n > Nz,
+// m > n, and m > 0 with n > Nt). With the zeros in the table every lane runs the same instructions.
+constexpr int kGpXN = EPH_GP_MAX_DEGREE + 1, kGpXM = EPH_GP_MAX_DEGREE + 3;
+constexpr int kGpX = kGpXN * kGpXM * 2;
+__device__ __forceinline__ void gp_expand(const double *__restrict__ tab, int Nz, int Nt, double *X, int t, int nt) {
+    for (int q = t; q < kGpX; q += nt) {
+        const int n = q / (kGpXM * 2), m = (q / 2) % kGpXM, sn = q & 1;
+        double v = 0;
+        if (n >= 2 && n <= Nz && m <= n) {
+            if (m == 0) v = sn ? 0.0 : -tab[n * n - 4];
+            else if (n <= Nt) v = tab[n * n - 4 + 2 * m - 1 + sn];
+        }
+        X[q] = v;
+    }
+}
+
+// The field from an expanded table, spread over a group of G consecutive lanes (G a power of two <= 32,
+// `mask` the group's lanes, q = lane index in the group): lane q walks columns q, q + G, ..., and the group
+// adds the lanes' sums with a butterfly. Each lane runs its diagonal recursion and its column in one loop
+// over the degree k = 0 .. Nz + 1 with selects instead of branches (the value of column m is zero below
+// degree m), adding for every value V_km, W_km the three gradient terms that read it:
+//   a_z -= (k-m) (C_{k-1,m} V + S_{k-1,m} W)
+//   a_x -= w_B (C_{k-1,m-1} V + S_{k-1,m-1} W),  a_y += w_B (S_{k-1,m-1} V - C_{k-1,m-1} W),  w_B = 1 (m = 1), 1/2 (m > 1)
+//   a_x += w_C (C_{k-1,m+1} V + S_{k-1,m+1} W),  a_y += w_C (S_{k-1,m+1} V - C_{k-1,m+1} W),  w_C = (k-m)(k-m-1)/2
+// so the group finishes in about the time of one column instead of all of them in turn. Every lane of the
+// group returns the field.
+template <int G>
+__device__ __forceinline__ v3 gp_field_lanes(const double *X, const double *rcp, int Nz, int Nt, double R, v3 r, int q,
+                                             unsigned mask) {
+    double ax = 0, ay = 0, az = 0;
+    if (Nz >= 2) {
+        double xs, ys, zs, rho2, v00;
+        gp_setup(R, r.x, r.y, r.z, xs, ys, zs, rho2, v00);
+        const int mlast = max(Nt + 1, 1), K = Nz + 1;
+        #pragma unroll 1
+        for (int m = q; m <= mlast; m += G) {
+            const double md = (double)m;
+            const double wB = m == 0 ? 0.0 : (m == 1 ? 1.0 : 0.5);
+            const double *XA = X + m * 2, *XB = X + (m == 0 ? 0 : m - 1) * 2, *XC = X + (m + 1) * 2;
+            double dv = v00, dw = 0;                 // diagonal V_kk, W_kk while k <= m
+            double v = 0, w = 0, vp = 0, wp = 0;     // column m at degrees k and k - 1
+            #pragma unroll 1
+            for (int k = 0; k <= K; ++k) {
+                const double kd = (double)k;
+                const double f = 2 * kd - 1;
+                const double ndv = f * (xs * dv - ys * dw), ndw = f * (xs * dw + ys * dv);
+                dv = (k >= 1 && k <= m) ? ndv : dv;
+                dw = (k >= 1 && k <= m) ? ndw : dw;
+                const double c = rcp[k > m ? k - m : 1];
+                const double a = f * zs, b = (kd + md - 1) * rho2;
+                double nv = (a * v - b * vp) * c, nw = (a * w - b * wp) * c;
+                nv = k == m ? dv : (k < m ? 0.0 : nv);
+                nw = k == m ? dw : (k < m ? 0.0 : nw);
+                vp = v; wp = w; v = nv; w = nw;
+                if (k >= 1) {
+                    const int row = (k - 1) * kGpXM * 2;
+                    const double CA = XA[row], SA = XA[row + 1], CB = XB[row], SB = XB[row + 1];
+                    const double CC = XC[row], SC = XC[row + 1];
+                    const double wA = kd - md, wC = 0.5 * (kd - md) * (kd - md - 1);
+                    az -= wA * (CA * v + SA * w);
+                    ax += wC * (CC * v + SC * w) - wB * (CB * v + SB * w);
+                    ay += wC * (SC * v - CC * w) + wB * (SB * v - CB * w);
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) {
+        ax += __shfl_xor_sync(mask, ax, o);
+        ay += __shfl_xor_sync(mask, ay, o);
+        az += __shfl_xor_sync(mask, az, o);
+    }
+    const double s = 1.0 / (R * R);
+    return mk(ax * s, ay * s, az * s);
+}
+
 // FP64 field of a geopotential model (any Nz, Nt), out of line: it sits on a cold path of the step kernel.
 static __device__ __noinline__ v3 gp_field(const double *__restrict__ tab, int Nz, int Nt, double R, v3 r) {
     v3 a = mk(0, 0, 0);
-    if (Nz >= 2) gp_core<double, false>(tab, Nz, Nt, R, r.x, r.y, r.z, a.x, a.y, a.z);
+    if (Nz >= 2) gp_core<double, false>(tab, GP_RCP, Nz, Nt, R, r.x, r.y, r.z, a.x, a.y, a.z);
     return a;
 }
 

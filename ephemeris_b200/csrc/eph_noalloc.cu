@@ -12,7 +12,7 @@
 // reactions, ownership lists, model tables, barrier and status words) lives in one file-scope
 // __device__ array, g_noalloc_scratch, sized for at most EPH_NOALLOC_MAX_BODIES bodies,
 // EPH_NOALLOC_MAX_EXT extended bodies, EPH_NOALLOC_MAX_GP geopotential and EPH_NOALLOC_MAX_RING ring
-// models (about 2.5 MB). The array is part of the library's device image: every GPU on which the library
+// models (about 3.2 MB). The array is part of the library's device image: every GPU on which the library
 // is loaded holds it from module load until the process exits. In host code `g_noalloc_scratch` names a
 // host-side stand-in for the symbol, not a device address; the device address comes from
 // cudaGetSymbolAddress, once per device, in noalloc_setup().
@@ -51,7 +51,8 @@ constexpr size_t kOffPub = 0;
 constexpr size_t kOffAux = kOffPub + r32((size_t)2 * PUB_NPLANES * kNB);
 constexpr size_t kOffCst = kOffAux + r32((size_t)AUX_NPLANES * kNB);
 constexpr size_t kOffReact = kOffCst + r32((size_t)CST_NPLANES * kNB);
-constexpr size_t kOffGpCoef = kOffReact + r32((size_t)kNE * kNB * 12);
+constexpr size_t kOffReactCta = kOffReact + r32((size_t)kNE * kNB * 12);
+constexpr size_t kOffGpCoef = kOffReactCta + r32((size_t)kNE * kNB * 6);
 constexpr size_t kOffRingParam = kOffGpCoef + r32((size_t)kNGP * EPH_GP_TABLE_SIZE);
 constexpr size_t kOffRingDisk = kOffRingParam + r32((size_t)kNRing * EPH_RING_PARAMS);
 constexpr size_t kOffOrig = kOffRingDisk + r32((size_t)kNRing * EPH_RING_MAX_DISKS * 3);
@@ -190,8 +191,10 @@ int body(int device, cudaStream_t stream, int n, double *d_planes, const eph_mod
     S.aux = scr + kOffAux;
     S.cst = scr + kOffCst;
     S.react = scr + kOffReact;
+    S.react_cta = scr + kOffReactCta;
     S.planes = d_planes;
     S.ext_body = I(kOffExt);
+    S.n_gp = n_gp;
     S.gp_nz = I(kOffGpNz);
     S.gp_nt = I(kOffGpNt);
     S.gp_coef = scr + kOffGpCoef;

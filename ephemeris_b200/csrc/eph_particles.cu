@@ -80,7 +80,7 @@ struct PartArgs {
 // perturber is zonal.
 __device__ __forceinline__ v3 gp_zonal(const double *__restrict__ c_table, int Nz, double R, v3 r) {
     v3 a = mk(0, 0, 0);
-    if (Nz >= 2) gp_core<double, true>(c_table, Nz, 0, R, r.x, r.y, r.z, a.x, a.y, a.z);
+    if (Nz >= 2) gp_core<double, true>(c_table, GP_RCP, Nz, 0, R, r.x, r.y, r.z, a.x, a.y, a.z);
     return a;
 }
 

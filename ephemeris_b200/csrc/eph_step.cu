@@ -86,6 +86,8 @@ struct Scratch {
     double react[kOwnMax][6];         // summed reactions of owned hosts
     double rterm[kOwnMax][kRingPar][kRingDiskPar][3];   // per-disk ring terms before their ordered sum
     int ring_e[kRingPar], n_ring_e, ring_dmax;
+    double gp_x[kGpSmem][kGpX];                     // expanded tables of the first kGpSmem geopotential models
+    double gp_rcp[EPH_GP_MAX_DEGREE + 2];          // 1/k of the degree recursion
     double rk_hi[EPH_RK12_NCOEF], rk_lo[EPH_RK12_NCOEF];   // a_kj (lane-divergent reads: shared, not constant, memory)
     unsigned long long t_last, t_phase[kPhases];
     unsigned long long mbar;          // mbarrier of the tile copies
@@ -121,20 +123,21 @@ __device__ __forceinline__ void mark(const SysDev &S, Scratch &sc, int ph) {
 
 // Barrier over all CTAs of the launch (co-resident by the cooperative launch). The arrival counter is a
 // 64-bit word zeroed before the launch that only grows: barrier number k of the launch is complete when it
-// reaches k * gridDim.x, so every CTA announces its arrival with one fire-and-forget release add and then
-// polls the counter; no CTA has to reset or flip anything. Returns false when the wait timed out here or
-// elsewhere (status word set); the caller then leaves the kernel.
+// reaches k * gridDim.x, so every CTA announces its arrival with one acquire-release add (which carries the
+// CTA's writes, ordered before it by the CTA barrier) and polls the counter only if its add was not the
+// last one; no CTA has to reset or flip anything. Returns false when the wait timed out here or elsewhere
+// (status word set); the caller then leaves the kernel.
 __device__ bool grid_sync(const SysDev &S, Scratch &sc) {
     __syncthreads();
     if (gridDim.x == 1) return true;
     if (threadIdx.x == 0) {
         unsigned long long *count = reinterpret_cast<unsigned long long *>(S.bar);
         const unsigned long long target = (sc.bar_target += gridDim.x);
-        __threadfence();
-        asm volatile("red.release.gpu.global.add.u64 [%0], 1;" ::"l"(count) : "memory");
+        unsigned long long old;
+        asm volatile("atom.acq_rel.gpu.global.add.u64 %0, [%1], 1;" : "=l"(old) : "l"(count) : "memory");
         int fail = 0;
         unsigned long long t0 = 0;
-        for (unsigned it = 0;; ++it) {
+        for (unsigned it = 0; old + 1 < target; ++it) {   // the last arrival does not wait
             unsigned long long v;
             asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(count) : "memory");
             if (v >= target) break;
@@ -171,8 +174,16 @@ __device__ __forceinline__ void mbar_init(Scratch &sc) {
 // Copy `rows` planes (row r from src[r] + j0, `count` bodies rounded up to kPad; rows from `tail_from` on
 // `count_tail` bodies; a null src[r] keeps tile row r as it is) into tile rows of `stride` doubles. Every
 // thread waits for completion (bounded). Returns false on timeout.
+struct NoSideWork {
+    __device__ void operator()() const {}
+};
+
+// `side()` runs on every thread after the copies are issued and before the wait: work whose own loads can
+// overlap the copies.
+template <typename Side = NoSideWork>
 __device__ bool load_tile(const SysDev &S, Scratch &sc, TileState &ts, double *tile, int stride,
-                          const double *const *src, int rows, int j0, int count, int count_tail, int tail_from) {
+                          const double *const *src, int rows, int j0, int count, int count_tail, int tail_from,
+                          const Side &side = Side()) {
     __syncthreads();   // the previous sweep's reads of the tile are done
     const int cpad = (count + kPad - 1) / kPad * kPad;
     const int tpad = (count_tail + kPad - 1) / kPad * kPad;
@@ -196,6 +207,7 @@ __device__ bool load_tile(const SysDev &S, Scratch &sc, TileState &ts, double *t
                 : "memory");
         }
     }
+    side();
     const unsigned parity = ts.parity;
     ts.parity ^= 1u;
     unsigned long long t0 = 0;
@@ -739,12 +751,48 @@ __device__ bool sweep_a(const SysDev &S, Own *own, int nb, unsigned mask, int bu
     return true;
 }
 
+// Geopotential items (owned body b, host e) of ext_field_items on `nthr` threads (t = this thread's index),
+// G lanes per item: every item's lanes evaluate it together (gp_field_lanes on the expanded table in shared
+// memory) and the group's first lane stores it; a model beyond the shared-memory copies runs gp_field on
+// that lane alone.
+template <int G, typename Put>
+__device__ __forceinline__ void gp_items(const SysDev &S, const Own *own, int nb, const double *pub, Scratch &sc, int t,
+                                         int nthr, const Put &put) {
+    const int ld = S.ld, n_ext = S.n_ext;
+    const int q = t & (G - 1), lane = threadIdx.x & 31;
+    const unsigned mask = G == 1 ? (1u << lane) : (((1u << G) - 1u) << (lane & ~(G - 1)));
+    #pragma unroll 1
+    for (int item = t / G; item < nb * n_ext; item += nthr / G) {
+        const int b = item / n_ext, e = item % n_ext;
+        const Own &o = own[b];
+        const int E = __ldg(S.ext_body + e);
+        const int gpE = (int)__ldg(S.cst + CST_GP * ld + E);
+        const bool live = gpE >= 0 && E != o.idx;
+        v3 r = mk(0, 0, 0), an = mk(0, 0, 0);
+        double GME = 0;
+        if (live) {   // uniform over the group
+            r = mk(dd_diff(o.r[0].hi, o.r[0].lo, __ldcg(pub + PUB_R_HI * ld + E), __ldcg(pub + PUB_R_LO * ld + E)),
+                   dd_diff(o.r[1].hi, o.r[1].lo, __ldcg(pub + (PUB_R_HI + 1) * ld + E), __ldcg(pub + (PUB_R_LO + 1) * ld + E)),
+                   dd_diff(o.r[2].hi, o.r[2].lo, __ldcg(pub + (PUB_R_HI + 2) * ld + E), __ldcg(pub + (PUB_R_LO + 2) * ld + E)));
+            GME = __ldcg(pub + PUB_GM * ld + E);
+            const m3 f = ld9(pub + PUB_FRAME * ld, ld, E);
+            const int nz = __ldg(S.gp_nz + gpE), nt = __ldg(S.gp_nt + gpE);
+            const double R = __ldg(S.cst + CST_R * ld + E);
+            v3 al = mk(0, 0, 0);
+            if (gpE < kGpSmem) al = gp_field_lanes<G>(sc.gp_x[gpE], sc.gp_rcp, nz, nt, R, tolocal(f, r), q, mask);
+            else if (q == 0) al = gp_field(S.gp_coef + (size_t)gpE * EPH_GP_TABLE_SIZE, nz, nt, R, tolocal(f, r));
+            an = toworld(f, al);
+        }
+        if (q == 0) put(0, b, e, o, r, an, GME, live);
+    }
+}
+
 // Field of every geopotential / ring host at the owned bodies, once per (host, body): the force on the
 // owned body goes to sc.ext, the host's reaction to S.react (APPLY_NONPOINT_FORCE, mass.impl:127-130;
 // r = r_body - r_host as `mj.r - mi.r` with mi the host, mass.cpp:358-371). Runs on warps
 // [first_warp, kWarps): ring items on the last warp, geopotential items on the others, so no warp
 // diverges between the two models.
-__device__ void ext_fields(const SysDev &S, const Own *own, int nb, int buf, Scratch &sc, int first_warp) {
+__device__ void ext_field_items(const SysDev &S, const Own *own, int nb, int buf, Scratch &sc, int first_warp) {
     const int ld = S.ld, n_ext = S.n_ext;
     const double *pub = S.pub + (size_t)buf * PUB_NPLANES * ld;
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -770,26 +818,12 @@ __device__ void ext_fields(const SysDev &S, const Own *own, int nb, int buf, Scr
         rc[0] = da.x; rc[1] = da.y; rc[2] = da.z; rc[3] = dt.x; rc[4] = dt.y; rc[5] = dt.z;
     };
     if (gp_warp) {
-        const int t0 = single ? lane : threadIdx.x - first_warp * 32;
-        const int stride = single ? 32 : (kWarps - 1 - first_warp) * 32;
-        #pragma unroll 1
-        for (int item = t0; item < nb * n_ext; item += stride) {
-            const int b = item / n_ext, e = item % n_ext;
-            const Own &o = own[b];
-            const int E = __ldg(S.ext_body + e);
-            const int gpE = (int)__ldg(S.cst + CST_GP * ld + E);
-            const bool live = gpE >= 0 && E != o.idx;
-            v3 r = mk(0, 0, 0), an = mk(0, 0, 0);
-            double GME = 0;
-            if (live) {
-                r = body_sep(o, E);
-                GME = __ldcg(pub + PUB_GM * ld + E);
-                m3 f = ld9(pub + PUB_FRAME * ld, ld, E);
-                an = toworld(f, gp_field(S.gp_coef + (size_t)gpE * EPH_GP_TABLE_SIZE, __ldg(S.gp_nz + gpE),
-                                       __ldg(S.gp_nt + gpE), __ldg(S.cst + CST_R * ld + E), tolocal(f, r)));
-            }
-            put(0, b, e, o, r, an, GME, live);
-        }
+        // one (body, host) item per lane when there are many, one per group of 8 lanes (one column of the
+        // recursion per lane) when they are few enough to run in one round that way
+        const int nthr = single ? 32 : (kWarps - 1 - first_warp) * 32;
+        const int t = single ? lane : threadIdx.x - first_warp * 32;
+        if (nb * n_ext * 8 <= nthr) gp_items<8>(S, own, nb, pub, sc, t, nthr, put);
+        else gp_items<1>(S, own, nb, pub, sc, t, nthr, put);
     }
     if (!ring_warp) return;
     // ring half (react slot 1, sc.ext2). With few hosts and disks each lane takes one (body, host, disk)
@@ -867,6 +901,26 @@ __device__ void ext_fields(const SysDev &S, const Own *own, int nb, int buf, Scr
             an = toworld(f, ret);
         }
         put(1, b, e, o, r, an, GME, live);
+    }
+}
+
+// ext_field_items, then this CTA's share of every host's reaction: the sum over its owned bodies (in
+// ownership order) of both model halves, S.react_cta[host][CTA][6], so that a host's owner adds one value per
+// CTA in pass B instead of one per body.
+__device__ void ext_fields(const SysDev &S, const Own *own, int nb, int buf, Scratch &sc, int first_warp) {
+    ext_field_items(S, own, nb, buf, sc, first_warp);
+    const int nthr = (kWarps - first_warp) * 32;
+    asm volatile("bar.sync 2, %0;" ::"r"(nthr) : "memory");
+    const int ld = S.ld;
+    #pragma unroll 1
+    for (int item = threadIdx.x - first_warp * 32; item < S.n_ext * 6; item += nthr) {
+        const int e = item / 6, c = item % 6;
+        double sum = 0;
+        for (int b = 0; b < nb; ++b) {
+            const double *rc = S.react + ((size_t)e * ld + own[b].idx) * 12;
+            sum += __ldcg(rc + c) + __ldcg(rc + 6 + c);
+        }
+        S.react_cta[((size_t)e * ld + blockIdx.x) * 6 + c] = sum;
     }
 }
 
@@ -1129,18 +1183,18 @@ __device__ bool pass_b(const SysDev &S, Own *own, int nb, int buf, Scratch &sc, 
             checked_maximize(ob.maxi, rr[10]);
         }
     } else {
-        // the last warp: reactions of the owned extended bodies, the sum over all bodies i of the table
-        // written in pass A (lane-strided over i, then a butterfly over the warp)
+        // the last warp: reactions of the owned extended bodies, the sum over all CTAs of their shares
+        // written in pass A (lane-strided over the CTAs, then a butterfly over the warp)
         const int lane = threadIdx.x & 31;
         #pragma unroll 1
         for (int b = 0; b < nb; ++b) {
             const int e = own[b].ext_slot;
             if (e < 0) continue;
             double part[6] = {0, 0, 0, 0, 0, 0};
-            const double *rc = S.react + (size_t)e * ld * 12;   // [i][geopotential, ring][6]
-            #pragma unroll 1
-            for (int i = lane; i < n; i += 32)
-                for (int c = 0; c < 6; ++c) part[c] += __ldcg(rc + (size_t)i * 12 + c) + __ldcg(rc + (size_t)i * 12 + 6 + c);
+            const double *rc = S.react_cta + (size_t)e * ld * 6;   // [CTA][6]
+            #pragma unroll 4
+            for (int g = lane; g < (int)gridDim.x; g += 32)
+                for (int c = 0; c < 6; ++c) part[c] += __ldcg(rc + (size_t)g * 6 + c);
             for (int c = 0; c < 6; ++c) {
                 const double v = warp_sum(part[c]);
                 if (lane == c) sc.react[b][c] = v;
@@ -1149,17 +1203,17 @@ __device__ bool pass_b(const SysDev &S, Own *own, int nb, int buf, Scratch &sc, 
     }
     __syncthreads();
     mark(S, sc, PH_B_SWEEP);
-    // reactions of the owned extended bodies, when every warp swept: sum over all bodies i of the table
+    // reactions of the owned extended bodies, when every warp swept: the sum over all CTAs of their shares
     // written in pass A
     #pragma unroll 1
     for (int b = 0; b < (nwb == kWarps ? nb : 0); ++b) {
         const int e = own[b].ext_slot;
         if (e < 0) continue;   // uniform over the CTA
         double part[6] = {0, 0, 0, 0, 0, 0};
-        const double *rc = S.react + (size_t)e * ld * 12;   // [i][geopotential, ring][6]
+        const double *rc = S.react_cta + (size_t)e * ld * 6;   // [CTA][6]
         #pragma unroll 1
-        for (int i = threadIdx.x; i < n; i += blockDim.x)
-            for (int c = 0; c < 6; ++c) part[c] += __ldcg(rc + (size_t)i * 12 + c) + __ldcg(rc + (size_t)i * 12 + 6 + c);
+        for (int g = threadIdx.x; g < (int)gridDim.x; g += blockDim.x)
+            for (int c = 0; c < 6; ++c) part[c] += __ldcg(rc + (size_t)g * 6 + c);
         const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
         for (int c = 0; c < 6; ++c) {
             double v = warp_sum(part[c]);
@@ -1379,6 +1433,9 @@ __global__ void __launch_bounds__(kThreads, 1) step_kernel(SysDev S, StepParams 
         sc.rk_hi[q] = c_rk_hi[q];
         sc.rk_lo[q] = c_rk_lo[q];
     }
+    for (int k = 0; k < min(S.n_gp, kGpSmem); ++k)
+        gp_expand(S.gp_coef + (size_t)k * EPH_GP_TABLE_SIZE, S.gp_nz[k], S.gp_nt[k], sc.gp_x[k], threadIdx.x, blockDim.x);
+    for (int q = threadIdx.x; q < EPH_GP_MAX_DEGREE + 2; q += blockDim.x) sc.gp_rcp[q] = GP_RCP[q];
     mbar_init(sc);
     int nb = 0;
     for (int b = 0; b < kOwnMax; ++b) {

@@ -11,7 +11,8 @@
 //   * constants cst[CST_NPLANES][ld]: sR2, tide_delay_factor, R^2, luminosity, R, model indices.
 //   * extended-body reactions react[n_ext][ld][2][6]: for host e and body i, -GM_i an and -GM_i (r x an)
 //     of host e's geopotential (slot 0) and ring (slot 1) field at body i (written in pass A by i's
-//     owner, summed by e's owner in pass B).
+//     owner), and react_cta[n_ext][ld][6], each CTA's sum of them over its bodies (summed over the CTAs by
+//     e's owner in pass B).
 //   * planes[EPH_NPLANES][n]: the whole `mass` record (include/eph_planes.h), loaded at kernel start
 //     and stored at kernel end by each body's owner.
 // A CTA keeps the private state of the bodies it owns (start-of-step state, RK12 stage accumulators,
@@ -29,6 +30,7 @@ constexpr int kOwnMax = 8;           // bodies owned by one CTA (private state l
 constexpr int kStages = 25;          // Feagin RK12 stages
 constexpr int kMaxExt = 64;          // extended bodies (geopotential or ring) per system
 constexpr int kPad = 32;             // plane stride granularity (bodies)
+constexpr int kGpSmem = 12;          // geopotential models a CTA keeps (expanded) in shared memory
 constexpr int kRingPar = 2;          // ring hosts whose disks are evaluated one per lane
 constexpr int kRingDiskPar = 8;      // disks per ring evaluated one per lane
 
@@ -67,10 +69,12 @@ struct SysDev {
     double *pub;              // [2][PUB_NPLANES][ld]
     double *aux;              // [AUX_NPLANES][ld]
     double *cst;              // [CST_NPLANES][ld]
-    double *react;            // [n_ext][ld][6]
+    double *react;            // [n_ext][ld][2][6]
+    double *react_cta;        // [n_ext][ld][6]: per-CTA sums of `react` over the CTA's bodies (CTA < grid <= ld)
     double *planes;           // [EPH_NPLANES][n]
     const int *ext_body;      // [n_ext] body index of each extended body
-    const int *gp_nz, *gp_nt; // geopotential models
+    int n_gp;                 // geopotential models
+    const int *gp_nz, *gp_nt;
     const double *gp_coef;    // [n_gp][EPH_GP_TABLE_SIZE]
     const int *ring_nd;       // ring models
     const double *ring_param; // [n_ring][4]

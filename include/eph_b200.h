@@ -227,16 +227,17 @@ int eph_serve_info(const eph_serve *s, int64_t *launches, int64_t *queued, int64
 /* ---- Force models evaluated on their own (geopotential::sum, src/physics/geopotential.h:36): the field
  * of a geopotential model coef[EPH_GP_TABLE_SIZE] (degrees 2..nz zonal, tesseral up to nt <= nz) of a body
  * of radius R at `count` body-frame positions r[count][3] (host arrays): out[count][3] = acceleration per
- * unit GM of the body, computed on `device` by the device function the integration kernels use. */
-int eph_geopotential_field(int device, const double *coef, int nz, int nt, double R, int64_t count, const double *r,
-                           double *out);
+ * unit GM of the body, computed on `device` by the device functions the integration kernels use: lanes = 1
+ * one point per thread (massless-particle kernels), lanes = 8 one point per 8 lanes (step kernel). */
+int eph_geopotential_field(int device, const double *coef, int nz, int nt, double R, int lanes, int64_t count,
+                           const double *r, double *out);
 
 /* Measurement aid (no counterpart in the reference): the throughput of the FP64 CUDA-core pipe that the
  * integration kernels use, measured on `device` with independent FMA chains on every SM (TFLOP/s, an FMA
  * counted as 2 flops). */
 int eph_fp64_fma_rate(int device, double *tflops);
 
-/* Limits of eph_integrate_noalloc's fixed scratch (about 2.5 MB of device memory per GPU). */
+/* Limits of eph_integrate_noalloc's fixed scratch (about 3.2 MB of device memory per GPU). */
 #define EPH_NOALLOC_MAX_BODIES 1024
 #define EPH_NOALLOC_MAX_EXT 16     /* bodies with a geopotential or ring model */
 #define EPH_NOALLOC_MAX_GP 16      /* geopotential models */

@@ -8,8 +8,9 @@ the value on it. The same grid and bound are used here against an independent ex
 (tests/harmonics_ref.py: harmonic polynomials with rational coefficients, longdouble evaluation):
 
 * the oracle's restatement of the reference's evaluation (CPU), and
-* the device function of the integration kernels (`eph_geopotential_field`, GPU), which uses Cunningham's
-  Cartesian recursion, plus a comparison with the oracle on random full models.
+* the device functions of the integration kernels (`eph_geopotential_field`, GPU: one point per thread as
+  the particle kernels evaluate it, and one point per 8 lanes as the step kernel does), which use
+  Cunningham's Cartesian recursion, plus a comparison with the oracle on random full models.
 """
 import ctypes
 
@@ -41,13 +42,13 @@ def test_oracle_geopotential_known_answer(oracle):
     assert worst < H.KAT_EPS, worst
 
 
-def _device_field(tab, nz, nt, R, pts):
+def _device_field(tab, nz, nt, R, pts, lanes=1):
     from ephemeris_b200 import load_library
     lib = load_library()
     pts = np.ascontiguousarray(pts, dtype=np.float64)
     out = np.zeros_like(pts)
     D = ctypes.POINTER(ctypes.c_double)
-    rc = lib.eph_geopotential_field(0, np.ascontiguousarray(tab).ctypes.data_as(D), nz, nt, R, len(pts),
+    rc = lib.eph_geopotential_field(0, np.ascontiguousarray(tab).ctypes.data_as(D), nz, nt, R, lanes, len(pts),
                                     pts.ctypes.data_as(D), out.ctypes.data_as(D))
     assert rc == 0, rc
     return out
@@ -60,32 +61,36 @@ def test_geopotential_field_rejects_bad_arguments():
     tab = np.zeros(77)
     p = np.zeros(3)
     o = np.zeros(3)
-    args = (tab.ctypes.data_as(D), 1.0, 1, p.ctypes.data_as(D), o.ctypes.data_as(D))
+    args = (tab.ctypes.data_as(D), 1.0, 1, 1, p.ctypes.data_as(D), o.ctypes.data_as(D))
     assert lib.eph_geopotential_field(0, args[0], 9, 0, *args[1:]) == 1       # degree above 8
     assert lib.eph_geopotential_field(0, args[0], 4, 5, *args[1:]) == 1       # tesseral above zonal
     assert lib.eph_geopotential_field(0, None, 4, 4, *args[1:]) == 1
+    assert lib.eph_geopotential_field(0, args[0], 4, 4, 1.0, 4, 1, args[4], args[5]) == 1   # lanes not 1 or 8
 
 
 @pytest.mark.gpu
-def test_device_geopotential_known_answer():
+@pytest.mark.parametrize("lanes", [1, 8])
+def test_device_geopotential_known_answer(lanes):
     worst, worst_axis = 0.0, 0.0
     for n, m, sine, tab, nz, nt in H.kat_cases():
         for k, pts in enumerate(H.kat_spheres()):
             ref = H.model_field(tab, nz, nt, H.KAT_R, pts)
-            got = _device_field(tab, nz, nt, H.KAT_R, pts)
+            got = _device_field(tab, nz, nt, H.KAT_R, pts, lanes)
             scale = np.linalg.norm(np.asarray(ref, dtype=float), axis=1).max()
             worst = max(worst, np.linalg.norm(got - np.asarray(ref, dtype=float), axis=1).max() / scale)
             rn = np.linalg.norm(pts[0])
             near = H.near_axis_points(k, rn)
-            on = _device_field(tab, nz, nt, H.KAT_R, np.stack([np.zeros(len(near)), np.zeros(len(near)), near[:, 2]], 1))
-            got_near = _device_field(tab, nz, nt, H.KAT_R, near)
+            on = _device_field(tab, nz, nt, H.KAT_R, np.stack([np.zeros(len(near)), np.zeros(len(near)), near[:, 2]], 1),
+                               lanes)
+            got_near = _device_field(tab, nz, nt, H.KAT_R, near, lanes)
             worst_axis = max(worst_axis, np.linalg.norm(got_near - on, axis=1).max() / scale)
     assert worst < H.KAT_EPS, worst
     assert worst_axis < H.KAT_EPS, worst_axis
 
 
 @pytest.mark.gpu
-def test_device_geopotential_matches_oracle(oracle):
+@pytest.mark.parametrize("lanes", [1, 8])
+def test_device_geopotential_matches_oracle(oracle, lanes):
     rng = np.random.default_rng(77)
     worst = 0.0
     for _ in range(40):
@@ -101,7 +106,7 @@ def test_device_geopotential_matches_oracle(oracle):
         pts *= (R * rng.uniform(1.02, 40.0, size=256) / np.linalg.norm(pts, axis=1))[:, None]
         md = _models(tab, nz, nt)
         ref = np.array([oracle.geopotential_sum(md, 0, R, p) for p in pts])
-        got = _device_field(tab, nz, nt, R, pts)
+        got = _device_field(tab, nz, nt, R, pts, lanes)
         err = np.linalg.norm(got - ref, axis=1) / np.linalg.norm(ref, axis=1)
         worst = max(worst, err.max())
     assert worst < 1e-13, worst

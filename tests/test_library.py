@@ -99,7 +99,21 @@ def test_algorithmic_flop_count(golden):
     f = bench.algorithmic_flops_per_step(g["load"], Models(m.gp_nz, m.gp_nt, m.gp_coef, m.ring_ndisk,
                                                           m.ring_param, m.ring_disk))
     n = 33
-    assert f == 25 * n * (n - 1) * 280 + n * 3900
+    # point-like bodies only: pass A (20) and 1PN (80) per ordered pair; the deformation, Lense-Thirring and
+    # radiation terms are exactly zero and not evaluated
+    assert f == 25 * n * (n - 1) * 100 + n * 3900
+    g2 = golden("config2")
+    m2 = g2.models()
+    pl = g2["load"]
+    f2 = bench.algorithmic_flops_per_step(pl, Models(m2.gp_nz, m2.gp_nt, m2.gp_coef, m2.ring_ndisk, m2.ring_param,
+                                                     m2.ring_disk))
+    n, nf = pl.shape[1], int(bench.full_class(pl).sum())
+    delayed = int(((pl[46] != 0) & (pl[48] != 0)).sum())
+    pairs_full = n * (n - 1) - (n - nf) * (n - nf - 1)
+    want = 25 * (n * (n - 1) * 100 + pairs_full * 180 + delayed * (n - 1) * 120 + 9 * (n - 1) * 250
+                 + 2 * (n - 1) * 60) + n * 3900
+    assert (nf, delayed) == (107, 86)
+    assert f2 == want
 
 
 def _gloo_worker(rank, world, port, q):
