@@ -93,6 +93,16 @@ def algorithmic_flops_per_step(planes, models):
     return 25 * per_stage + n * FLOP_RK
 
 
+_CAPTURE = None   # when a list, result lines are collected here (sub-records) instead of printed
+
+
+def _emit(line):
+    if _CAPTURE is not None:
+        _CAPTURE.append(line)
+    else:
+        print(json.dumps(line), flush=True)
+
+
 class ClockSampler:
     """nvidia-smi clocks / throttle reasons sampled every 200 ms while the timed region runs."""
 
@@ -335,6 +345,79 @@ def ensemble_cpu(cfgs, sizes, n_members, n_step):
                       f"{el:.1f} s"}
 
 
+# Members of the ensemble recipe whose own one-ulp sensitivity after 1000 steps is below 1e-12 (checked by
+# tests/test_gpu_long.py): the 1000-step error sample of the config3 comparison.
+ENS_ERR_MEMBERS = [(3003500, 16), (3003502, 32), (3003504, 48), (3003506, 64)]
+
+
+def _oracle_run(job):
+    """Worker process: the oracle's integration of one system (planes, model arrays, dt, steps)."""
+    pl, mdl, dt, steps = job
+    from oracle.pyoracle import Models, Oracle
+    return Oracle().integrate(pl, Models(*mdl), dt, steps)[0]
+
+
+def ensemble_one_by_one(pls, mds, dts, ks, device, stream, n_probe=24, probe_steps=10):
+    """The plain FP64 GPU path on the ensemble: members one after another through a Context (the
+    single-system kernel, msystem::integrate semantics). Measured on `n_probe` members spread over the
+    sizes (CUDA events over `probe_steps` steps each); the whole ensemble's time is the sum over all members
+    of their step counts times the per-step time interpolated at their size."""
+    import torch
+    from ephemeris_b200 import Context
+    order = np.argsort([p.shape[1] for p in pls])
+    pick = sorted(set(order[np.linspace(0, len(order) - 1, n_probe).round().astype(int)].tolist()))
+    sizes, per_step = [], []
+    for s in pick:
+        c = Context(device)
+        c.set_stream(stream.cuda_stream)
+        c.upload(pls[s], mds[s])
+        c.integrate(dts[s], 2)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        c.integrate(dts[s], probe_steps)
+        e1.record(stream)
+        e1.synchronize()
+        sizes.append(pls[s].shape[1])
+        per_step.append(e0.elapsed_time(e1) / probe_steps)
+        c.close()
+    n_all = np.array([p.shape[1] for p in pls], float)
+    t_ms = float(np.sum(np.asarray(ks, float) * np.interp(n_all, sizes, per_step)))
+    body_steps = float(np.sum(n_all * np.asarray(ks, float)))
+    return {"value": body_steps / (t_ms / 1e3), "unit": UNIT, "estimated_s": t_ms / 1e3,
+            "sample": f"{len(pick)} members of {min(sizes)}-{max(sizes)} bodies, {probe_steps} RK12 steps each through "
+                      f"eph_integrate (CUDA events); per-step time interpolated in body count for all members",
+            "ms_per_rk_step_by_bodies": dict(zip(map(int, sizes), map(float, per_step)))}
+
+
+def ensemble_errors(device, td, pool):
+    """1000-step position error against the oracle of well-conditioned ensemble members, FP64 and mixed."""
+    from ephemeris_b200 import Batch, MSystem, synth
+    from tests.parity import position_error
+    mem = []
+    for seed, n in ENS_ERR_MEMBERS:
+        cfg = synth.write_system(synth.make_ensemble_member(seed, n), os.path.join(td, f"err{seed}"))
+        ms = MSystem(device)
+        if not ms.load(cfg):
+            raise RuntimeError("error-sample member failed to load")
+        mem.append((ms.planes(), ms.models(), ms.delta_t))
+        ms.close()
+    futs = [pool.submit(_oracle_run, (pl, (md.gp_nz, md.gp_nt, md.gp_coef, md.ring_ndisk, md.ring_param, md.ring_disk),
+                                      dt, 1000)) for pl, md, dt in mem]
+    out = {}
+    for mixed in (False, True):
+        b = Batch(device)
+        b.set_precision(mixed)
+        b.upload([m[0] for m in mem], [m[1] for m in mem])
+        b.integrate([m[2] for m in mem], [1000] * len(mem))
+        out[mixed] = b.download()
+        b.close()
+    refs = [f.result() for f in futs]
+    return {"members": [n for _, n in ENS_ERR_MEMBERS],
+            "fp64": max(position_error(o, r) for o, r in zip(out[False], refs)),
+            "mixed": max(position_error(o, r) for o, r in zip(out[True], refs)),
+            "measure": "max_i |dr_i| / |r_i - r_star| after 1000 RK12 steps of dt = 0.05 day, max over the members"}
+
+
 def run_b200_ensemble(args):
     import torch
     from ephemeris_b200 import Batch
@@ -371,6 +454,33 @@ def run_b200_ensemble(args):
         dev_ms_max = reduce_max(pg, dev_ms, dev)
         body_steps = float(sum(p.shape[1] * k for p, k in zip(pls, ks)))
         value = world * body_steps * args.steps / (dev_ms_max / 1e3)
+        compare = None
+        if args.ens_compare and world == 1:
+            # the same ensemble in the mixed-precision form, the plain FP64 path one member at a time, and
+            # the 1000-step errors of both forms on a sample (oracle in spawned worker processes)
+            import concurrent.futures as cf
+            import multiprocessing as mp
+            pool = cf.ProcessPoolExecutor(max_workers=len(ENS_ERR_MEMBERS), mp_context=mp.get_context("spawn"))
+            b.set_precision(True)
+            mixed_ms = 0.0
+            for k in range(args.steps):
+                b.upload(pls, mds)
+                flush.fill_(float(k))
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                b.integrate(dts, ks)
+                e1.record(stream)
+                torch.cuda.synchronize(dev)
+                mixed_ms += e0.elapsed_time(e1)
+            b.set_precision(False)
+            mixed_value = body_steps * args.steps / (mixed_ms / 1e3)
+            plain = ensemble_one_by_one(pls, mds, dts, ks, local, stream)
+            errs = ensemble_errors(local, td, pool)
+            pool.shutdown()
+            compare = {"plain_fp64_one_by_one": plain, "batched_fp64": value, "batched_mixed": mixed_value,
+                       "ratio_batched_mixed_vs_plain_fp64": mixed_value / plain["value"],
+                       "ratio_batched_fp64_vs_plain_fp64": value / plain["value"],
+                       "error_1000_steps": errs}
         # end to end: host planes up, integrate, host planes down
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
@@ -410,9 +520,11 @@ def run_b200_ensemble(args):
                 "gpu_launches": launches,
                 "clocks": clk,
             }
+            if compare is not None:
+                line["comparison"] = compare
             if cpu is not None:
                 line["cpu_baseline"] = cpu
-            print(json.dumps(line), flush=True)
+            _emit(line)
     if pg is not None:
         pg.destroy_process_group()
 
@@ -619,7 +731,7 @@ def run_b200_particles(args):
                 line["mixed_vs_fp64_position_error"] = mixed_err
             if cpu is not None:
                 line["cpu_baseline"] = cpu
-            print(json.dumps(line), flush=True)
+            _emit(line)
         p.close()
     if pg is not None:
         pg.destroy_process_group()
@@ -779,7 +891,7 @@ def run_b200_serving(args):
             }
             if cpu is not None:
                 line["cpu_baseline"] = cpu
-            print(json.dumps(line), flush=True)
+            _emit(line)
         srv.close()
     if pg is not None:
         pg.destroy_process_group()
@@ -948,21 +1060,65 @@ def run_b200(args):
             }
             if cpu is not None:
                 line["cpu_baseline"] = cpu
-            print(json.dumps(line), flush=True)
+            if world == 1 and args.workload == "config2" and not args.no_sub_records:
+                ctx.close()
+                line["sub_records"] = collect_sub_records(args)
+            _emit(line)
     if pg is not None:
         pg.destroy_process_group()
+
+
+def collect_sub_records(args):
+    """The other workloads of the path on the same GPU, each with its own metric, value, roofline, e2e,
+    clocks and CPU reference sample: config3 (the 512-system ensemble at its full 500-20000-step durations,
+    with the mixed-precision form, the plain FP64 path one member at a time and 1000-step errors), config5
+    (2 M massless particles x 100 steps per bench step) and config4 (serving: capacity and p50/p99 latency)."""
+    import copy
+    global _CAPTURE
+    plans = [("config3", run_b200_ensemble, dict(ens_frac=1.0, steps=1, warmup=1, ens_compare=True,
+                                                 ens_cpu_members=32, ens_cpu_steps=100)),
+             ("config5", run_b200_particles, dict(steps=3, warmup=2, p_cpu_steps=100, mixed=False)),
+             ("config4", run_b200_serving, dict(warmup=3, serve_requests=100, serve_rate=10.0, p_cpu_steps=100))]
+    subs = {}
+    for name, fn, over in plans:
+        a = copy.copy(args)
+        a.workload = name
+        for k, v in over.items():
+            setattr(a, k, v)
+        _CAPTURE = []
+        try:
+            fn(a)
+            subs[name] = _CAPTURE[0] if _CAPTURE else {"unavailable": "the run produced no result"}
+        except Exception as exc:   # a sub-record is reported, never fatal to the main line
+            subs[name] = {"unavailable": f"{type(exc).__name__}: {exc}"}
+        finally:
+            _CAPTURE = None
+    return subs
+
+
+_PEAKS = {}
 
 
 def fp64_pipe_peak(device: int):
     """Measured throughput of the FP64 CUDA-core pipe (TFLOP/s), the pipe the RK12 kernels run on."""
     import ctypes
     from ephemeris_b200 import load_library
+    if ("pipe", device) in _PEAKS:
+        return _PEAKS[("pipe", device)]
     v = ctypes.c_double(0)
-    return v.value if load_library().eph_fp64_fma_rate(device, ctypes.byref(v)) == 0 else None
+    out = v.value if load_library().eph_fp64_fma_rate(device, ctypes.byref(v)) == 0 else None
+    _PEAKS[("pipe", device)] = out
+    return out
 
 
 def fp64_peak(dev):
-    """Measured FP64 peak: cuBLAS DGEMM 8192^3 (best of 5, CUDA events)."""
+    """Measured FP64 peak: cuBLAS DGEMM 8192^3 (best of 5, CUDA events), once per process."""
+    if ("dgemm", str(dev)) not in _PEAKS:
+        _PEAKS[("dgemm", str(dev))] = _fp64_peak(dev)
+    return _PEAKS[("dgemm", str(dev))]
+
+
+def _fp64_peak(dev):
     import torch
     try:
         a = torch.randn(8192, 8192, dtype=torch.float64, device=dev)
@@ -1000,6 +1156,11 @@ def main():
     ap.add_argument("--ens-systems", type=int, default=512, help="config3: ensemble members")
     ap.add_argument("--ens-frac", type=float, default=0.1, help="config3: fraction of each member's drawn duration")
     ap.add_argument("--ens-cpu-members", type=int, default=64, help="config3: members in the CPU sample")
+    ap.add_argument("--ens-compare", action="store_true",
+                    help="config3: also the mixed-precision form, the plain FP64 path one member at a time, and "
+                         "1000-step errors against the oracle")
+    ap.add_argument("--no-sub-records", action="store_true",
+                    help="config2 on 1 GPU: skip the config3/config5/config4 sub-records of the default run")
     ap.add_argument("--ens-cpu-steps", type=int, default=200, help="config3: RK12 steps per member in the CPU sample")
     ap.add_argument("--particles", type=int, default=2_000_000, help="config5: massless particles per GPU")
     ap.add_argument("--p-steps", type=int, default=100, help="config5: RK12 steps per bench step")

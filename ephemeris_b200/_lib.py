@@ -43,6 +43,7 @@ SIGNATURES = [
     ("eph_accel", ctypes.c_int, [_VP]),
     ("eph_deform", ctypes.c_int, [_VP]),
     ("eph_set_stream", ctypes.c_int, [_VP, _VP]),
+    ("eph_selftest_wait_timeout", ctypes.c_int, [_VP, ctypes.c_int64]),
     ("eph_set_launch", ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int]),
     ("eph_get_launch", ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     ("eph_launch_count", ctypes.c_int64, [_VP]),
@@ -59,6 +60,7 @@ SIGNATURES = [
     ("eph_batch_integrate", ctypes.c_int, [_VP, _D, ctypes.POINTER(ctypes.c_int64), _D, _D]),
     ("eph_batch_download", ctypes.c_int, [_VP, ctypes.POINTER(_D)]),
     ("eph_batch_set_stream", ctypes.c_int, [_VP, _VP]),
+    ("eph_batch_set_precision", ctypes.c_int, [_VP, ctypes.c_int]),
     ("eph_batch_info", ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int64)]),
     ("eph_particles_create", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_VP)]),
     ("eph_particles_destroy", ctypes.c_int, [_VP]),

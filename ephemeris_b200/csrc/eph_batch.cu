@@ -16,7 +16,8 @@
 //           (DAMPED_TIDAL_DEFORMATION_MATRIX_NK2, mass.impl:38-46)
 //   prepare beta = v / c, beta^2, phi / c^2, a_N / c^2 (PREPARE_RELATIVITY, mass.impl:76-80)
 //   pass B  EIH 1PN (RELATIVITY, mass.impl:82-97) and the per-pair maxima of 1/r and GM_j/r^3
-//           (RungeKutta.cu:229-230), recomputed exactly for the extremal pair
+//           (RungeKutta.cu:229-230), recomputed exactly for the extremal pair; in the mixed-precision form
+//           (eph_batch_set_precision) the 1PN terms in FP32 (pair_point_b32)
 //   final   phi c^2, a_N c^2 (FINALIZE_RELATIVITY, mass.impl:133-135); f = (gaccel + daccel) + naccel
 // For such bodies the reference's angular velocity, G*L and harmonics stay constant (w = G*L = 0), the
 // frame rotations are the identity and only the end-of-step orthogonalisation of the frame acts
@@ -66,7 +67,11 @@ struct BatchSys {
 // shared-memory rows of one system, stride `ld` bodies
 enum BRow { BR_R_HI = 0, BR_R_LO = 3, BR_GM = 6, BR_SR2 = 7, BR_PHI = 8, BR_NACC = 9, BR_BETA = 12, BR_BETA2 = 15,
             BR_V_HI = 16, BR_V_LO = 19, BR_FA = 22, BR_GA = 25, BR_MIND = 28, BR_MAXI = 29, BR_GM0 = 30, BR_DGM = 31,
-            BR_ROWS = 32 };
+            BR_F32 = 32, BR_ROWS = 37 };
+// FP32 rows of the mixed-precision form (single-precision copies of what its pass-B pair terms read of body
+// j), packed two to a double row from BR_F32 on
+enum FRow { F_GM = 0, F_PHI = 1, F_NACC = 2, F_BETA = 5, F_BETA2 = 8, F_ROWS = 9 };
+static_assert((F_ROWS + 1) / 2 <= BR_ROWS - BR_F32, "FP32 rows do not fit");
 
 struct BatchView {
     double *T;    // rows
@@ -74,6 +79,9 @@ struct BatchView {
 };
 
 __device__ __forceinline__ double &row(const BatchView &V, int r, int i) { return V.T[r * V.ld + i]; }
+__device__ __forceinline__ float &frow(const BatchView &V, int r, int i) {
+    return reinterpret_cast<float *>(V.T + BR_F32 * V.ld)[r * V.ld + i];
+}
 
 // pass A pair (i, j): acc = {phi, a_N}
 __device__ __forceinline__ void pair_point_a(const BatchView &V, int i, int j, double acc[4]) {
@@ -128,6 +136,65 @@ __device__ __forceinline__ void pair_point_b(const BatchView &V, int i, int j, d
     acc[2] += g.z;
 }
 
+// Mixed-precision form of the pass-B pair: the separation and its floored square stay FP64 (so the per-pair
+// maxima keep the reference's exact recomputation of the extremal pair), the EIH 1PN acceleration (about
+// 1e-8 of the Newtonian one for solar-system speeds and potentials, so FP32's 6e-8 relative rounding is
+// ~1e-15 of the total) is formed in FP32 from FP32 copies of the pass-A outputs and summed with a
+// compensated FP32 sum (Fast2Sum after each add), which the caller converts into its FP64 totals. The
+// extremal pair of max_influence is chosen on the FP32 value of GM/r^3, so in a near-tie (within FP32
+// rounding) another pair's value may be the one recomputed.
+struct BodyF32 {   // body i's FP32 pass-B inputs
+    float phi, beta2, bx, by, bz;
+};
+struct Comp32 {    // compensated FP32 sums of the three 1PN components
+    float s[3], c[3];
+};
+struct PairMax32 {
+    double m_min;          // smallest floored r^2 (FP64)
+    float tq;              // largest FP32 GM_j/r^3 seen
+    double tq_m, tq_gm;    // its r^2 and GM_j
+};
+__device__ __forceinline__ void comp_add(float &s, float &c, float x) {
+    const float t = __fadd_rn(s, x);
+    const float big = fabsf(s) >= fabsf(x) ? s : x, small = fabsf(s) >= fabsf(x) ? x : s;
+    c = __fadd_rn(c, __fadd_rn(__fsub_rn(big, t), small));
+    s = t;
+}
+__device__ __forceinline__ void pair_point_b32(const BatchView &V, int i, int j, const BodyF32 &bi, Comp32 &acc,
+                                               PairMax32 &x) {
+    const v3 r = mk(sep_diff(row(V, BR_R_HI + 0, j), row(V, BR_R_LO + 0, j), row(V, BR_R_HI + 0, i), row(V, BR_R_LO + 0, i)),
+                    sep_diff(row(V, BR_R_HI + 1, j), row(V, BR_R_LO + 1, j), row(V, BR_R_HI + 1, i), row(V, BR_R_LO + 1, i)),
+                    sep_diff(row(V, BR_R_HI + 2, j), row(V, BR_R_LO + 2, j), row(V, BR_R_HI + 2, i), row(V, BR_R_LO + 2, i)));
+    const double q = dot(r, r), sm = row(V, BR_SR2, i) + row(V, BR_SR2, j);
+    const double m = (q < sm) ? sm : q;
+    if (x.m_min == x.m_min) x.m_min = (m != m || m < x.m_min) ? m : x.m_min;
+    const float rr = rsqrtf((float)m);
+    const float rr2 = rr * rr;
+    const float tp_dphi = rr * frow(V, F_GM, j);
+    const float tp_dg = rr2 * tp_dphi;
+    if (x.tq == x.tq) {
+        if (tp_dg != tp_dg) x.tq = tp_dg;
+        else if (tp_dg > x.tq) { x.tq = tp_dg; x.tq_m = m; x.tq_gm = row(V, BR_GM, j); }
+    }
+    const float rx = (float)r.x, ry = (float)r.y, rz = (float)r.z;
+    const float bjx = frow(V, F_BETA + 0, j), bjy = frow(V, F_BETA + 1, j), bjz = frow(V, F_BETA + 2, j);
+    const float rbj = rx * bjx + ry * bjy + rz * bjz;
+    float tp = rbj * rr;
+    tp *= tp;
+    const float nax = frow(V, F_NACC + 0, j), nay = frow(V, F_NACC + 1, j), naz = frow(V, F_NACC + 2, j);
+    const float delta1 = 4 * bi.phi + frow(V, F_PHI, j) + bi.beta2 + 2 * frow(V, F_BETA2, j) -
+                         4 * (bi.bx * bjx + bi.by * bjy + bi.bz * bjz) + ((rx * nax + ry * nay + rz * naz) - 3 * tp) / 2;
+    const float bx = bjx - bi.bx, by = bjy - bi.by, bz = bjz - bi.bz;
+    const float c1 = 7 * tp_dphi / 2, c2 = tp_dg * delta1, c3 = tp_dg * (rbj - (rx * bx + ry * by + rz * bz) * 4);
+    comp_add(acc.s[0], acc.c[0], c1 * nax + c2 * rx + c3 * bx);
+    comp_add(acc.s[1], acc.c[1], c1 * nay + c2 * ry + c3 * by);
+    comp_add(acc.s[2], acc.c[2], c1 * naz + c2 * rz + c3 * bz);
+}
+__device__ __forceinline__ BodyF32 body_f32(const BatchView &V, int i) {
+    return BodyF32{frow(V, F_PHI, i), frow(V, F_BETA2, i), frow(V, F_BETA + 0, i), frow(V, F_BETA + 1, i),
+                   frow(V, F_BETA + 2, i)};
+}
+
 // Threads of a pass: with n <= blockDim bodies, G consecutive lanes of a warp share body i and split its j
 // range (G = the largest power of two <= min(32, blockDim / n)); their partial sums are combined by warp
 // shuffles. With more bodies than threads each thread takes whole bodies.
@@ -176,6 +243,13 @@ __device__ __forceinline__ void prepare_body(const BatchView &V, int i, const do
     row(V, BR_NACC + 0, i) = na.x;
     row(V, BR_NACC + 1, i) = na.y;
     row(V, BR_NACC + 2, i) = na.z;
+    // FP32 copies for the mixed-precision pass B (written in both forms; unused by the FP64 one)
+    frow(V, F_PHI, i) = (float)row(V, BR_PHI, i);
+    frow(V, F_BETA2, i) = (float)row(V, BR_BETA2, i);
+    for (int c = 0; c < 3; ++c) {
+        frow(V, F_NACC + c, i) = (float)row(V, BR_NACC + c, i);
+        frow(V, F_BETA + c, i) = (float)row(V, BR_BETA + c, i);
+    }
 }
 
 // pass A (and PREPARE_RELATIVITY) of the bodies i in [lo, hi) against all n bodies
@@ -240,6 +314,61 @@ __device__ __forceinline__ void extremes_of(const PairMax &x, double &inv_r, dou
         const double r2 = 1.0 / x.tq_m;
         infl = r2 * (sqrt(r2) * x.tq_gm);
     } else infl = 0.0;
+}
+
+// exact extremes of the mixed form's tracking (the same expressions on the tracked FP64 values)
+__device__ __forceinline__ void extremes_of32(const PairMax32 &x, double &inv_r, double &infl) {
+    inv_r = sqrt(1.0 / x.m_min);
+    if (x.tq != x.tq) infl = (double)x.tq;
+    else if (x.tq > 0) {
+        const double r2 = 1.0 / x.tq_m;
+        infl = r2 * (sqrt(r2) * x.tq_gm);
+    } else infl = 0.0;
+}
+
+// mixed-precision pass B: two pair chains per thread like the FP64 form, FP32 1PN sums converted into FP64
+__device__ void pass_point_b32(const BatchView &V, int n, int lo, int hi) {
+    const PassMap m = pass_map(lo, hi);
+    const double inf = __longlong_as_double(0x7ff0000000000000ll);
+    auto sweep = [&](int i, int j0, int step, double s[5]) {
+        const BodyF32 bi = body_f32(V, i);
+        Comp32 a{{0, 0, 0}, {0, 0, 0}}, a2{{0, 0, 0}, {0, 0, 0}};
+        PairMax32 x{inf, 0.0f, 0.0, 0.0}, x2{inf, 0.0f, 0.0, 0.0};
+        int j = j0;
+#pragma unroll 1
+        for (; j + step < n; j += 2 * step) {
+            if (j != i) pair_point_b32(V, i, j, bi, a, x);
+            if (j + step != i) pair_point_b32(V, i, j + step, bi, a2, x2);
+        }
+        if (j < n && j != i) pair_point_b32(V, i, j, bi, a, x);
+        for (int c = 0; c < 3; ++c)
+            s[c] = ((double)a.s[c] + (double)a.c[c]) + ((double)a2.s[c] + (double)a2.c[c]);
+        double f0, f1;
+        extremes_of32(x, s[3], s[4]);
+        extremes_of32(x2, f0, f1);
+        checked_maximize(s[3], f0);
+        checked_maximize(s[4], f1);
+    };
+    if (m.grouped) {
+        double s[5] = {0, 0, 0, 0, 0};
+        if (m.active) sweep(m.i, m.sub, m.G, s);
+        else {
+            const PairMax32 none{inf, 0.0f, 0.0, 0.0};
+            extremes_of32(none, s[3], s[4]);
+        }
+        for (int c = 0; c < 3; ++c) s[c] = group_sum(s[c], m.G);
+        s[3] = group_max(s[3], m.G);
+        s[4] = group_max(s[4], m.G);
+        if (m.active && m.sub == 0) finish_body(V, m.i, s);
+    } else {
+#pragma unroll 1
+        for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+            double s[5];
+            sweep(i, 0, 1, s);
+            finish_body(V, i, s);
+        }
+    }
+    __syncthreads();
 }
 
 // pass B and finalisation of the bodies i in [lo, hi) against all n bodies
@@ -333,10 +462,26 @@ __device__ void broadcast_rows(const BatchView &V, int row0, int nrows, int lo, 
     }
 }
 
+// The same for FP32 rows [row0, row0 + nrows).
+__device__ void broadcast_frows(const BatchView &V, int row0, int nrows, int lo, int hi, int rank) {
+    cg::cluster_group cl = cg::this_cluster();
+    const int cnt = hi - lo;
+    float *mine = reinterpret_cast<float *>(V.T + BR_F32 * V.ld);
+    for (int q = 0; q < kCluster; ++q) {
+        if (q == rank) continue;
+        float *peer = reinterpret_cast<float *>(cl.map_shared_rank(V.T, q) + BR_F32 * V.ld);
+        for (int idx = threadIdx.x; idx < nrows * cnt; idx += blockDim.x) {
+            const int r = row0 + idx / cnt, i = lo + idx % cnt;
+            peer[r * V.ld + i] = mine[r * V.ld + i];
+        }
+    }
+}
+
 // One system on one CTA (coop = false) or on the kCluster CTAs of a cluster (coop = true), this CTA
 // owning bodies [lo, hi): every CTA holds all bodies' rows, computes its own bodies' stages and passes,
 // and sends the rows the other CTAs read (positions and GM after the state update, the pass-A outputs
 // after pass A) to their shared memory.
+template <bool MIXED>
 __device__ void integrate_system(const BatchSys &Y, const BatchView &V, bool coop, int rank) {
     const int n = Y.n;
     const int lo = coop ? (int)((long long)rank * n / kCluster) : 0;
@@ -353,6 +498,7 @@ __device__ void integrate_system(const BatchSys &Y, const BatchView &V, bool coo
             row(V, BR_GA + c, i) = PLV(EPH_P_GACCEL + c, i);
         }
         row(V, BR_GM, i) = PLV(EPH_P_GM, i);
+        frow(V, F_GM, i) = (float)PLV(EPH_P_GM, i);
         row(V, BR_SR2, i) = PLV(EPH_P_SR2, i);
         row(V, BR_GM0, i) = PLV(EPH_P_GM0, i);
         row(V, BR_DGM, i) = PLV(EPH_P_DGM, i);
@@ -418,6 +564,7 @@ __device__ void integrate_system(const BatchSys &Y, const BatchView &V, bool coo
                     row(V, BR_V_LO + c, i) = v.lo;
                 }
                 row(V, BR_GM, i) = row(V, BR_GM0, i) + row(V, BR_DGM, i) * t;
+                frow(V, F_GM, i) = (float)row(V, BR_GM, i);
                 if (k == kStages) orthogonalize_frame(pl, n, i);
             }
             __syncthreads();
@@ -426,14 +573,17 @@ __device__ void integrate_system(const BatchSys &Y, const BatchView &V, bool coo
                 // in its own shared memory, before they are overwritten there
                 cg::this_cluster().sync();
                 broadcast_rows(V, BR_R_HI, BR_GM + 1 - BR_R_HI, lo, hi, rank);
+                if (MIXED) broadcast_frows(V, F_GM, 1, lo, hi, rank);
                 cg::this_cluster().sync();
             }
             pass_point_a(V, n, lo, hi);
             if (coop) {
                 broadcast_rows(V, BR_PHI, BR_BETA2 + 1 - BR_PHI, lo, hi, rank);
+                if (MIXED) broadcast_frows(V, F_PHI, F_ROWS - F_PHI, lo, hi, rank);
                 cg::this_cluster().sync();
             }
-            pass_point_b(V, n, lo, hi);
+            if (MIXED) pass_point_b32(V, n, lo, hi);
+            else pass_point_b(V, n, lo, hi);
         }
     }
     // store (cuda_rungekutta_kernel_config::save of RungeKutta.cu:124-133); min_distance inverted (mass.cpp:436)
@@ -463,6 +613,7 @@ __device__ void integrate_system(const BatchSys &Y, const BatchView &V, bool coo
 // Persistent CTAs in clusters of kCluster. Jobs [0, n_coop) of the queue (the large systems) are taken a
 // cluster at a time and shared by its CTAs; once a cluster draws a job past them, its CTAs take the
 // remaining jobs one CTA each.
+template <bool MIXED>
 __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kBThreads, 2)
     ensemble_kernel(const BatchSys *sys, const int *order, int n_sys, int n_coop, int *next, int ld) {
     extern __shared__ __align__(16) double bsm[];
@@ -482,7 +633,7 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kBThreads, 2)
             cl.sync();   // read by all before rank 0 may reuse s_job
             if (job >= n_sys) return;
             if (job < n_coop) {
-                integrate_system(sys[order[job]], V, true, rank);
+                integrate_system<MIXED>(sys[order[job]], V, true, rank);
                 continue;
             }
             together = false;
@@ -494,7 +645,7 @@ __global__ void __cluster_dims__(kCluster, 1, 1) __launch_bounds__(kBThreads, 2)
             __syncthreads();
             if (job >= n_sys) return;
         }
-        integrate_system(sys[order[job]], V, false, 0);
+        integrate_system<MIXED>(sys[order[job]], V, false, 0);
     }
 }
 
@@ -510,7 +661,10 @@ cudaError_t batch_setup(int device) {
     cudaError_t e = cudaMemcpyToSymbol(b_rk_hi, hi, sizeof(hi));
     if (e == cudaSuccess) e = cudaMemcpyToSymbol(b_rk_lo, lo, sizeof(lo));
     if (e == cudaSuccess) e = cudaMemcpyToSymbol(b_dtk, dtk, sizeof(dtk));
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(ensemble_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBMaxSmem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(ensemble_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBMaxSmem);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(ensemble_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBMaxSmem);
     if (e == cudaSuccess && device >= 0 && device < 64) g_batch_ready[device] = true;
     return e;
 }
@@ -524,6 +678,7 @@ struct eph_batch {
     int device = 0;
     cudaStream_t stream = nullptr;     // work stream (own_stream unless eph_batch_set_stream chose another)
     cudaStream_t own_stream = nullptr;
+    int mixed = 0;                     // 1: EIH 1PN terms of the ensemble kernel in FP32 (eph_batch_set_precision)
     std::mutex mu;
     char err[512] = {0};
     int n_sys = 0;
@@ -709,13 +864,16 @@ int eph_batch_integrate(eph_batch *b, const double *dt, const int64_t *n_step, d
         BCK(cudaMemsetAsync(b->d_next, 0, sizeof(int), b->stream), "reset batch queue");
         const size_t smem = ensemble_smem(b->ld);
         int per_sm = 0, sms = 0;
-        BCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ensemble_kernel, kBThreads, smem), "occupancy");
+        BCK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ensemble_kernel<false>, kBThreads, smem), "occupancy");
         BCK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device), "SM count");
         // whole clusters; clusters that find no room start when others finish (no CTA waits on another cluster)
         int grid = std::min((int)order.size() * kCluster, std::max(per_sm * sms, kCluster));
         grid = std::max(kCluster, grid / kCluster * kCluster);
-        ensemble_kernel<<<grid, kBThreads, smem, b->stream>>>(b->d_sys, b->d_order, (int)order.size(), n_coop, b->d_next,
-                                                              b->ld);
+        const int nj = (int)order.size();
+        if (b->mixed)
+            ensemble_kernel<true><<<grid, kBThreads, smem, b->stream>>>(b->d_sys, b->d_order, nj, n_coop, b->d_next, b->ld);
+        else
+            ensemble_kernel<false><<<grid, kBThreads, smem, b->stream>>>(b->d_sys, b->d_order, nj, n_coop, b->d_next, b->ld);
         BCK(cudaGetLastError(), "launch ensemble kernel");
         b->launches++;
     }
@@ -781,6 +939,13 @@ int eph_batch_set_stream(eph_batch *b, void *stream) {
     std::lock_guard<std::mutex> lock(b->mu);
     if (!b->own_stream) b->own_stream = b->stream;
     b->stream = stream ? (cudaStream_t)stream : b->own_stream;
+    return EPH_OK;
+}
+
+int eph_batch_set_precision(eph_batch *b, int mode) {
+    if (!b || (mode != EPH_PREC_FP64 && mode != EPH_PREC_MIXED)) return bfail(b, EPH_ERR_ARG, "eph_batch_set_precision: unknown mode");
+    std::lock_guard<std::mutex> lock(b->mu);
+    b->mixed = mode == EPH_PREC_MIXED;
     return EPH_OK;
 }
 

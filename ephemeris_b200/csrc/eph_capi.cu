@@ -53,6 +53,8 @@ struct eph_ctx {
     int timers_grid = 0;
     double *d_traj = nullptr;            // stage records for massless particles (caller-owned), or null
     long long traj_base = 0;
+    long long wait_ns = kWaitDefaultNs;  // limit of the kernel's bounded waits
+    int stall_barrier = 0;               // set only for the duration of eph_selftest_wait_timeout
 };
 
 namespace eph {
@@ -334,6 +336,8 @@ static int run(eph_ctx *ctx, const StepParams &P) {
     S.timers = nullptr;
     S.traj = ctx->d_traj;
     S.traj_base = ctx->traj_base;
+    S.wait_ns = ctx->wait_ns;
+    S.stall_barrier = ctx->stall_barrier;
     if (ctx->d_timers) {
         if (ctx->timers_grid < ctx->grid) {
             cudaFree(ctx->d_timers);
@@ -401,6 +405,18 @@ int eph_deform(eph_ctx *ctx) {
     std::lock_guard<std::mutex> lock(ctx->mu);
     StepParams P{MODE_DEFORM, 0, 0, 0, 0.0, 0.0};
     return run(ctx, P);
+}
+
+int eph_selftest_wait_timeout(eph_ctx *ctx, int64_t wait_ns) {
+    if (!ctx || wait_ns < 100000 || wait_ns > kWaitDefaultNs) return fail(ctx, EPH_ERR_ARG, "eph_selftest_wait_timeout: bad arguments");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    ctx->wait_ns = wait_ns;
+    ctx->stall_barrier = 1;
+    StepParams P{MODE_ACCEL, 0, 0, 0, 0.0, 0.0};
+    const int rc = run(ctx, P);
+    ctx->wait_ns = kWaitDefaultNs;
+    ctx->stall_barrier = 0;
+    return rc;
 }
 
 int eph_set_stream(eph_ctx *ctx, void *stream) {

@@ -207,6 +207,8 @@ int body(int device, cudaStream_t stream, int n, double *d_planes, const eph_mod
     S.timers = nullptr;
     S.traj = nullptr;
     S.traj_base = 0;
+    S.wait_ns = kWaitDefaultNs;
+    S.stall_barrier = 0;
     if (n_step < 0) {   // mass.cpp:401-404
         n_step = -n_step;
         dt = -dt;

@@ -75,13 +75,39 @@ struct PartArgs {
     int *next;                  // particle-block queue
 };
 
-// Field of a purely zonal geopotential (Nt = 0), inline: gp_core's columns 0 and 1 only, with rolled
-// loops in a handful of registers, so the particle kernel keeps its occupancy when its only extended
-// perturber is zonal.
+// Field of a purely zonal geopotential (Nt = 0), inline: the Cunningham recursion of gp_core with its two
+// columns (m = 0 and m = 1, the only ones zonal terms read) advanced together in one loop over the degree,
+// V_k0 for a_z and V_k1 + i W_k1 for a_x, a_y, in a handful of registers, so the particle kernel keeps its
+// occupancy when its only extended perturber is zonal:
+//   a_z += k J_{k-1} V_k0,  a_x += J_{k-1} V_k1,  a_y += J_{k-1} W_k1   (k - 1 = 2 .. Nz), all / R^2.
 __device__ __forceinline__ v3 gp_zonal(const double *__restrict__ c_table, int Nz, double R, v3 r) {
-    v3 a = mk(0, 0, 0);
-    if (Nz >= 2) gp_core<double, true>(c_table, GP_RCP, Nz, 0, R, r.x, r.y, r.z, a.x, a.y, a.z);
-    return a;
+    if (Nz < 2) return mk(0, 0, 0);
+    double xs, ys, zs, rho2, v00;
+    gp_setup(R, r.x, r.y, r.z, xs, ys, zs, rho2, v00);
+    double a0 = v00, a0p = 0;            // column 0 at degrees k, k - 1
+    double b1 = xs * v00, c1 = ys * v00; // column 1 (V, W) at degree k = 1 (the diagonal)
+    double b1p = 0, c1p = 0;
+    a0p = a0;
+    a0 = zs * v00;                       // V_10
+    double ax = 0, ay = 0, az = 0;
+#pragma unroll 1
+    for (int k = 2; k <= Nz + 1; ++k) {
+        const double kd = (double)k, f = 2 * kd - 1;
+        const double n0 = (f * zs * a0 - (kd - 1) * rho2 * a0p) * __ldg(GP_RCP + k);
+        const double rc = __ldg(GP_RCP + (k - 1));
+        const double nb = (f * zs * b1 - kd * rho2 * b1p) * rc, nc = (f * zs * c1 - kd * rho2 * c1p) * rc;
+        a0p = a0; a0 = n0;
+        b1p = b1; b1 = nb;
+        c1p = c1; c1 = nc;
+        if (k >= 3) {
+            const double J = __ldg(c_table + ((k - 1) * (k - 1) - 4));
+            az += kd * (J * a0);
+            ax += J * b1;
+            ay += J * c1;
+        }
+    }
+    const double s = 1.0 / (R * R);
+    return mk(ax * s, ay * s, az * s);
 }
 
 // Mixed precision: the perturber fields that the FP32 form reads, as floats, kPF32 per perturber.

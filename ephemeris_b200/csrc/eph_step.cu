@@ -26,7 +26,7 @@
 //   * the RK12 combination sum_j a_kj f_j is accumulated incrementally: when f_j is known it is added into
 //     the accumulators of every later stage k, in ascending j, which is the reference's summation order.
 //
-// All waits are bounded (kWaitTimeoutNs): a grid-barrier or copy wait that runs out records a status
+// All waits are bounded (S.wait_ns, 2 s by default): a grid-barrier or copy wait that runs out records a status
 // word and the kernel returns (after waiting, again bounded, for its own copies in flight); it never traps.
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -44,7 +44,6 @@
 namespace eph {
 
 constexpr double kC = 299792458.0;                      // src/math/basic_math.h:10,18
-constexpr unsigned long long kWaitTimeoutNs = 2000000000ull;
 
 __constant__ double c_rk_hi[EPH_RK12_NCOEF];            // a_kj, double-double
 __constant__ double c_rk_lo[EPH_RK12_NCOEF];
@@ -132,7 +131,8 @@ __device__ bool grid_sync(const SysDev &S, Scratch &sc) {
     if (gridDim.x == 1) return true;
     if (threadIdx.x == 0) {
         unsigned long long *count = reinterpret_cast<unsigned long long *>(S.bar);
-        const unsigned long long target = (sc.bar_target += gridDim.x);
+        // (S.stall_barrier: a self-test asks for one arrival more than the launch has, so every wait runs out)
+        const unsigned long long target = (sc.bar_target += gridDim.x + (S.stall_barrier ? 1u : 0u));
         unsigned long long old;
         asm volatile("atom.acq_rel.gpu.global.add.u64 %0, [%1], 1;" : "=l"(old) : "l"(count) : "memory");
         int fail = 0;
@@ -144,7 +144,7 @@ __device__ bool grid_sync(const SysDev &S, Scratch &sc) {
             if ((it & 15) == 15) {
                 const unsigned long long t = global_ns();
                 if (t0 == 0) t0 = t;
-                else if (t - t0 > kWaitTimeoutNs) {
+                else if (t - t0 > (unsigned long long)S.wait_ns) {
                     atomicExch(S.status, (int)ST_BARRIER_TIMEOUT);
                     fail = 1;
                     break;
@@ -222,7 +222,7 @@ __device__ bool load_tile(const SysDev &S, Scratch &sc, TileState &ts, double *t
         if ((it & 63) == 0) {
             unsigned long long t = global_ns();
             if (t0 == 0) t0 = t;
-            else if (t - t0 > kWaitTimeoutNs) {
+            else if (t - t0 > (unsigned long long)S.wait_ns) {
                 if (threadIdx.x == 0) atomicExch(S.status, (int)ST_COPY_TIMEOUT);
                 // give the copies in flight one more bounded wait before the CTA leaves
                 const unsigned long long t1 = global_ns();
@@ -232,7 +232,7 @@ __device__ bool load_tile(const SysDev &S, Scratch &sc, TileState &ts, double *t
                         : "=r"(done)
                         : "r"(mb), "r"(parity)
                         : "memory");
-                    if (done || global_ns() - t1 > kWaitTimeoutNs) break;
+                    if (done || global_ns() - t1 > (unsigned long long)S.wait_ns) break;
                 }
                 return false;
             }

@@ -85,7 +85,11 @@ struct SysDev {
     unsigned long long *timers;   // optional [grid][kPhases] nanoseconds per phase (profiling), or null
     double *traj;             // optional stage records [slot][n][kTrajRec] (massless-particle integration), or null
     long long traj_base;      // slot of this launch's first stage evaluation
+    long long wait_ns;        // limit of every bounded wait (grid barrier, tile copy), nanoseconds
+    int stall_barrier;        // self-test only: the grid barriers wait for one arrival more than the launch has
 };
+
+constexpr long long kWaitDefaultNs = 2000000000ll;   // 2 s
 
 // One stage record of a body (written after pass A, caller's body order): what a massless particle's
 // stage evaluation reads of the massive bodies.

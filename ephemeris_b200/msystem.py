@@ -198,6 +198,10 @@ class Batch:
         self._check(self.lib.eph_batch_upload(self.h, len(pls), n, ptrs, mptrs), "batch upload")
         self.sizes = [p.shape[1] for p in pls]
 
+    def set_precision(self, mixed: bool):
+        """FP32 EIH 1PN terms in the ensemble launch (True) or plain FP64 (False)."""
+        self._check(self.lib.eph_batch_set_precision(self.h, 1 if mixed else 0), "batch set_precision")
+
     def integrate(self, dt, n_step, t_eph=None):
         k = len(self.sizes)
         dts = np.ascontiguousarray(np.broadcast_to(np.asarray(dt, np.float64), (k,)))

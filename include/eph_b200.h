@@ -84,6 +84,13 @@ int eph_accel(eph_ctx *ctx);
  * state (potential, Newtonian acceleration, C_potential, GI), as used by the loader. */
 int eph_deform(eph_ctx *ctx);
 
+/* Self-test of the bounded waits (no counterpart in the reference, whose kernel's grid.sync cannot time
+ * out): one acceleration evaluation of the uploaded system whose grid barriers wait for one arrival more
+ * than the launch has, with every wait limited to wait_ns (1e5 .. 2e9 ns). Every CTA's wait runs out, the
+ * kernel records the timeout and returns, and the call returns EPH_ERR_TIMEOUT; the context stays usable and
+ * the next call runs normally (with the default 2 s limit). The uploaded planes are not written. */
+int eph_selftest_wait_timeout(eph_ctx *ctx, int64_t wait_ns);
+
 /* Issue this context's device work on `stream` (a cudaStream_t of the context's device; NULL restores
  * the context's own stream). Calls still return only after their work has finished. */
 int eph_set_stream(eph_ctx *ctx, void *stream);
@@ -118,6 +125,10 @@ int eph_phase_times(eph_ctx *ctx, uint64_t *out, int *grid, int *phases);
  * each with its own dt, step count and ephemeris time, integrated with msystem::integrate semantics
  * (mass.cpp:399-442). Systems whose bodies are all point-like (Newtonian + 1PN only) share one persistent
  * launch, one CTA per system; any other system runs through the single-system kernel. */
+/* Arithmetic modes of the batched and particle paths */
+#define EPH_PREC_FP64 0
+#define EPH_PREC_MIXED 1
+
 typedef struct eph_batch eph_batch;
 int eph_batch_create(int device, eph_batch **out);
 int eph_batch_destroy(eph_batch *b);
@@ -134,6 +145,11 @@ int eph_batch_download(eph_batch *b, double *const *planes);
 /* Issue the batch's device work on `stream` (a cudaStream_t of its device; NULL restores its own stream).
  * Calls still return only after their work has finished. */
 int eph_batch_set_stream(eph_batch *b, void *stream);
+/* Arithmetic of the ensemble launch's EIH 1PN terms: EPH_PREC_FP64 (default) or EPH_PREC_MIXED (those terms in
+ * FP32 from FP32 copies of the pass-A outputs, summed with a compensated FP32 sum and added into the FP64
+ * totals; state, separations, the Newtonian sums, the per-pair maxima and the RK12 combination stay FP64 /
+ * double-double). Applies from the next integrate; systems on the single-system path are not affected. */
+int eph_batch_set_precision(eph_batch *b, int mode);
 /* Systems in the shared ensemble launch, and launches issued so far. */
 int eph_batch_info(const eph_batch *b, int32_t *n_ensemble, int64_t *launches);
 
@@ -159,8 +175,6 @@ int eph_particles_set_stream(eph_particles *p, void *stream);
 /* Arithmetic of the particles' EIH 1PN terms: EPH_PREC_FP64 (default) or EPH_PREC_MIXED (those terms,
  * ~1e-8 of the Newtonian acceleration, in FP32; state, separations, Newtonian, deformation, field terms
  * and the RK12 combination stay FP64 / double-double). Applies from the next integrate. */
-#define EPH_PREC_FP64 0
-#define EPH_PREC_MIXED 1
 int eph_particles_set_precision(eph_particles *p, int mode);
 /* Kernels launched so far and the summed device time of the particle kernel (CUDA events, ms). */
 int eph_particles_info(const eph_particles *p, int64_t *launches, double *particle_kernel_ms);

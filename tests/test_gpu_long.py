@@ -77,8 +77,10 @@ def _ulp_sensitivity(oracle, pl, om, dt, steps, ref):
     return position_error(oracle.integrate(p2, om, dt, steps)[0], ref)
 
 
-def test_thousand_steps_ensemble_members(tmp_path, oracle):
-    """Members of the ensemble recipe (Newtonian + 1PN) in one eph_batch launch, 1000 steps against the oracle.
+@pytest.mark.parametrize("mixed", [False, True])
+def test_thousand_steps_ensemble_members(tmp_path, oracle, mixed):
+    """Members of the ensemble recipe (Newtonian + 1PN) in one eph_batch launch, 1000 steps against the oracle,
+    in FP64 and in the mixed-precision form (FP32 1PN terms).
 
     The first four are well conditioned (a one-ulp change of the start moves the oracle by < 1e-12 after
     1000 steps): they must meet 1e-12. The last one has a close moon pair whose own one-ulp sensitivity is
@@ -93,6 +95,7 @@ def test_thousand_steps_ensemble_members(tmp_path, oracle):
         assert ms.load(cfg)
         mem.append((ms.planes(), ms.models(), ms.delta_t))
     b = Batch(0)
+    b.set_precision(mixed)
     b.upload([m[0] for m in mem], [m[1] for m in mem])
     assert b.info()[0] == len(cases)
     b.integrate([m[2] for m in mem], [1000] * len(cases))
@@ -102,8 +105,8 @@ def test_thousand_steps_ensemble_members(tmp_path, oracle):
         ref = oracle.integrate(pl, om, dt, 1000)[0]
         pe = position_error(out, ref)
         sens = _ulp_sensitivity(oracle, pl, om, dt, 1000, ref)
-        print(f"ensemble member seed {cases[k][0]} n={pl.shape[1]} step 1000: position {pe:.2e} "
-              f"(oracle one-ulp sensitivity {sens:.2e})")
+        print(f"ensemble member ({'mixed' if mixed else 'fp64'}) seed {cases[k][0]} n={pl.shape[1]} step 1000: "
+              f"position {pe:.2e} (oracle one-ulp sensitivity {sens:.2e})")
         assert np.isfinite(out[0:12]).all()
         if k < 4:
             assert sens < POS_TOL
@@ -144,3 +147,35 @@ def test_thousand_steps_particles(tmp_path, oracle, mixed):
     assert np.isfinite(out[0:12]).all()
     assert pe_pert <= POS_TOL
     assert pe_part <= POS_TOL
+
+
+MIXED_ACC_TOL = 1e-13
+
+
+def test_mixed_ensemble_stage_acceleration(tmp_path, oracle):
+    """The mixed-precision ensemble's accelerations after one step against the oracle's. The 1e-14 per-stage
+    bound is the plain FP64 path's; the mixed form's criterion is the 1000-step position error (1e-12, above).
+    Its per-stage error is the FP32 rounding of the 1PN terms: each ~6e-8 of a term ~1e-8 of the Newtonian
+    acceleration, summed over up to 300 partners, so it is held to MIXED_ACC_TOL of sum_j |GM_j/r_ij^2|. The
+    per-pair maxima within 1e-6 (their extremal pair is chosen on FP32 values, then recomputed in FP64)."""
+    from ephemeris_b200 import Batch, MSystem, synth
+    from tests.parity import accel_error
+    mem = []
+    for k, n in enumerate((33, 120, 300)):
+        cfg = synth.write_system(synth.make_ensemble_member(3003 * 1000 + 600 + k, n), os.path.join(str(tmp_path), f"a{k}"))
+        ms = MSystem(0)
+        assert ms.load(cfg)
+        mem.append((ms.planes(), ms.models(), ms.delta_t))
+    b = Batch(0)
+    b.set_precision(True)
+    b.upload([m[0] for m in mem], [m[1] for m in mem])
+    b.integrate([m[2] for m in mem], [1, 1, 1])
+    for (pl, md, dt), out in zip(mem, b.download()):
+        ref = oracle.integrate(pl, _omodels(md), dt, 1)[0]
+        ae = accel_error(out, ref)
+        print(f"mixed ensemble n={pl.shape[1]} one step: acceleration {ae:.2e}, position {position_error(out, ref):.2e}")
+        assert ae <= MIXED_ACC_TOL
+        assert position_error(out, ref) <= POS_TOL
+        for p in (100, 101):
+            assert rel_err(out[p], ref[p]) <= 1e-6
+    b.close()
