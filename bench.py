@@ -209,6 +209,24 @@ def cpu_baseline(cfg, n_steps: int):
     raise RuntimeError("oracle/_ref missing")
 
 
+def reference_gpu_baseline(cfg, rk_steps: int = 10, calls: int = 3):
+    """The reference's own GPU integrator (its cooperative kernel compiled unchanged for sm_100a,
+    oracle/_ref/libephref_gpu.so) on the same system, in a child process (its CUDA error handler exits the
+    process): one step checked against its CPU integrator with its own bounds, then timed by wall clock."""
+    path = os.path.join(ROOT, "oracle", "_ref", "libephref_gpu.so")
+    if not os.path.exists(path):
+        return {"unavailable": "oracle/_ref/libephref_gpu.so not built"}
+    try:
+        out = subprocess.run([sys.executable, "-m", "oracle.ref_gpu_timing", cfg, str(rk_steps), str(calls)],
+                             cwd=ROOT, capture_output=True, text=True, timeout=240)
+        lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
+        if out.returncode != 0 or not lines:
+            return {"unavailable": f"exit {out.returncode}: {(out.stderr or out.stdout)[-200:]}"}
+        return json.loads(lines[-1])
+    except Exception as exc:
+        return {"unavailable": f"{type(exc).__name__}: {exc}"}
+
+
 def run_reference(args):
     """--impl reference: the reference CPU integrator, rank 0 only."""
     rank = int(os.environ.get("RANK", "0"))
@@ -426,6 +444,11 @@ def run_b200_ensemble(args):
     dev = torch.device("cuda", local)
     with tempfile.TemporaryDirectory() as td:
         pls, mds, dts, ks, cfgs = load_ensemble(args, td, local)
+        body_steps_all = float(sum(p.shape[1] * k for p, k in zip(pls, ks)))
+        if world > 1:   # this rank's share of the members (longest processing time first; no exchange)
+            from ephemeris_b200 import shard
+            mine = shard.partition([shard.member_cost(p.shape[1], k) for p, k in zip(pls, ks)], world)[rank]
+            pls, mds, dts, ks, cfgs = ([x[i] for i in mine] for x in (pls, mds, dts, ks, cfgs))
         stream = torch.cuda.Stream(dev)
         torch.cuda.set_stream(stream)
         b = Batch(local)
@@ -453,7 +476,7 @@ def run_b200_ensemble(args):
         launches = b.info()[1] - l0
         dev_ms_max = reduce_max(pg, dev_ms, dev)
         body_steps = float(sum(p.shape[1] * k for p, k in zip(pls, ks)))
-        value = world * body_steps * args.steps / (dev_ms_max / 1e3)
+        value = body_steps_all * args.steps / (dev_ms_max / 1e3)
         compare = None
         if args.ens_compare and world == 1:
             # the same ensemble in the mixed-precision form, the plain FP64 path one member at a time, and
@@ -489,7 +512,7 @@ def run_b200_ensemble(args):
             b.integrate(dts, ks)
             b.download()
         e2e_s = reduce_max(pg, time.perf_counter() - t0, dev)
-        e2e = world * body_steps * args.steps / e2e_s
+        e2e = body_steps_all * args.steps / e2e_s
         bytes_io = int(sum(p.nbytes for p in pls))
         flops = _ensemble_flops(pls, ks)
         achieved = flops / (dev_ms / args.steps / 1e3) / 1e12
@@ -511,7 +534,8 @@ def run_b200_ensemble(args):
                                        f"(Newtonian + 1PN), durations {min(ks)}-{max(ks)} RK12 steps "
                                        f"(the 500-20000 draw scaled by {args.ens_frac}), dt=0.05 day",
                            "systems": len(pls), "bodies": int(sum(sizes)), "body_steps_per_step": body_steps,
-                           "parallelism": f"replicas x{world}" if world > 1 else "one persistent launch, 1 GPU",
+                           "parallelism": (f"members sharded over {world} GPUs (longest processing time first, no "
+                                           f"exchange)") if world > 1 else "one persistent launch, 1 GPU",
                            "l2": "flushed between timed steps (256 MB write)"},
                 "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": bytes_io, "d2h_bytes_per_step": bytes_io},
                 "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
@@ -578,11 +602,13 @@ def particle_flops_per_step(pl, models):
     return 25 * per_stage + FLOP_RK
 
 
-def load_particles(args, tmpdir, rank, device=0):
-    """Perturbers (loaded by the product loader) and this rank's particles [6][n]."""
-    from ephemeris_b200 import MSystem, synth
-    sysm, parts = synth.make_config5(5005, n_particles=args.particles,
-                                     particle_seed=None if rank == 0 else 5005 * 1000 + rank)
+def load_particles(args, tmpdir, rank, device=0, world=1):
+    """Perturbers (loaded by the product loader) and this rank's particles [6][n]: one particle set of
+    --particles x world particles, cut into contiguous slices, one per rank (the perturbers replicated)."""
+    from ephemeris_b200 import MSystem, shard, synth
+    sysm, parts = synth.make_config5(5005, n_particles=args.particles * world)
+    lo, hi = shard.particle_slice(parts.shape[1], world, rank)
+    parts = np.ascontiguousarray(parts[:, lo:hi])
     cfg = synth.write_system(sysm, os.path.join(tmpdir, "perturbers"))
     ms = MSystem(device)
     if not ms.load(cfg):
@@ -634,8 +660,9 @@ def run_b200_particles(args):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     with tempfile.TemporaryDirectory() as td:
-        pl, md, dt, parts, sysm = load_particles(args, td, rank, local)
+        pl, md, dt, parts, sysm = load_particles(args, td, rank, local, world)
         n_part, ks = parts.shape[1], args.p_steps
+        n_total = args.particles * world
         stream = torch.cuda.Stream(dev)
         torch.cuda.set_stream(stream)
         p = Particles(local)
@@ -665,7 +692,7 @@ def run_b200_particles(args):
         part_launches = args.steps                   # one particle-kernel launch per call (all steps fit one round)
         kern_ms = (k1 - k0) / part_launches
         dev_ms_max = reduce_max(pg, dev_ms, dev)
-        value = world * n_part * ks * args.steps / (dev_ms_max / 1e3)
+        value = n_total * ks * args.steps / (dev_ms_max / 1e3)
         # end to end through the public API: host particles up, integrate, host particles down (pinned
         # host buffers: the state as double-double rows, as the API takes and returns it)
         z = np.zeros((3, n_part))
@@ -678,8 +705,11 @@ def run_b200_particles(args):
             p.upload(pl, md, pin)
             p.integrate(dt, ks)
             p.download(pl_out, pin_out)
+            if pg is not None:   # the one collective: the final states of every slice gathered to rank 0
+                from ephemeris_b200 import shard
+                shard.gather_rows(pin_out, n_total, pg, device=dev)
         e2e_s = reduce_max(pg, time.perf_counter() - t0, dev)
-        e2e = world * n_part * ks * args.steps / e2e_s
+        e2e = n_total * ks * args.steps / e2e_s
         mixed_err = None
         if args.mixed:   # position error of the mixed run against the FP64 run of the same particles
             part_mixed = pin_out.copy()
@@ -713,7 +743,8 @@ def run_b200_particles(args):
                                        f"i < 20 deg) against {pl.shape[1]} perturbers (star with J2-J4, 8 planets; "
                                        f"Newtonian + 1PN), dt=0.5 day, {ks} RK12 steps per bench step",
                            "particles": n_part, "perturbers": int(pl.shape[1]), "rk_steps_per_step": ks,
-                           "parallelism": f"particles sharded x{world}, perturbers replicated" if world > 1
+                           "parallelism": (f"one set of {n_total} particles cut into {world} slices, perturbers "
+                                           f"replicated, one gather of the final states (e2e)") if world > 1
                            else "1 GPU",
                            "l2": "flushed between timed steps (256 MB write); particle state 240 MB > L2",
                            "precision": "mixed (EIH 1PN in FP32)" if args.mixed else "fp64"},
@@ -966,8 +997,13 @@ def run_b200(args):
         rk = args.rk_steps
         ctx = Context(local)
         ctx.upload(planes0, models)
+        tune = None
         if args.grid or args.per_cta:
             ctx.set_launch(args.grid, args.per_cta)
+        elif not args.no_autotune:
+            g_, b_, t_tuned, t_default = ctx.autotune(dt, n_step=3, reps=2, use_cache=False)
+            tune = {"grid": g_, "bodies_per_cta": b_, "ms_per_rk_step_tuned": t_tuned,
+                    "ms_per_rk_step_heuristic": t_default, "by": "eph_autotune (outside the timed region)"}
         # a dedicated (non-default) stream: the context's kernels, the L2 flush and the events all go on it
         stream = torch.cuda.Stream(dev)
         ctx.set_stream(stream.cuda_stream)
@@ -1031,11 +1067,13 @@ def run_b200(args):
         peak, peak_src = fp64_peak(dev)
         pipe = fp64_pipe_peak(local)
         cpu = None
+        ref_gpu = None
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
             try:
                 cpu = cpu_baseline(cfg, args.cpu_rk_steps)
             except Exception as exc:   # the baseline is reported, not required
                 cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "unavailable", "sample": str(exc)}
+            ref_gpu = reference_gpu_baseline(cfg)
         if rank == 0:
             grid, per = ctx.launch_shape()
             line = {
@@ -1045,7 +1083,8 @@ def run_b200(args):
                 "config": {"workload": f"{args.workload}: {n}-body full-physics synthetic system (seeded), "
                                        f"dt=0.05 day", "rk_steps_per_step": rk, "bodies": n,
                            "parallelism": f"replicas x{world}" if world > 1 else "single system, 1 GPU",
-                           "l2": "flushed between timed steps (256 MB write)", "grid": grid, "bodies_per_cta": per},
+                           "l2": "flushed between timed steps (256 MB write)", "grid": grid, "bodies_per_cta": per,
+                           "autotune": tune},
                 "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(planes0.nbytes),
                         "d2h_bytes_per_step": int(planes0.nbytes)},
                 "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
@@ -1060,6 +1099,10 @@ def run_b200(args):
             }
             if cpu is not None:
                 line["cpu_baseline"] = cpu
+            if ref_gpu is not None:
+                if "value" in ref_gpu:
+                    ref_gpu["speedup_of_value"] = value / ref_gpu["value"]
+                line["reference_gpu"] = ref_gpu
             if world == 1 and args.workload == "config2" and not args.no_sub_records:
                 ctx.close()
                 line["sub_records"] = collect_sub_records(args)
@@ -1153,6 +1196,7 @@ def main():
     ap.add_argument("--grid", type=int, default=0)
     ap.add_argument("--per-cta", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="config2: keep the built-in launch shape")
     ap.add_argument("--ens-systems", type=int, default=512, help="config3: ensemble members")
     ap.add_argument("--ens-frac", type=float, default=0.1, help="config3: fraction of each member's drawn duration")
     ap.add_argument("--ens-cpu-members", type=int, default=64, help="config3: members in the CPU sample")

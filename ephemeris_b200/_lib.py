@@ -48,6 +48,8 @@ SIGNATURES = [
     ("eph_get_launch", ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     ("eph_launch_count", ctypes.c_int64, [_VP]),
     ("eph_set_body_costs", ctypes.c_int, [_VP, _D]),
+    ("eph_autotune", ctypes.c_int, [_VP, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                     ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), _D, _D]),
     ("eph_get_ownership", ctypes.c_int, [_VP, _I32, ctypes.POINTER(ctypes.c_int)]),
     ("eph_profile_phases", ctypes.c_int, [_VP, ctypes.c_int]),
     ("eph_phase_times", ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_int),

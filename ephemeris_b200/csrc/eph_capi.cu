@@ -5,7 +5,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <numeric>
 #include <vector>
 
@@ -465,6 +467,129 @@ int eph_get_ownership(const eph_ctx *ctx, int32_t *bodies, int *grid) {
         bodies[q] = k < 0 ? -1 : ctx->h_orig[k];
     }
     *grid = ctx->grid;
+    return EPH_OK;
+}
+
+// ---- autotuner: candidates of the launch shape and the ownership cost model, timed on the uploaded system
+namespace {
+struct TuneKey {
+    int device, n, n_full, n_delayed, n_ext;
+    bool operator<(const TuneKey &o) const {
+        return std::tie(device, n, n_full, n_delayed, n_ext) < std::tie(o.device, o.n, o.n_full, o.n_delayed, o.n_ext);
+    }
+};
+struct TuneChoice {
+    int req_grid, req_per;
+    double delayed_weight;   // 0: the built-in cost model
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, TuneChoice> g_tune_cache;
+}  // namespace
+
+static int apply_choice(eph_ctx *ctx, const double *h_planes, const TuneChoice &c) {
+    const int n = ctx->n;
+    if (c.delayed_weight > 0) {
+        std::vector<double> cost(n);
+        for (int i = 0; i < n; ++i) {
+            const bool full = plan_full_class(h_planes, n, i);
+            const bool delayed = h_planes[(size_t)EPH_P_K2 * n + i] != 0 && h_planes[(size_t)EPH_P_TIDE_DELAY * n + i] != 0;
+            cost[i] = delayed ? c.delayed_weight : plan_cost(h_planes, n, i, full);
+        }
+        ctx->cost_override = cost;
+    } else {
+        ctx->cost_override.clear();
+    }
+    ctx->req_grid = c.req_grid;
+    ctx->req_per_cta = c.req_per;
+    int rc = prepare_constants(ctx, h_planes);
+    return rc ? rc : choose_shape(ctx);
+}
+
+int eph_autotune(eph_ctx *ctx, double dt, int n_step, int reps, int use_cache, int *grid, int *bodies_per_cta,
+                 double *ms_tuned, double *ms_default) {
+    if (!ctx || !(dt != 0) || n_step < 1 || reps < 1 || !grid || !bodies_per_cta || !ms_tuned || !ms_default)
+        return fail(ctx, EPH_ERR_ARG, "eph_autotune: bad arguments");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    if (!ctx->n) return fail(ctx, EPH_ERR_STATE, "no system uploaded");
+    CK(cudaSetDevice(ctx->device), "cudaSetDevice");
+    const int n = ctx->n;
+    std::vector<double> h_planes((size_t)EPH_NPLANES * n);
+    CK(cudaMemcpy(h_planes.data(), ctx->d_planes, h_planes.size() * sizeof(double), cudaMemcpyDeviceToHost), "read planes");
+    int n_delayed = 0;
+    for (int i = 0; i < n; ++i)
+        n_delayed += h_planes[(size_t)EPH_P_K2 * n + i] != 0 && h_planes[(size_t)EPH_P_TIDE_DELAY * n + i] != 0;
+    const TuneKey key{ctx->device, n, ctx->n_full, n_delayed, ctx->n_ext};
+    // every trial integrates from the uploaded state, which is restored afterwards
+    double *d_save = nullptr;
+    CK(cudaMalloc(&d_save, h_planes.size() * sizeof(double)), "cudaMalloc(autotune)");
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int rc = EPH_OK;
+    auto time_choice = [&](const TuneChoice &c, double *ms) -> int {
+        int r = apply_choice(ctx, h_planes.data(), c);
+        if (r) return r;
+        double best = 1e300;
+        for (int q = 0; q < reps + 1 && r == EPH_OK; ++q) {   // the first run warms up
+            if (cudaMemcpyAsync(ctx->d_planes, d_save, h_planes.size() * sizeof(double), cudaMemcpyDeviceToDevice,
+                                ctx->stream) != cudaSuccess)
+                return fail(ctx, EPH_ERR_CUDA, "autotune restore");
+            cudaEventRecord(e0, ctx->stream);
+            const StepParams P{MODE_INTEGRATE, 0, 0, (long long)n_step, dt, 0.0};
+            r = run(ctx, P);
+            cudaEventRecord(e1, ctx->stream);
+            float t = 0;
+            if (r == EPH_OK && cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&t, e0, e1) == cudaSuccess) {
+                if (q > 0) best = std::min(best, (double)t / n_step);
+            }
+        }
+        *ms = best;
+        return r;
+    };
+    if (cudaMemcpy(d_save, ctx->d_planes, h_planes.size() * sizeof(double), cudaMemcpyDeviceToDevice) != cudaSuccess ||
+        cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
+        rc = fail(ctx, EPH_ERR_CUDA, "autotune set-up");
+    const TuneChoice heuristic{0, 0, 0.0};
+    double t_def = 1e300, t_best = 1e300;
+    TuneChoice best = heuristic;
+    if (rc == EPH_OK) rc = time_choice(heuristic, &t_def);
+    t_best = t_def;
+    bool cached = false;
+    if (rc == EPH_OK && use_cache) {
+        std::lock_guard<std::mutex> g(g_tune_mu);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) { best = it->second; cached = true; }
+    }
+    if (rc == EPH_OK && cached) {
+        rc = time_choice(best, &t_best);
+    } else if (rc == EPH_OK) {
+        std::vector<TuneChoice> cands;
+        for (int per : {1, 2, 3, 4, 6, 8}) cands.push_back(TuneChoice{0, per, 0.0});
+        if (n_delayed > 0)
+            for (double wd : {15.0, 25.0, 80.0})
+                for (int per : {0, 4, 8}) cands.push_back(TuneChoice{0, per, wd});
+        for (const TuneChoice &c : cands) {
+            double t = 1e300;
+            const int r = time_choice(c, &t);
+            if (r == EPH_ERR_ARG) continue;   // a shape that does not fit the co-resident CTAs
+            if (r) { rc = r; break; }
+            if (t < t_best) { t_best = t; best = c; }
+        }
+        if (rc == EPH_OK) {
+            std::lock_guard<std::mutex> g(g_tune_mu);
+            g_tune_cache[key] = best;
+        }
+    }
+    // leave the context on the chosen shape, with the uploaded state
+    if (rc == EPH_OK) rc = apply_choice(ctx, h_planes.data(), best);
+    if (cudaMemcpy(ctx->d_planes, d_save, h_planes.size() * sizeof(double), cudaMemcpyDeviceToDevice) != cudaSuccess && !rc)
+        rc = fail(ctx, EPH_ERR_CUDA, "autotune restore");
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(d_save);
+    if (rc) return rc;
+    *grid = ctx->grid;
+    *bodies_per_cta = ctx->per_cta;
+    *ms_tuned = t_best;
+    *ms_default = t_def;
     return EPH_OK;
 }
 

@@ -131,6 +131,15 @@ class Context:
     def launches(self) -> int:
         return int(self.lib.eph_launch_count(self.h))
 
+    def autotune(self, dt: float, n_step: int = 3, reps: int = 2, use_cache: bool = True):
+        """Time candidate launch shapes / cost models on the uploaded system and keep the fastest.
+        Returns (grid, bodies_per_cta, ms_per_step_tuned, ms_per_step_default)."""
+        g, b = ctypes.c_int(), ctypes.c_int()
+        t1, t0 = ctypes.c_double(), ctypes.c_double()
+        check(self.lib.eph_autotune(self.h, dt, n_step, reps, 1 if use_cache else 0, ctypes.byref(g), ctypes.byref(b),
+                                    ctypes.byref(t1), ctypes.byref(t0)), self.h, "autotune")
+        return g.value, b.value, t1.value, t0.value
+
     def set_body_costs(self, cost=None):
         """Per-body work estimates (caller order) for the ownership split; None restores the built-in ones."""
         if cost is None:

@@ -96,11 +96,20 @@ int eph_selftest_wait_timeout(eph_ctx *ctx, int64_t wait_ns);
 int eph_set_stream(eph_ctx *ctx, void *stream);
 
 /* Launch shape: grid = CTAs (0: automatic), bodies_per_cta (0: automatic, at most EPH_MAX_BODIES_PER_CTA).
- * The reference fixes its shape in code (RungeKutta.cu:80-88). */
+ * The reference fixes its shape in code (RungeKutta.cu:80-88); eph_autotune picks one by timing. */
 #define EPH_MAX_BODIES_PER_CTA 8
 int eph_set_launch(eph_ctx *ctx, int grid, int bodies_per_cta);
 /* Current launch shape. */
 int eph_get_launch(const eph_ctx *ctx, int *grid, int *bodies_per_cta);
+/* Autotuner (the reference fixes its launch shape in code, RungeKutta.cu:80-88): times candidate launch
+ * shapes (bodies per CTA, hence the grid) and ownership cost models (the weight of a delayed-tide body) of
+ * the step kernel on the uploaded system, n_step RK12 steps of dt each, best of `reps` after a warm-up run,
+ * every trial starting from the uploaded state; keeps the fastest through eph_set_launch /
+ * eph_set_body_costs and caches it per (device, bodies, body classes), so that with use_cache a later call on
+ * a system of the same key times only the cached choice. Leaves the uploaded state as it was. Returns the
+ * chosen shape and the per-RK12-step times of the choice and of the built-in heuristic. */
+int eph_autotune(eph_ctx *ctx, double dt, int n_step, int reps, int use_cache, int *grid, int *bodies_per_cta,
+                 double *ms_per_step_tuned, double *ms_per_step_default);
 /* Work estimates of the uploaded system's bodies (cost[n] > 0, caller order) that the split of bodies over
  * CTAs balances (longest processing time first); NULL restores the built-in estimate. Re-plans at once; an
  * upload keeps the override while the body count stays the same. */
