@@ -1,7 +1,8 @@
 """Regenerate the two constant data tables that the reference ships as hex source data.
 
 Run from the repository root with the reference tree available:
-    python oracle/gen_tables.py [/root/reference]
+    python oracle/gen_tables.py [REFERENCE_ROOT]
+(default: the REF_ROOT environment variable, as for oracle/Makefile)
 
 Outputs (committed, plain C headers usable from C, C++ and CUDA):
   include/eph_rk12_table.h  Feagin's 12th-order, 25-stage Runge-Kutta coefficients as 325
@@ -16,7 +17,9 @@ import os
 import re
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("REF_ROOT", "")
+if not REF:
+    sys.exit("usage: python oracle/gen_tables.py REFERENCE_ROOT (or set REF_ROOT)")
 HERE = os.path.dirname(os.path.abspath(__file__))
 INC = os.path.join(HERE, "..", "include")
 
