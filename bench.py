@@ -457,6 +457,12 @@ def run_b200_ensemble(args):
         for _ in range(args.warmup):   # warm-up: every member, 20 steps at most
             b.upload(pls, mds)
             b.integrate(dts, [min(k, 20) for k in ks])
+        tune = None
+        if args.ens_compare:   # the cluster-sharing threshold, tuned on 2 % of every member's steps
+            b.upload(pls, mds)
+            cm, t1, t0 = b.autotune(dts, ks, step_frac=0.02)
+            tune = {"coop_min_bodies": cm, "ms_tuned": t1, "ms_default": t0,
+                    "by": "eph_batch_autotune on 2 % of each member's steps (outside the timed region)"}
         barrier(pg, dev)
         torch.cuda.synchronize(dev)
         clocks = ClockSampler(local)
@@ -536,6 +542,7 @@ def run_b200_ensemble(args):
                            "systems": len(pls), "bodies": int(sum(sizes)), "body_steps_per_step": body_steps,
                            "parallelism": (f"members sharded over {world} GPUs (longest processing time first, no "
                                            f"exchange)") if world > 1 else "one persistent launch, 1 GPU",
+                           "autotune": tune,
                            "l2": "flushed between timed steps (256 MB write)"},
                 "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": bytes_io, "d2h_bytes_per_step": bytes_io},
                 "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",

@@ -63,6 +63,9 @@ SIGNATURES = [
     ("eph_batch_download", ctypes.c_int, [_VP, ctypes.POINTER(_D)]),
     ("eph_batch_set_stream", ctypes.c_int, [_VP, _VP]),
     ("eph_batch_set_precision", ctypes.c_int, [_VP, ctypes.c_int]),
+    ("eph_batch_set_coop_min", ctypes.c_int, [_VP, ctypes.c_int]),
+    ("eph_batch_autotune", ctypes.c_int, [_VP, _D, ctypes.POINTER(ctypes.c_int64), ctypes.c_double,
+                                           ctypes.POINTER(ctypes.c_int), _D, _D]),
     ("eph_batch_info", ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int64)]),
     ("eph_particles_create", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_VP)]),
     ("eph_particles_destroy", ctypes.c_int, [_VP]),

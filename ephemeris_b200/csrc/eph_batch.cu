@@ -45,7 +45,7 @@ namespace {
 
 constexpr int kBThreads = 256;          // threads per ensemble CTA
 constexpr int kCluster = 4;             // CTAs of a thread-block cluster that share one large system
-constexpr int kCoopMin = 96;            // bodies from which a system is shared by a cluster
+constexpr int kCoopMin = 96;            // default: bodies from which a system is shared by a cluster
 constexpr double kCB = 299792458.0;     // src/math/basic_math.h:10,18
 constexpr int kAcc = 9;                 // stored values per (body, stage): velocity dd (hi 3, lo 3), acceleration 3
 
@@ -679,6 +679,7 @@ struct eph_batch {
     cudaStream_t stream = nullptr;     // work stream (own_stream unless eph_batch_set_stream chose another)
     cudaStream_t own_stream = nullptr;
     int mixed = 0;                     // 1: EIH 1PN terms of the ensemble kernel in FP32 (eph_batch_set_precision)
+    int coop_min = kCoopMin;           // bodies from which a system is shared by a cluster (eph_batch_set_coop_min)
     std::mutex mu;
     char err[512] = {0};
     int n_sys = 0;
@@ -850,12 +851,12 @@ int eph_batch_integrate(eph_batch *b, const double *dt, const int64_t *n_step, d
     // the large systems (shared by a cluster) first, then the others; each group heaviest first, so the
     // last systems to start are short ones
     std::stable_sort(order.begin(), order.end(), [&](int a, int c) {
-        const bool ca = b->n_body[a] >= kCoopMin, cc = b->n_body[c] >= kCoopMin;
+        const bool ca = b->n_body[a] >= b->coop_min, cc = b->n_body[c] >= b->coop_min;
         if (ca != cc) return ca;
         return work[a] > work[c];
     });
     int n_coop = 0;
-    for (int s : order) n_coop += b->n_body[s] >= kCoopMin;
+    for (int s : order) n_coop += b->n_body[s] >= b->coop_min;
     if (!order.empty()) {
         BCK(cudaMemcpyAsync(b->d_sys, tab.data(), (size_t)n_sys * sizeof(BatchSys), cudaMemcpyHostToDevice, b->stream),
             "upload batch table");
@@ -939,6 +940,86 @@ int eph_batch_set_stream(eph_batch *b, void *stream) {
     std::lock_guard<std::mutex> lock(b->mu);
     if (!b->own_stream) b->own_stream = b->stream;
     b->stream = stream ? (cudaStream_t)stream : b->own_stream;
+    return EPH_OK;
+}
+
+int eph_batch_set_coop_min(eph_batch *b, int bodies) {
+    if (!b || bodies < 0) return bfail(b, EPH_ERR_ARG, "eph_batch_set_coop_min: bad arguments");
+    std::lock_guard<std::mutex> lock(b->mu);
+    b->coop_min = bodies == 0 ? kCoopMin : bodies;
+    return EPH_OK;
+}
+
+int eph_batch_autotune(eph_batch *b, const double *dt, const int64_t *n_step, double step_frac, int *coop_min,
+                       double *ms_tuned, double *ms_default) {
+    if (!b || !dt || !n_step || !(step_frac > 0 && step_frac <= 1) || !coop_min || !ms_tuned || !ms_default)
+        return bfail(b, EPH_ERR_ARG, "eph_batch_autotune: bad arguments");
+    int n_sys = 0;
+    size_t planes_doubles = 0;
+    {
+        std::lock_guard<std::mutex> lock(b->mu);
+        if (!b->n_sys) return bfail(b, EPH_ERR_STATE, "no batch uploaded");
+        n_sys = b->n_sys;
+        for (int s = 0; s < n_sys; ++s) planes_doubles = std::max(planes_doubles, b->off[s] + (size_t)EPH_NPLANES * b->n_body[s]);
+    }
+    BCK(cudaSetDevice(b->device), "cudaSetDevice");
+    // every trial runs the shared launch from the uploaded state with step counts scaled by step_frac (the
+    // members keep their relative durations); the systems of the per-system path are left out
+    std::vector<int64_t> steps(n_sys);
+    for (int s = 0; s < n_sys; ++s) {
+        const int64_t k = n_step[s] < 0 ? -n_step[s] : n_step[s];
+        const int64_t t = k == 0 ? 0 : std::max<int64_t>(1, (int64_t)std::llround((double)k * step_frac));
+        steps[s] = n_step[s] < 0 ? -t : t;
+    }
+    double *d_save = nullptr;
+    BCK(cudaMalloc(&d_save, planes_doubles * sizeof(double)), "cudaMalloc(autotune)");
+    BCK(cudaMemcpy(d_save, b->d_planes, planes_doubles * sizeof(double), cudaMemcpyDeviceToDevice), "save planes");
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    std::vector<double> th(n_sys), tl(n_sys);
+    const int saved_coop = b->coop_min;
+    for (int s = 0; s < n_sys; ++s) if (!b->point[s]) steps[s] = 0;   // ensemble members only
+    int rc = EPH_OK;
+    auto trial = [&](int cm, double *ms) {
+        double best = 1e300;
+        for (int rep = 0; rep < 2 && rc == EPH_OK; ++rep) {
+            b->coop_min = cm;
+            if (cudaMemcpy(b->d_planes, d_save, planes_doubles * sizeof(double), cudaMemcpyDeviceToDevice) != cudaSuccess) {
+                rc = bfail(b, EPH_ERR_CUDA, "restore planes");
+                break;
+            }
+            std::fill(th.begin(), th.end(), 0.0);
+            std::fill(tl.begin(), tl.end(), 0.0);
+            cudaEventRecord(e0, b->stream);
+            rc = eph_batch_integrate(b, dt, steps.data(), th.data(), tl.data());
+            cudaEventRecord(e1, b->stream);
+            float t = 0;
+            if (rc == EPH_OK && cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&t, e0, e1) == cudaSuccess)
+                best = std::min(best, (double)t);
+        }
+        *ms = best;
+    };
+    double t_def = 1e300, t_best = 1e300;
+    int best = saved_coop;
+    trial(saved_coop, &t_def);
+    t_best = t_def;
+    for (int cm : {48, 64, 128, 192, 1 << 30}) {
+        if (rc || cm == saved_coop) continue;
+        double t = 1e300;
+        trial(cm, &t);
+        if (rc == EPH_OK && t < t_best) { t_best = t; best = cm; }
+    }
+    b->coop_min = rc ? saved_coop : best;
+    if (cudaMemcpy(b->d_planes, d_save, planes_doubles * sizeof(double), cudaMemcpyDeviceToDevice) != cudaSuccess && !rc)
+        rc = bfail(b, EPH_ERR_CUDA, "restore planes");
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(d_save);
+    if (rc) return rc;
+    *coop_min = best;
+    *ms_tuned = t_best;
+    *ms_default = t_def;
     return EPH_OK;
 }
 

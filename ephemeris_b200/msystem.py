@@ -207,6 +207,22 @@ class Batch:
         self._check(self.lib.eph_batch_upload(self.h, len(pls), n, ptrs, mptrs), "batch upload")
         self.sizes = [p.shape[1] for p in pls]
 
+    def set_coop_min(self, bodies: int = 0):
+        """Bodies from which a system is shared by a 4-CTA cluster (0: the default)."""
+        self._check(self.lib.eph_batch_set_coop_min(self.h, bodies), "batch set_coop_min")
+
+    def autotune(self, dt, n_step, step_frac: float = 0.05):
+        """Time cluster-sharing thresholds on the uploaded batch; keeps the fastest.
+        Returns (coop_min, ms_tuned, ms_default)."""
+        k = len(self.sizes)
+        dts = np.ascontiguousarray(np.broadcast_to(np.asarray(dt, np.float64), (k,)))
+        ns = (ctypes.c_int64 * k)(*np.broadcast_to(np.asarray(n_step, np.int64), (k,)).tolist())
+        cm = ctypes.c_int()
+        t1, t0 = ctypes.c_double(), ctypes.c_double()
+        self._check(self.lib.eph_batch_autotune(self.h, _dptr(dts), ns, step_frac, ctypes.byref(cm), ctypes.byref(t1),
+                                                ctypes.byref(t0)), "batch autotune")
+        return cm.value, t1.value, t0.value
+
     def set_precision(self, mixed: bool):
         """FP32 EIH 1PN terms in the ensemble launch (True) or plain FP64 (False)."""
         self._check(self.lib.eph_batch_set_precision(self.h, 1 if mixed else 0), "batch set_precision")

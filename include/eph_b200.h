@@ -159,6 +159,15 @@ int eph_batch_set_stream(eph_batch *b, void *stream);
  * totals; state, separations, the Newtonian sums, the per-pair maxima and the RK12 combination stay FP64 /
  * double-double). Applies from the next integrate; systems on the single-system path are not affected. */
 int eph_batch_set_precision(eph_batch *b, int mode);
+/* Systems of at least `bodies` bodies are shared by the 4 CTAs of a thread-block cluster in the ensemble
+ * launch (0: the default, 96). */
+int eph_batch_set_coop_min(eph_batch *b, int bodies);
+/* Autotuner of the ensemble launch: times the uploaded batch's shared launch (step counts scaled by
+ * step_frac, so the members keep their relative durations; best of 2 from the uploaded state, which is
+ * restored) for several cluster-sharing thresholds, keeps the fastest (eph_batch_set_coop_min) and returns
+ * it with the times (ms) of the choice and of the threshold in force before. */
+int eph_batch_autotune(eph_batch *b, const double *dt, const int64_t *n_step, double step_frac, int *coop_min,
+                       double *ms_tuned, double *ms_default);
 /* Systems in the shared ensemble launch, and launches issued so far. */
 int eph_batch_info(const eph_batch *b, int32_t *n_ensemble, int64_t *launches);
 

@@ -60,3 +60,37 @@ def test_autotuned_shape_not_slower_and_correct(golden, name):
     assert d.autotune(dt, n_step=1, reps=1, use_cache=True)[:2] == (grid, per)
     for x in (c, h, d):
         x.close()
+
+
+def test_ensemble_autotune(tmp_path, oracle):
+    """The ensemble launch's cluster-sharing threshold, tuned on a 48-member ensemble (5 % of each member's
+    steps): never slower than the default, the uploaded state left as it was, and the members integrated
+    with the chosen threshold still within the parity tolerances."""
+    import os
+    from ephemeris_b200 import Batch, MSystem, synth
+    from oracle.pyoracle import Models as OModels
+    ens = synth.make_ensemble(48, seed=3011)
+    pls, mds, dts, ks = [], [], [], []
+    for s, (m, k) in enumerate(ens):
+        ms = MSystem(0)
+        assert ms.load(synth.write_system(m, os.path.join(str(tmp_path), f"s{s}")))
+        pls.append(ms.planes())
+        mds.append(ms.models())
+        dts.append(ms.delta_t)
+        ks.append(k)
+    b = Batch(0)
+    b.upload(pls, mds)
+    cm, t_tuned, t_default = b.autotune(dts, ks, step_frac=0.05)
+    print(f"ensemble: cluster threshold {cm} bodies, {t_tuned:.1f} ms tuned, {t_default:.1f} ms default")
+    assert t_tuned <= t_default
+    for out, pl in zip(b.download(), pls):
+        assert np.array_equal(out, pl)
+    b.integrate(dts, [3] * len(pls))
+    outs = b.download()
+    big = int(np.argmax([p.shape[1] for p in pls]))
+    for s in (0, big):
+        md = mds[s]
+        ref = oracle.integrate(pls[s], OModels(md.gp_nz, md.gp_nt, md.gp_coef, md.ring_ndisk, md.ring_param,
+                                               md.ring_disk), dts[s], 3)[0]
+        assert position_error(outs[s], ref) <= 1e-12
+    b.close()
