@@ -67,6 +67,7 @@ struct Own {
     double phi, nacc[3], C[9], GI[9], beta[3], beta2;
     double gacc[3], dacc[3], dtq[3], Egrad[3], mind, maxi;
     double sumA[13];
+    double Cs[9];                     // s (C_static + exJ2 terms) s^T of the stage (fixed during the fixed point)
     double fa[3];                     // f_s acceleration of the current stage
     double wnew[3], dw[3];            // stage angular velocity and its 2/3 increment (state update)
     // RK12 accumulators of stages k = 1..25 (index k-1)
@@ -74,17 +75,28 @@ struct Own {
     double acca[kStages][3], accw[kStages][3], acct[kStages][3];
 };
 
+// An extended body (geopotential and/or ring host): fixed for the launch, read by every field item
+struct HostInfo {
+    int E;                            // body index
+    short gp, ring;                   // model indices, or -1
+    unsigned char nz, nt, nd, pad;    // geopotential zonal / tesseral degree, ring disks
+};
+
 struct Scratch {
     double part[kWarps][16];          // per-warp partial sums
-    int split[kOwnMax + 1];           // warp groups of a pass-A re-sweep (equal split of the active bodies)
     int split_a0[kOwnMax + 1];        // warp groups of the first pass-A sweep (all owned bodies, weighted)
     int split_b[kOwnMax + 1];         // warp groups of the pass-B sweep (all owned bodies, weighted)
     int nw_b;                         // warps of the pass-B sweep (the last one sums host reactions meanwhile)
     double ext[kOwnMax][kMaxExt][3];  // other hosts' fields on the owned bodies (geopotential, or ring)
     double ext2[kOwnMax][kMaxExt][3]; // ring half of a host that has both models
     double react[kOwnMax][6];         // summed reactions of owned hosts
-    double rterm[kOwnMax][kRingPar][kRingDiskPar][3];   // per-disk ring terms before their ordered sum
-    int ring_e[kRingPar], n_ring_e, ring_dmax;
+    HostInfo host[kMaxExt];           // the extended bodies
+    unsigned char gp_list[kMaxExt], ring_list[kMaxExt];   // extended-body slots with a geopotential / a ring
+    int n_gp_e, n_ring_e, ring_dmax;
+    int ext_overlap;                  // geopotential items on warps [kWarps - kExtWarps, kWarps - 1) beside the pass-A sweeps
+    int ring_side;                    // ring items on the last warp beside the pass-A sweeps
+    int has_delayed;                  // the CTA owns a delayed tide
+    int nw_a;                         // warps of the pass-A sweeps (fields computed)
     double gp_x[kGpSmem][kGpX];                     // expanded tables of the first kGpSmem geopotential models
     double gp_rcp[EPH_GP_MAX_DEGREE + 2];          // 1/k of the degree recursion
     double rk_hi[EPH_RK12_NCOEF], rk_lo[EPH_RK12_NCOEF];   // a_kj (lane-divergent reads: shared, not constant, memory)
@@ -582,124 +594,63 @@ __device__ __forceinline__ void pair_a(const Own &o, const double *T, int ts, in
     acc[10] -= fk * M.z.x; acc[11] -= fk * M.z.y; acc[12] -= fk * M.z.z;
 }
 
-// UPDATE_HARMONICS followed by UPDATE_ANGULAR_VELOCITY (mass.impl:48-72) for owned body o on one warp:
-// lane q < 9 owns element q of the 3x3 matrices (column q/3, row q%3). Sets o.converged.
-__device__ void update_warp(Own &o, int lane, bool deform_only) {
-    const unsigned full = 0xffffffffu;
-    const int q = lane < 9 ? lane : 0, col = q / 3, row = q % 3;
-    const v3 w = ldv(o.w);
-    const double *wp = o.w;
-    const m3 f = fast9(o.s);
-    const double *fr = &f.x.x;   // column m at fr[3m]
-    // C = R^3/(2GM) (tidal sums + k2r (w^2/3 - w w^T)) + s (C_static + exJ2 terms) s^T
-    double Cq = o.sumA[4 + q];
-    if (col == row) Cq += dot(w, w) * o.k2r / 3;
-    Cq -= wp[col] * (o.k2r * wp[row]);
-    Cq = (o.R * o.R2 / (2 * o.GM)) * Cq;
-    auto mc0 = [&](int c, int r) {
-        double v = o.Cst[3 * c + r];
-        if (c == r) v += (c < 2) ? o.exJ2 / 2 : -o.exJ2;
-        return v;
-    };
-    // sa = s % mc0: column col, row row
-    const double saq = (fr[0 + row] * mc0(col, 0) + fr[3 + row] * mc0(col, 1)) + fr[6 + row] * mc0(col, 2);
-    const double sa0 = __shfl_sync(full, saq, 0 + row), sa1 = __shfl_sync(full, saq, 3 + row),
-                 sa2 = __shfl_sync(full, saq, 6 + row);
-    // toworld: column col = (s.x[col] sa.x + s.y[col] sa.y) + s.z[col] sa.z
-    const double mcq = (fr[0 + col] * sa0 + fr[3 + col] * sa1) + fr[6 + col] * sa2;
-    Cq = Cq + mcq;
-    const double GIq = ((-2.0) / 3 * o.R2) * (col == row ? Cq - o.A : Cq);
-    if (lane < 9) { o.C[q] = Cq; o.GI[q] = GIq; }
-    if (lane == 0) {
+// UPDATE_HARMONICS followed by UPDATE_ANGULAR_VELOCITY (mass.impl:48-72) for owned body o, on one thread,
+// from the pass-A sums in o.sumA. The first iteration of a stage (`first`) also sets the potential and the
+// Newtonian acceleration and rotates the static harmonics into the world frame once for the stage (they do
+// not depend on the angular velocity). Sets o.converged: the reference's convergence test, or an iteration
+// that reproduces w exactly (a fixed point: every further iteration of the reference's loop recomputes the
+// same sums, harmonics and w, so stopping leaves the identical state; needed for w = 0, where
+// 0 < 1e-18 * 0 never passes). Small and branch-light on purpose: it runs once per fixed-point iteration on
+// the critical path of the stage.
+__device__ void update_body(Own &o, bool first, bool deform_only) {
+    if (first) {
         o.phi = o.sumA[0];
         o.nacc[0] = o.sumA[1]; o.nacc[1] = o.sumA[2]; o.nacc[2] = o.sumA[3];
+        m3 mc = ldm(o.Cst);
+        mc.x.x += o.exJ2 / 2;
+        mc.y.y += o.exJ2 / 2;
+        mc.z.z -= o.exJ2;
+        stm(o.Cs, toworld(fast9(o.s), mc));
     }
-    __syncwarp();
-    if (deform_only) {
-        if (lane == 0) o.converged = 1;
-        __syncwarp();
-        return;
-    }
-    bool finite = true;
-    for (int c = 0; c < 3; ++c) finite = finite && dd_finite(o.GL[c]);
-    if (!finite) {   // UPDATE_ANGULAR_VELOCITY's else-branch: GL = GI w
-        if (lane == 0) {
-            v3 gl = mul(ldm(o.GI), w);
-            o.GL[0] = dd_make(gl.x); o.GL[1] = dd_make(gl.y); o.GL[2] = dd_make(gl.z);
-            o.gl_fixed = 1;
-            o.converged = 1;
-        }
-        __syncwarp();
-        return;
-    }
-    // w = GI^-1 GL (vec_t.h:443-454): adjoint element of this lane, determinant from column z of the adjoint
-    const m3 G = ldm(o.GI);
-    const double *g = &G.x.x;
-#define GE(c, r) g[3 * (c) + (r)]
-    auto adj = [&](int c, int r) {   // mat_t::adjoint, element (column c, row r)
-        const int c1 = (c + 1) % 3, c2 = (c + 2) % 3, r1 = (r + 1) % 3, r2 = (r + 2) % 3;
-        // cofactor of element (r, c) of the transpose convention used by mat_t::adjoint
-        return GE(r1, c1) * GE(r2, c2) - GE(r1, c2) * GE(r2, c1);
-    };
-    const double rdet = 1.0 / (adj(0, 2) * GE(2, 0) + adj(1, 2) * GE(2, 1) + adj(2, 2) * GE(2, 2));
-    const double invq = rdet * adj(col, row);
-#undef GE
-    const double i0 = __shfl_sync(full, invq, 0 + row), i1 = __shfl_sync(full, invq, 3 + row),
-                 i2 = __shfl_sync(full, invq, 6 + row);
-    const v3 gl = fast3(o.GL);
-    const double nw = (i0 * gl.x + i1 * gl.y) + i2 * gl.z;   // lanes 0..2: component `row`
-    const double n0 = __shfl_sync(full, nw, 0), n1 = __shfl_sync(full, nw, 1), n2 = __shfl_sync(full, nw, 2);
-    if (lane == 0) {
-        const v3 nv = mk(n0, n1, n2);
-        const v3 d = nv - w;
-        const bool same = nv.x == w.x && nv.y == w.y && nv.z == w.z;
-        stv(o.w, nv);
-        o.converged = (same || dot(d, d) < 1e-18 * dot(w, w)) ? 1 : 0;
-    }
-    __syncwarp();
-}
-
-// UPDATE_HARMONICS (mass.impl:48-61) from the pass-A sums of owned body o
-__device__ void update_harmonics(Own &o) {
-    o.phi = o.sumA[0];
-    o.nacc[0] = o.sumA[1]; o.nacc[1] = o.sumA[2]; o.nacc[2] = o.sumA[3];
+    const v3 w = ldv(o.w);
     m3 C = ldm(o.sumA + 4);
-    v3 w = ldv(o.w);
-    double w2 = dot(w, w);
-    C = add_diag(C, w2 * o.k2r / 3);
+    C = add_diag(C, dot(w, w) * o.k2r / 3);
     C = C - outer(o.k2r * w, w);
     C = (o.R * o.R2 / (2 * o.GM)) * C;
-    m3 fmis = fast9(o.s);
-    m3 mc = ldm(o.Cst);
-    mc.x.x += o.exJ2 / 2;
-    mc.y.y += o.exJ2 / 2;
-    mc.z.z -= o.exJ2;
-    mc = toworld(fmis, mc);
-    C = C + mc;
+    C = C + ldm(o.Cs);
     stm(o.C, C);
-    stm(o.GI, ((-2.0) / 3 * o.R2) * add_diag(C, -o.A));
-}
-
-// UPDATE_ANGULAR_VELOCITY (mass.impl:63-72); returns should_break
-__device__ bool update_angular_velocity(Own &o) {
+    const m3 GI = ((-2.0) / 3 * o.R2) * add_diag(C, -o.A);
+    stm(o.GI, GI);
+    if (deform_only) { o.converged = 1; return; }
     bool finite = true;
     for (int c = 0; c < 3; ++c) finite = finite && dd_finite(o.GL[c]);
-    m3 GI = ldm(o.GI);
-    v3 w = ldv(o.w);
-    if (finite) {
-        v3 nw = mul(inverse(GI), fast3(o.GL));
-        stv(o.w, nw);
-        v3 d = nw - w;
-        // An iteration that reproduces w exactly is a fixed point: every further iteration of the
-        // reference's loop recomputes the same sums, harmonics and w, so stopping here leaves the
-        // identical state. (Needed for w = 0, where the reference's test 0 < 1e-18*0 never passes.)
-        const bool same = nw.x == w.x && nw.y == w.y && nw.z == w.z;
-        return same || dot(d, d) < 1e-18 * dot(w, w);
+    if (!finite) {   // UPDATE_ANGULAR_VELOCITY's else-branch: G*L = GI w
+        const v3 gl = mul(GI, w);
+        o.GL[0] = dd_make(gl.x); o.GL[1] = dd_make(gl.y); o.GL[2] = dd_make(gl.z);
+        o.gl_fixed = 1;
+        o.converged = 1;
+        return;
     }
-    v3 gl = mul(GI, w);
-    o.GL[0] = dd_make(gl.x); o.GL[1] = dd_make(gl.y); o.GL[2] = dd_make(gl.z);
-    o.gl_fixed = 1;
-    return true;
+    const v3 nw = mul(inverse(GI), fast3(o.GL));
+    stv(o.w, nw);
+    const v3 d = nw - w;
+    const bool same = nw.x == w.x && nw.y == w.y && nw.z == w.z;
+    o.converged = (same || dot(d, d) < 1e-18 * dot(w, w)) ? 1 : 0;
+}
+
+// Sources of the pass-A tile rows. Only a delayed tide reads the velocities and tidal delay factors of the
+// bodies j: a CTA without one leaves those rows out of the copy (null source).
+__device__ __forceinline__ void tile_a_rows(const SysDev &S, const double *pub, bool need_v, const double *(&src)[TA_ROWS]) {
+    const int ld = S.ld;
+    for (int c = 0; c < 3; ++c) {
+        src[TA_R_HI + c] = pub + (PUB_R_HI + c) * ld;
+        src[TA_R_LO + c] = pub + (PUB_R_LO + c) * ld;
+        src[TA_V_HI + c] = need_v ? pub + (PUB_V_HI + c) * ld : nullptr;
+        src[TA_V_LO + c] = need_v ? pub + (PUB_V_LO + c) * ld : nullptr;
+    }
+    src[TA_GM] = pub + PUB_GM * ld;
+    src[TA_SR2] = S.cst + CST_SR2 * ld;
+    src[TA_TDF] = need_v ? S.cst + CST_TDF * ld : nullptr;
 }
 
 // Pair sums of pass A for the owned bodies in `mask` over all bodies j, by the first `nw` warps (tile
@@ -708,23 +659,31 @@ __device__ bool update_angular_velocity(Own &o) {
 // independent pair chains in flight per thread.
 __device__ bool sweep_a(const SysDev &S, Own *own, int nb, unsigned mask, int buf, Scratch &sc, TileState &ts,
                         double *tile, bool staged, int nw, const int *first_all) {
-    int act[kOwnMax], na = 0;
-    for (int b = 0; b < nb; ++b)
-        if ((mask >> b) & 1) act[na++] = b;
+    const int na = __popc(mask);
     if (na == 0) return true;
     const int ld = S.ld, n = S.n, T = S.tile;
     const double *pub = S.pub + (size_t)buf * PUB_NPLANES * ld;
-    // the first sweep of a stage covers every owned body (`first_all`, fixed per launch); a re-sweep covers
-    // the unconverged delayed tides, which all cost the same: equal split
-    const int *first = first_all;
-    if (!first) {
-        if (threadIdx.x == 0)
-            for (int a = 0; a <= na; ++a) sc.split[a] = (a * nw + na - 1) / na;
-        part_sync(nw * 32);
-        first = sc.split;
-    }
-    const Group g = group_of(first, na);
-    const Own &o = own[act[g.slot]];
+    // Warp groups: the first sweep of a stage covers every owned body (`first_all`, weighted, fixed per
+    // launch); a re-sweep covers the unconverged delayed tides, which all cost the same, so the nw warps are
+    // split equally: slot a owns warps [ceil(a nw / na), ceil((a + 1) nw / na)), i.e. warp w is in slot
+    // floor(w na / nw). Every thread works its group out itself: no shared list, no barrier.
+    auto bounds = [&](int slot, int &w0, int &w1) {
+        if (first_all) { w0 = first_all[slot]; w1 = first_all[slot + 1]; }
+        else { w0 = (slot * nw + na - 1) / na; w1 = ((slot + 1) * nw + na - 1) / na; }
+    };
+    auto body_of = [&](int slot) {   // the slot-th set bit of mask
+        unsigned m = mask;
+        for (int k = 0; k < slot; ++k) m &= m - 1;
+        return __ffs(m) - 1;
+    };
+    const int warp = threadIdx.x >> 5;
+    int my_slot;
+    if (first_all) { my_slot = 0; while (my_slot + 1 < na && warp >= first_all[my_slot + 1]) ++my_slot; }
+    else my_slot = (warp * na) / nw;
+    int gw0, gw1;
+    bounds(my_slot, gw0, gw1);
+    const Group g{my_slot, (warp - gw0) * 32 + (int)(threadIdx.x & 31), (gw1 - gw0) * 32};
+    const Own &o = own[body_of(my_slot)];
     double acc[13];
 #pragma unroll
     for (int c = 0; c < 13; ++c) acc[c] = 0;
@@ -732,11 +691,8 @@ __device__ bool sweep_a(const SysDev &S, Own *own, int nb, unsigned mask, int bu
     for (int j0 = 0; j0 < n; j0 += T) {
         const int cnt = min(T, n - j0);
         if (!staged) {
-            const double *src[TA_ROWS] = {pub + (PUB_R_HI + 0) * ld, pub + (PUB_R_HI + 1) * ld, pub + (PUB_R_HI + 2) * ld,
-                                          pub + (PUB_R_LO + 0) * ld, pub + (PUB_R_LO + 1) * ld, pub + (PUB_R_LO + 2) * ld,
-                                          pub + (PUB_V_HI + 0) * ld, pub + (PUB_V_HI + 1) * ld, pub + (PUB_V_HI + 2) * ld,
-                                          pub + (PUB_V_LO + 0) * ld, pub + (PUB_V_LO + 1) * ld, pub + (PUB_V_LO + 2) * ld,
-                                          pub + PUB_GM * ld, S.cst + CST_SR2 * ld, S.cst + CST_TDF * ld};
+            const double *src[TA_ROWS];
+            tile_a_rows(S, pub, sc.has_delayed, src);
             if (!load_tile(S, sc, ts, tile, T, src, TA_ROWS, j0, cnt, cnt, TA_ROWS)) return false;
         }
         const int self = o.idx - j0;
@@ -744,68 +700,97 @@ __device__ bool sweep_a(const SysDev &S, Own *own, int nb, unsigned mask, int bu
         for (int jj = g.tid; jj < cnt; jj += g.size)
             if (jj != self) pair_a(o, tile, T, jj, acc);
     }
-    __shared__ double red[kOwnMax][16];
-    group_reduce<13>(acc, first, na, nw, sc, red, 13);
-    for (int idx = threadIdx.x; idx < na * 13; idx += nw * 32) own[act[idx / 13]].sumA[idx % 13] = red[idx / 13][idx % 13];
+    // sums over each body's warp group: a warp reduce-scatter, then the group's warps in ascending order
+    {
+        const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        double v[16];
+#pragma unroll
+        for (int c = 0; c < 16; ++c) v[c] = c < 13 ? acc[c] : 0.0;
+        const double r = warp_reduce_scatter16(v, lane);
+        if ((lane & 1) == 0 && (lane >> 1) < 13) sc.part[w][lane >> 1] = r;
+    }
+    part_sync(nw * 32);
+    #pragma unroll 1
+    for (int idx = threadIdx.x; idx < na * 13; idx += nw * 32) {
+        const int slot = idx / 13, c = idx % 13;
+        int w0, w1;
+        bounds(slot, w0, w1);
+        double p[kWarps];   // every load first, then the sum in warp order
+#pragma unroll
+        for (int k = 0; k < kWarps; ++k) p[k] = w0 + k < w1 ? sc.part[w0 + k][c] : 0.0;
+        double sum = p[0];
+#pragma unroll
+        for (int k = 1; k < kWarps; ++k)
+            if (w0 + k < w1) sum += p[k];
+        own[body_of(slot)].sumA[c] = sum;
+    }
     part_sync(nw * 32);
     return true;
 }
 
-// Geopotential items (owned body b, host e) of ext_field_items on `nthr` threads (t = this thread's index),
-// G lanes per item: every item's lanes evaluate it together (gp_field_lanes on the expanded table in shared
-// memory) and the group's first lane stores it; a model beyond the shared-memory copies runs gp_field on
-// that lane alone.
+// Reactions of the field items before the CTA's ordered sum, per (host slot e, owned body b, model half):
+// six values (force, torque). They stay in the pass-A tile's free rows when those hold them, else they go
+// through the global table S.react.
+struct ReactStage {
+    double *smem;   // [n_ext][nb][2][6] in shared memory, or null
+    int nb;
+    __device__ __forceinline__ double *slot(const SysDev &S, int e, int b, int idx, int half) const {
+        return smem ? smem + ((size_t)(e * nb + b) * 2 + half) * 6 : S.react + (((size_t)e * S.ld + idx) * 2 + half) * 6;
+    }
+    __device__ __forceinline__ double get(const double *p) const { return smem ? *p : __ldcg(p); }
+};
+constexpr int kRingTerms = kOwnMax * kRingPar * kRingDiskPar * 3;   // per-disk ring terms, [b][h][d][3]
+#ifndef EPH_OVERLAP_ALL
+constexpr bool kOverlapAll = false;   // fields beside the sweeps in every CTA, not only the delayed tides'
+#else
+constexpr bool kOverlapAll = true;
+#endif
+
+// Geopotential items (owned body b, geopotential host slot e) on `nthr` threads (t = this
+// thread's index), G lanes per item: every item's lanes evaluate it together (gp_field_lanes on the
+// expanded table in shared memory, columns of the recursion split over the lanes) and the group's first
+// lane stores it; a model beyond the shared-memory copies runs gp_field on that lane alone.
 template <int G, typename Put>
-__device__ __forceinline__ void gp_items(const SysDev &S, const Own *own, int nb, const double *pub, Scratch &sc, int t,
-                                         int nthr, const Put &put) {
-    const int ld = S.ld, n_ext = S.n_ext;
+__device__ __forceinline__ void gp_items(const SysDev &S, const Own *own, int nb, const double *pub, const Scratch &sc,
+                                         int t, int nthr, const Put &put) {
+    const int ld = S.ld, ng = sc.n_gp_e;
     const int q = t & (G - 1), lane = threadIdx.x & 31;
     const unsigned mask = G == 1 ? (1u << lane) : (((1u << G) - 1u) << (lane & ~(G - 1)));
     #pragma unroll 1
-    for (int item = t / G; item < nb * n_ext; item += nthr / G) {
-        const int b = item / n_ext, e = item % n_ext;
+    for (int item = t / G; item < nb * ng; item += nthr / G) {
+        const int b = item / ng, e = sc.gp_list[item % ng];
         const Own &o = own[b];
-        const int E = __ldg(S.ext_body + e);
-        const int gpE = (int)__ldg(S.cst + CST_GP * ld + E);
-        const bool live = gpE >= 0 && E != o.idx;
+        const HostInfo h = sc.host[e];
+        const bool live = h.E != o.idx;
         v3 r = mk(0, 0, 0), an = mk(0, 0, 0);
         double GME = 0;
         if (live) {   // uniform over the group
+            const int E = h.E;
             r = mk(dd_diff(o.r[0].hi, o.r[0].lo, __ldcg(pub + PUB_R_HI * ld + E), __ldcg(pub + PUB_R_LO * ld + E)),
                    dd_diff(o.r[1].hi, o.r[1].lo, __ldcg(pub + (PUB_R_HI + 1) * ld + E), __ldcg(pub + (PUB_R_LO + 1) * ld + E)),
                    dd_diff(o.r[2].hi, o.r[2].lo, __ldcg(pub + (PUB_R_HI + 2) * ld + E), __ldcg(pub + (PUB_R_LO + 2) * ld + E)));
             GME = __ldcg(pub + PUB_GM * ld + E);
             const m3 f = ld9(pub + PUB_FRAME * ld, ld, E);
-            const int nz = __ldg(S.gp_nz + gpE), nt = __ldg(S.gp_nt + gpE);
             const double R = __ldg(S.cst + CST_R * ld + E);
             v3 al = mk(0, 0, 0);
-            if (gpE < kGpSmem) al = gp_field_lanes<G>(sc.gp_x[gpE], sc.gp_rcp, nz, nt, R, tolocal(f, r), q, mask);
-            else if (q == 0) al = gp_field(S.gp_coef + (size_t)gpE * EPH_GP_TABLE_SIZE, nz, nt, R, tolocal(f, r));
+            if (h.gp < kGpSmem) al = gp_field_lanes<G>(sc.gp_x[h.gp], sc.gp_rcp, h.nz, h.nt, R, tolocal(f, r), q, mask);
+            else if (q == 0) al = gp_field(S.gp_coef + (size_t)h.gp * EPH_GP_TABLE_SIZE, h.nz, h.nt, R, tolocal(f, r));
             an = toworld(f, al);
         }
         if (q == 0) put(0, b, e, o, r, an, GME, live);
     }
 }
 
-// Field of every geopotential / ring host at the owned bodies, once per (host, body): the force on the
-// owned body goes to sc.ext, the host's reaction to S.react (APPLY_NONPOINT_FORCE, mass.impl:127-130;
-// r = r_body - r_host as `mj.r - mi.r` with mi the host, mass.cpp:358-371). Runs on warps
-// [first_warp, kWarps): ring items on the last warp, geopotential items on the others, so no warp
-// diverges between the two models.
-__device__ void ext_field_items(const SysDev &S, const Own *own, int nb, int buf, Scratch &sc, int first_warp) {
-    const int ld = S.ld, n_ext = S.n_ext;
-    const double *pub = S.pub + (size_t)buf * PUB_NPLANES * ld;
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const bool single = first_warp == kWarps - 1;               // one warp runs both halves
-    const bool ring_warp = single || w == kWarps - 1;
-    const bool gp_warp = single || w < kWarps - 1;
-    auto body_sep = [&](const Own &o, int E) {   // r = r_body - r_host (mass.cpp:184,198)
-        return mk(dd_diff(o.r[0].hi, o.r[0].lo, __ldcg(pub + PUB_R_HI * ld + E), __ldcg(pub + PUB_R_LO * ld + E)),
-                  dd_diff(o.r[1].hi, o.r[1].lo, __ldcg(pub + (PUB_R_HI + 1) * ld + E), __ldcg(pub + (PUB_R_LO + 1) * ld + E)),
-                  dd_diff(o.r[2].hi, o.r[2].lo, __ldcg(pub + (PUB_R_HI + 2) * ld + E), __ldcg(pub + (PUB_R_LO + 2) * ld + E)));
-    };
-    // geopotential half: force on the body into sc.ext, reaction on the host into react slot 0
-    auto put = [&](int half, int b, int e, const Own &o, v3 r, v3 an, double GME, bool live) {
+// Fields of the geopotential / ring hosts at the owned bodies, once per (host, body) item: the force on
+// the owned body goes to sc.ext (geopotential) / sc.ext2 (ring), the host's reaction to the staging `st`
+// (APPLY_NONPOINT_FORCE, mass.impl:127-130; r = r_body - r_host as `mj.r - mi.r` with mi the host,
+// mass.cpp:358-371). Only the halves of a host's models are written: the readers skip the half a host does
+// not have.
+struct FieldPut {
+    const SysDev &S;
+    Scratch &sc;
+    const ReactStage &st;
+    __device__ void operator()(int half, int b, int e, const Own &o, v3 r, v3 an, double GME, bool live) const {
         v3 add3 = mk(0, 0, 0), da = mk(0, 0, 0), dt = mk(0, 0, 0);
         if (live) {
             add3 = GME * an;
@@ -814,89 +799,93 @@ __device__ void ext_field_items(const SysDev &S, const Own *own, int nb, int buf
         }
         double (*dst)[kMaxExt][3] = half ? sc.ext2 : sc.ext;
         dst[b][e][0] = add3.x; dst[b][e][1] = add3.y; dst[b][e][2] = add3.z;
-        double *rc = S.react + (((size_t)e * ld + o.idx) * 2 + half) * 6;
+        double *rc = st.slot(S, e, b, o.idx, half);
         rc[0] = da.x; rc[1] = da.y; rc[2] = da.z; rc[3] = dt.x; rc[4] = dt.y; rc[5] = dt.z;
-    };
-    if (gp_warp) {
-        // one (body, host) item per lane when there are many, one per group of 8 lanes (one column of the
-        // recursion per lane) when they are few enough to run in one round that way
-        const int nthr = single ? 32 : (kWarps - 1 - first_warp) * 32;
-        const int t = single ? lane : threadIdx.x - first_warp * 32;
-        if (nb * n_ext * 8 <= nthr) gp_items<8>(S, own, nb, pub, sc, t, nthr, put);
-        else gp_items<1>(S, own, nb, pub, sc, t, nthr, put);
     }
-    if (!ring_warp) return;
-    // ring half (react slot 1, sc.ext2). With few hosts and disks each lane takes one (body, host, disk)
-    // term and the terms are added in disk order afterwards (ring.impl:2122-2192); otherwise one lane
-    // per (body, host) runs ring::sum whole.
-    if (lane == 0) {
-        int nr = 0, dmax = 0;
-        for (int e = 0; e < n_ext; ++e) {
-            const int E = S.ext_body[e];
-            const int rg = (int)S.cst[CST_RING * ld + E];
-            if (rg < 0) continue;
-            if (nr < kRingPar) sc.ring_e[nr] = e;
-            ++nr;
-            dmax = max(dmax, S.ring_nd[rg]);
-        }
-        sc.n_ring_e = nr;
-        sc.ring_dmax = dmax;
-    }
-    __syncwarp();
+};
+
+__device__ __forceinline__ v3 body_sep(const Own &o, const double *pub, int ld, int E) {   // r_body - r_host (mass.cpp:184,198)
+    return mk(dd_diff(o.r[0].hi, o.r[0].lo, __ldcg(pub + PUB_R_HI * ld + E), __ldcg(pub + PUB_R_LO * ld + E)),
+              dd_diff(o.r[1].hi, o.r[1].lo, __ldcg(pub + (PUB_R_HI + 1) * ld + E), __ldcg(pub + (PUB_R_LO + 1) * ld + E)),
+              dd_diff(o.r[2].hi, o.r[2].lo, __ldcg(pub + (PUB_R_HI + 2) * ld + E), __ldcg(pub + (PUB_R_LO + 2) * ld + E)));
+}
+
+// Geopotential items on warps [w_lo, w_hi), as many lanes per item as one round over the items allows
+// (more lanes: shorter chains).
+__device__ void ext_gp(const SysDev &S, const Own *own, int nb, int buf, Scratch &sc, const ReactStage &st, int w_lo,
+                       int w_hi) {
+    if (sc.n_gp_e == 0) return;
+    const double *pub = S.pub + (size_t)buf * PUB_NPLANES * S.ld;
+    const FieldPut put{S, sc, st};
+    const int nthr = (w_hi - w_lo) * 32, t = threadIdx.x - w_lo * 32;
+    const int items = nb * sc.n_gp_e;
+    if (items * 8 <= nthr) gp_items<8>(S, own, nb, pub, sc, t, nthr, put);
+    else if (items * 4 <= nthr) gp_items<4>(S, own, nb, pub, sc, t, nthr, put);
+    else if (items * 2 <= nthr) gp_items<2>(S, own, nb, pub, sc, t, nthr, put);
+    else gp_items<1>(S, own, nb, pub, sc, t, nthr, put);
+}
+
+// Ring items on the calling warp. With few hosts and disks each lane takes one (body, host, disk) term and
+// the terms are added in disk order afterwards (ring.impl:2122-2192, staged in `rterm`); otherwise one lane
+// per (body, host) runs ring::sum whole.
+__device__ void ext_ring(const SysDev &S, const Own *own, int nb, int buf, Scratch &sc, const ReactStage &st,
+                         double *rterm) {
+    const int ld = S.ld, lane = threadIdx.x & 31;
+    const double *pub = S.pub + (size_t)buf * PUB_NPLANES * ld;
+    const FieldPut put{S, sc, st};
     const int nr = sc.n_ring_e, dmax = sc.ring_dmax;
-    const bool parallel = nr <= kRingPar && dmax <= kRingDiskPar;
-    #pragma unroll 1
-    for (int item = lane; item < nb * n_ext; item += 32) {   // zero the slots of hosts without a ring
-        const int b = item / n_ext, e = item % n_ext;
-        const int E = __ldg(S.ext_body + e);
-        if ((int)__ldg(S.cst + CST_RING * ld + E) >= 0 && parallel) continue;
-        const Own &o = own[b];
-        const int rg = (int)__ldg(S.cst + CST_RING * ld + E);
-        const bool live = rg >= 0 && E != o.idx;
-        v3 r = mk(0, 0, 0), an = mk(0, 0, 0);
-        double GME = 0;
-        if (live) {   // sequential fallback
-            r = body_sep(o, E);
-            GME = __ldcg(pub + PUB_GM * ld + E);
-            m3 f = ld9(pub + PUB_RFRAME * ld, ld, E);
-            an = toworld(f, ring_sum(S.ring_disk + (size_t)rg * EPH_RING_MAX_DISKS * 3, __ldg(S.ring_nd + rg),
-                                     __ldg(S.cst + CST_R * ld + E), tolocal(f, r)));
+    if (nr == 0) return;
+    if (nr > kRingPar || dmax > kRingDiskPar) {
+        #pragma unroll 1
+        for (int item = lane; item < nb * nr; item += 32) {
+            const int b = item / nr, e = sc.ring_list[item % nr];
+            const Own &o = own[b];
+            const HostInfo h = sc.host[e];
+            const bool live = h.E != o.idx;
+            v3 r = mk(0, 0, 0), an = mk(0, 0, 0);
+            double GME = 0;
+            if (live) {
+                r = body_sep(o, pub, ld, h.E);
+                GME = __ldcg(pub + PUB_GM * ld + h.E);
+                m3 f = ld9(pub + PUB_RFRAME * ld, ld, h.E);
+                an = toworld(f, ring_sum(S.ring_disk + (size_t)h.ring * EPH_RING_MAX_DISKS * 3, h.nd,
+                                         __ldg(S.cst + CST_R * ld + h.E), tolocal(f, r)));
+            }
+            put(1, b, e, o, r, an, GME, live);
         }
-        put(1, b, e, o, r, an, GME, live);
+        return;
     }
-    if (!parallel) return;
     #pragma unroll 1
     for (int item = lane; item < nb * nr * dmax; item += 32) {
-        const int b = item / (nr * dmax), h = (item / dmax) % nr, d = item % dmax;
+        const int b = item / (nr * dmax), hh = (item / dmax) % nr, d = item % dmax;
         const Own &o = own[b];
-        const int e = sc.ring_e[h], E = __ldg(S.ext_body + e);
-        const int rg = (int)__ldg(S.cst + CST_RING * ld + E);
+        const HostInfo h = sc.host[sc.ring_list[hh]];
         v3 t = mk(0, 0, 0);
-        if (E != o.idx && d < __ldg(S.ring_nd + rg)) {
-            m3 f = ld9(pub + PUB_RFRAME * ld, ld, E);
-            const RingGeom g = ring_geom(tolocal(f, body_sep(o, E)));
-            t = ring_disk_term(S.ring_disk + ((size_t)rg * EPH_RING_MAX_DISKS + d) * 3, __ldg(S.cst + CST_R * ld + E), g);
+        if (h.E != o.idx && d < h.nd) {
+            m3 f = ld9(pub + PUB_RFRAME * ld, ld, h.E);
+            const RingGeom g = ring_geom(tolocal(f, body_sep(o, pub, ld, h.E)));
+            t = ring_disk_term(S.ring_disk + ((size_t)h.ring * EPH_RING_MAX_DISKS + d) * 3, __ldg(S.cst + CST_R * ld + h.E), g);
         }
-        sc.rterm[b][h][d][0] = t.x; sc.rterm[b][h][d][1] = t.y; sc.rterm[b][h][d][2] = t.z;
+        double *rt = rterm + ((b * kRingPar + hh) * kRingDiskPar + d) * 3;
+        rt[0] = t.x; rt[1] = t.y; rt[2] = t.z;
     }
     __syncwarp();
     #pragma unroll 1
     for (int item = lane; item < nb * nr; item += 32) {
-        const int b = item / nr, h = item % nr;
+        const int b = item / nr, hh = item % nr, e = sc.ring_list[hh];
         const Own &o = own[b];
-        const int e = sc.ring_e[h], E = __ldg(S.ext_body + e);
-        const int rg = (int)__ldg(S.cst + CST_RING * ld + E);
-        const bool live = E != o.idx;
+        const HostInfo h = sc.host[e];
+        const bool live = h.E != o.idx;
         v3 r = mk(0, 0, 0), an = mk(0, 0, 0);
         double GME = 0;
         if (live) {
-            r = body_sep(o, E);
-            GME = __ldcg(pub + PUB_GM * ld + E);
-            m3 f = ld9(pub + PUB_RFRAME * ld, ld, E);
+            r = body_sep(o, pub, ld, h.E);
+            GME = __ldcg(pub + PUB_GM * ld + h.E);
+            m3 f = ld9(pub + PUB_RFRAME * ld, ld, h.E);
             const RingGeom g = ring_geom(tolocal(f, r));
             v3 ret = mk(0, 0, 0);
-            const int nd = __ldg(S.ring_nd + rg);
-            for (int d = 0; d < nd; ++d) ret += mk(sc.rterm[b][h][d][0], sc.rterm[b][h][d][1], sc.rterm[b][h][d][2]);
+            const double *rt = rterm + (b * kRingPar + hh) * kRingDiskPar * 3;
+            for (int d = 0; d < h.nd; ++d) ret += mk(rt[3 * d], rt[3 * d + 1], rt[3 * d + 2]);
             if (g.psign) ret.z = -ret.z;
             an = toworld(f, ret);
         }
@@ -904,21 +893,22 @@ __device__ void ext_field_items(const SysDev &S, const Own *own, int nb, int buf
     }
 }
 
-// ext_field_items, then this CTA's share of every host's reaction: the sum over its owned bodies (in
+// This CTA's share of every host's reaction on threads [t0, t0 + nthr): the sum over its owned bodies (in
 // ownership order) of both model halves, S.react_cta[host][CTA][6], so that a host's owner adds one value per
 // CTA in pass B instead of one per body.
-__device__ void ext_fields(const SysDev &S, const Own *own, int nb, int buf, Scratch &sc, int first_warp) {
-    ext_field_items(S, own, nb, buf, sc, first_warp);
-    const int nthr = (kWarps - first_warp) * 32;
-    asm volatile("bar.sync 2, %0;" ::"r"(nthr) : "memory");
+__device__ void ext_react(const SysDev &S, const Own *own, int nb, const Scratch &sc, const ReactStage &st, int t0,
+                          int nthr) {
     const int ld = S.ld;
     #pragma unroll 1
-    for (int item = threadIdx.x - first_warp * 32; item < S.n_ext * 6; item += nthr) {
+    for (int item = threadIdx.x - t0; item < S.n_ext * 6; item += nthr) {
         const int e = item / 6, c = item % 6;
+        const HostInfo h = sc.host[e];
         double sum = 0;
         for (int b = 0; b < nb; ++b) {
-            const double *rc = S.react + ((size_t)e * ld + own[b].idx) * 12;
-            sum += __ldcg(rc + c) + __ldcg(rc + 6 + c);
+            const double *rc = st.slot(S, e, b, own[b].idx, 0);   // halves at rc[0..5] and rc[6..11]
+            const double g = h.gp >= 0 ? st.get(rc + c) : 0.0;
+            const double r = h.ring >= 0 ? st.get(rc + 6 + c) : 0.0;
+            sum += g + r;
         }
         S.react_cta[((size_t)e * ld + blockIdx.x) * 6 + c] = sum;
     }
@@ -955,22 +945,27 @@ __device__ bool pass_a(const SysDev &S, Own *own, int nb, int buf, bool deform_o
     if (threadIdx.x < nb) { own[threadIdx.x].converged = 0; own[threadIdx.x].gl_fixed = 0; }
     const bool one_tile = S.n <= S.tile;
     if (one_tile) {
-        const double *src[TA_ROWS] = {pub + (PUB_R_HI + 0) * ld, pub + (PUB_R_HI + 1) * ld, pub + (PUB_R_HI + 2) * ld,
-                                      pub + (PUB_R_LO + 0) * ld, pub + (PUB_R_LO + 1) * ld, pub + (PUB_R_LO + 2) * ld,
-                                      pub + (PUB_V_HI + 0) * ld, pub + (PUB_V_HI + 1) * ld, pub + (PUB_V_HI + 2) * ld,
-                                      pub + (PUB_V_LO + 0) * ld, pub + (PUB_V_LO + 1) * ld, pub + (PUB_V_LO + 2) * ld,
-                                      pub + PUB_GM * ld, S.cst + CST_SR2 * ld, S.cst + CST_TDF * ld};
+        const double *src[TA_ROWS];
+        tile_a_rows(S, pub, sc.has_delayed, src);
         if (!load_tile(S, sc, ts, tile, S.tile, src, TA_ROWS, 0, S.n, S.n, TA_ROWS)) return false;
     } else {
         __syncthreads();
     }
-    // The extended bodies' fields do not depend on the angular velocity: they run on the last kExtWarps warps
-    // alongside every pass-A sweep and angular-velocity update of the stage (one tile only: streaming tiles
-    // needs every warp, and the fields then run after the first sweep).
-    const bool ext_overlap = !deform_only && S.n_ext > 0 && one_tile;
+    // The extended bodies' fields do not depend on the angular velocity, so they run beside the pass-A sweeps
+    // where the CTA can spare the warps (one tile only: streaming tiles needs every warp): the ring items on
+    // the last warp in every CTA, and in a CTA that iterates a delayed tide (sc.ext_overlap) the geopotential
+    // items on the kExtWarps - 1 warps before it. The rest runs on every warp after the sweeps. The per-disk
+    // ring terms and, when they fit, the reactions are staged in the rows of the pass-A tile that pass A
+    // does not use.
+    const bool fields = !deform_only && S.n_ext > 0;
+    const bool ring_side = fields && sc.ring_side;
+    const bool gp_side = fields && sc.ext_overlap;
     const int max_iter = deform_only ? 1 : 4;   // MAX_ANGULAR_VELOCITY_ITER (mass.impl:74)
-    const int nw = ext_overlap ? kWarps - kExtWarps : kWarps;
-    if ((threadIdx.x >> 5) < nw) {
+    const int nw = deform_only ? kWarps : sc.nw_a;
+    double *xa = tile + (size_t)TA_ROWS * S.tile;
+    const ReactStage st{kRingTerms + nb * S.n_ext * 12 <= (kTileRows - TA_ROWS) * S.tile ? xa + kRingTerms : nullptr, nb};
+    const int warp = threadIdx.x >> 5;
+    if (warp < nw) {
         #pragma unroll 1
         for (int it = 0; it < max_iter; ++it) {
             unsigned mask = 0;
@@ -981,28 +976,31 @@ __device__ bool pass_a(const SysDev &S, Own *own, int nb, int buf, bool deform_o
             if (!sweep_a(S, own, nb, mask, buf, sc, ts, tile, one_tile, nw, it == 0 ? sc.split_a0 : nullptr)) return false;
             if (S.timers && threadIdx.x == 0) sc.t_phase[PH_A_COUNT] += 1;
             mark(S, sc, PH_A_SWEEP);   // thread 0 sits in a sweep warp
-            // harmonics and angular velocity of the owned bodies: warp b updates body b
-            {
-                const int wb = threadIdx.x >> 5;
-                if (wb < nb && !own[wb].converged) update_warp(own[wb], threadIdx.x & 31, deform_only);
-            }
+            // harmonics and angular velocity of the owned bodies: lane 0 of warp b updates body b
+            if (warp < nb && (threadIdx.x & 31) == 0 && !own[warp].converged) update_body(own[warp], it == 0, deform_only);
             part_sync(nw * 32);
             mark(S, sc, PH_A_UPDATE);
-            if (!deform_only && it == 0 && S.n_ext > 0 && !one_tile) {
-                __syncthreads();   // nw == kWarps here
-                ext_fields(S, own, nb, buf, sc, 0);
-                __syncthreads();
-                mark(S, sc, PH_B_EXT);
-            }
             int all = 1;
             for (int b = 0; b < nb; ++b) all &= own[b].converged;
             if (all) break;
         }
+    } else if (ring_side && warp == kWarps - 1) {
+        ext_ring(S, own, nb, buf, sc, st, xa);
     } else {
-        ext_fields(S, own, nb, buf, sc, kWarps - kExtWarps);
+        ext_gp(S, own, nb, buf, sc, st, kWarps - kExtWarps, ring_side ? kWarps - 1 : kWarps);
     }
     __syncthreads();
-    mark(S, sc, PH_B_EXT);   // the wait for the field warps beyond the sweeps and updates
+    if (fields) {
+        const bool ring_after = !ring_side && sc.n_ring_e > 0;
+        if (!gp_side || ring_after) {
+            if (ring_after && warp == kWarps - 1) ext_ring(S, own, nb, buf, sc, st, xa);
+            else if (!gp_side) ext_gp(S, own, nb, buf, sc, st, 0, ring_after ? kWarps - 1 : kWarps);
+            __syncthreads();
+        }
+        ext_react(S, own, nb, sc, st, 0, blockDim.x);
+        __syncthreads();
+    }
+    mark(S, sc, PH_B_EXT);   // the fields beyond the sweeps and updates
     if (deform_only) return true;
     // PREPARE_RELATIVITY (mass.impl:76-80) and the pass-A outputs other CTAs read in pass B
     const double c2 = kC * kC;
@@ -1236,9 +1234,10 @@ __device__ bool pass_b(const SysDev &S, Own *own, int nb, int buf, Scratch &sc, 
         Own &ob = own[b];
         v3 da = ldv(ob.dacc);
         v3 tq = ldv(ob.dtq);
-        for (int e = 0; e < n_ext; ++e) {
-            da += mk(sc.ext[b][e][0], sc.ext[b][e][1], sc.ext[b][e][2]);
-            da += mk(sc.ext2[b][e][0], sc.ext2[b][e][1], sc.ext2[b][e][2]);
+        for (int e = 0; e < n_ext; ++e) {   // the halves of the host's models (a missing half adds zero)
+            const HostInfo h = sc.host[e];
+            da += h.gp >= 0 ? mk(sc.ext[b][e][0], sc.ext[b][e][1], sc.ext[b][e][2]) : mk(0, 0, 0);
+            da += h.ring >= 0 ? mk(sc.ext2[b][e][0], sc.ext2[b][e][1], sc.ext2[b][e][2]) : mk(0, 0, 0);
         }
         if (ob.ext_slot >= 0) {
             da += mk(sc.react[b][0], sc.react[b][1], sc.react[b][2]);
@@ -1267,10 +1266,100 @@ __device__ bool pass_b(const SysDev &S, Own *own, int nb, int buf, Scratch &sc, 
 }
 
 // ------------------------------------------------------------------ RK12 stage combination and update
+// Adds a_{k,s} f_s into the accumulators of stages k = k_lo..k_hi (RungeKutta.impl:148-162 in incremental
+// form: every accumulator receives its terms in ascending s, the reference's summation order); 12
+// components per stage, the velocity as double-double.
+__device__ void combine_stage(Own *own, int nb, int s, int k_lo, int k_hi, const Scratch &sc) {
+    const int nk = k_hi - k_lo + 1;
+    if (nk <= 0) return;
+    #pragma unroll 1
+    for (int item = threadIdx.x; item < nb * nk * 12; item += blockDim.x) {
+        const int b = item / (nk * 12);
+        const int rem = item % (nk * 12);
+        const int k = k_lo + rem / 12;
+        const int c = rem % 12;
+        Own &o = own[b];
+        const int ci = k * (k - 1) / 2 + s;
+        const dd a = dd{sc.rk_hi[ci], sc.rk_lo[ci]};
+        const bool nz = a.hi != 0;
+        if (c < 3) {
+            dd cur = (s == 0) ? dd_make(0) : o.accv[k - 1][c];
+            if (nz) cur = dd_add(cur, dd_mul(a, o.v[c]));
+            o.accv[k - 1][c] = cur;
+        } else {
+            const double fa = dd_val(a);
+            double *slot;
+            double f;
+            if (c < 6) { slot = &o.acca[k - 1][c - 3]; f = o.fa[c - 3]; }
+            else if (c < 9) { slot = &o.accw[k - 1][c - 6]; f = o.w[c - 6]; }
+            else { slot = &o.acct[k - 1][c - 9]; f = o.dtq[c - 9]; }
+            double cur = (s == 0) ? 0.0 : *slot;
+            if (nz) cur = __dadd_rn(cur, __dmul_rn(fa, f));
+            *slot = cur;
+        }
+    }
+}
+
+// Frame of stage k = s + 1 for body o on its warp (RungeKutta.impl:170-186): s = s0, then s += R % fast(s)
+// for the passes R0 (w - dw), R1 (w + dw) and, at the last stage, R2 (Egrad), element (col, row) =
+// sum_m R[m][row] * s[col][m]; the increment matrices depend only on w, dw and Egrad, so every lane builds
+// the one of its pass (lanes 9p .. 9p+8 apply pass p) at the same time and the passes are applied in
+// order. At the last stage mass::orthogonalize follows (mass.h:147-150).
+__device__ void rotate_frame(Own &o, int lane, int s, double dt) {
+    const int k = s + 1;
+    const double dt_k = c_dtk[k];
+    if (lane < 9) o.s[lane] = o.s0[lane];
+    __syncwarp();
+    const v3 wv = ldv(o.wnew), dwv = ldv(o.dw), eg = ldv(o.Egrad);
+    // A body that does not rotate (w, its stage change and Egrad all exactly zero) has zero rotation
+    // increments R (rotation_matrix of a zero vector), so its frame keeps s0 exactly: skip the passes.
+    const bool still = wv.x == 0 && wv.y == 0 && wv.z == 0 && dwv.x == 0 && dwv.y == 0 && dwv.z == 0 &&
+                       (k != kStages || (eg.x == 0 && eg.y == 0 && eg.z == 0));
+    const int npass = still ? 0 : (k == kStages ? 3 : 2);
+    if (npass) {
+        const int my = min(lane / 9, 2);
+        // one evaluation per lane on its pass's arguments (one copy of the code, no divergence)
+        const v3 axis = my == 0 ? wv - dwv : my == 1 ? wv + dwv : eg;
+        const m3 R = rotation_matrix(axis, my < 2 ? dt * dt_k / 2 : 1.0 / 72);
+        const double *Rr = &R.x.x;   // R column m at Rr[3m]
+        const int q = lane - 9 * my, col = q / 3, row = q % 3;
+        #pragma unroll 1
+        for (int pass = 0; pass < npass; ++pass) {
+            const bool mine = my == pass && q < 9;
+            double add = 0;
+            if (mine) {
+                const v3 sc = fast3(o.s + 3 * col);
+                add = (Rr[0 + row] * sc.x + Rr[3 + row] * sc.y) + Rr[6 + row] * sc.z;
+            }
+            __syncwarp();
+            if (mine) o.s[q] = dd_add(o.s[q], dd_make(add));
+            __syncwarp();
+        }
+    }
+    if (k == kStages) {
+        // s += 0.5 fmis % (1 - fmis^T % fmis)
+        double add = 0;
+        if (lane < 9) {
+            const int col = lane / 3, row = lane % 3;
+            const m3 f = fast9(o.s);
+            // column `col` of (1 - f^T f): entries m = (1 if m == col) - dot(f[m], f[col])
+            const v3 fc = (col == 0) ? f.x : (col == 1) ? f.y : f.z;
+            const double o0 = (col == 0 ? 1.0 : 0.0) - dot(f.x, fc);
+            const double o1 = (col == 1 ? 1.0 : 0.0) - dot(f.y, fc);
+            const double o2 = (col == 2 ? 1.0 : 0.0) - dot(f.z, fc);
+            const double *fr = &f.x.x;
+            add = (0.5 * fr[0 + row] * o0 + 0.5 * fr[3 + row] * o1) + 0.5 * fr[6 + row] * o2;
+        }
+        __syncwarp();
+        if (lane < 9) o.s[lane] = dd_add(o.s[lane], dd_make(add));
+        __syncwarp();
+    }
+}
+
 // Called with f_s known for all owned bodies (s = 0..24). Adds a_{k,s} f_s into the accumulators of
-// stages k = s+1..25 (RungeKutta.impl:148-162 in incremental form), then forms the state of stage s+1
-// (RungeKutta.impl:164-186) and publishes it to buffer `buf_out`. The state update of body b runs on
-// warp b: lanes 0..2 take the vector components, lanes 0..8 the 3x3 frame elements.
+// stages k = s+1..25, then forms the state of stage s+1 (RungeKutta.impl:164-186) and publishes it to
+// buffer `buf_out`. The state update of body b runs on warp b: lanes 0..2 take the vector components,
+// lanes 0..8 the 3x3 frame elements.
 __device__ void rk_stage(const SysDev &S, Own *own, int nb, int s, long long i_step, const StepParams &P,
                          int buf_out, const Scratch &sc) {
     const double dt = P.dt;
@@ -1308,34 +1397,7 @@ __device__ void rk_stage(const SysDev &S, Own *own, int nb, int s, long long i_s
         }
     }
     __syncthreads();
-    // incremental combination: 12 components (velocity as double-double) per later stage
-    const int nk = kStages - s;   // stages s+1..25
-    #pragma unroll 1
-    for (int item = threadIdx.x; item < nb * nk * 12; item += blockDim.x) {
-        const int b = item / (nk * 12);
-        const int rem = item % (nk * 12);
-        const int k = s + 1 + rem / 12;
-        const int c = rem % 12;
-        Own &o = own[b];
-        const int ci = k * (k - 1) / 2 + s;
-        const dd a = dd{sc.rk_hi[ci], sc.rk_lo[ci]};
-        const bool nz = a.hi != 0;
-        if (c < 3) {
-            dd cur = (s == 0) ? dd_make(0) : o.accv[k - 1][c];
-            if (nz) cur = dd_add(cur, dd_mul(a, o.v[c]));
-            o.accv[k - 1][c] = cur;
-        } else {
-            const double fa = dd_val(a);
-            double *slot;
-            double f;
-            if (c < 6) { slot = &o.acca[k - 1][c - 3]; f = o.fa[c - 3]; }
-            else if (c < 9) { slot = &o.accw[k - 1][c - 6]; f = o.w[c - 6]; }
-            else { slot = &o.acct[k - 1][c - 9]; f = o.dtq[c - 9]; }
-            double cur = (s == 0) ? 0.0 : *slot;
-            if (nz) cur = __dadd_rn(cur, __dmul_rn(fa, f));
-            *slot = cur;
-        }
-    }
+    combine_stage(own, nb, s, s + 1, kStages, sc);
     __syncthreads();
     // state of stage k = s+1, warp b for body b
     const int k = s + 1;
@@ -1355,58 +1417,9 @@ __device__ void rk_stage(const SysDev &S, Own *own, int nb, int s, long long i_s
             o.dw[c] = (2.0 / 3) * (wc - o.w0[c]);
         }
         __syncwarp();
-        if (lane < 9) o.s[lane] = o.s0[lane];
-        __syncwarp();
-        const v3 wv = ldv(o.wnew), dwv = ldv(o.dw), eg = ldv(o.Egrad);
-        // A body that does not rotate (w, its stage change and Egrad all exactly zero) has zero rotation
-        // increments R (rotation_matrix of a zero vector), so its frame keeps s0 exactly: skip the passes.
-        const bool still = wv.x == 0 && wv.y == 0 && wv.z == 0 && dwv.x == 0 && dwv.y == 0 && dwv.z == 0 &&
-                           (k != kStages || (eg.x == 0 && eg.y == 0 && eg.z == 0));
-        // s += R % fast(s), element (col, row) = sum_m R[m][row] * s[col][m], for the passes R0 (w - dw),
-        // R1 (w + dw) and, at the last stage, R2 (Egrad). The increment matrices depend only on w, dw and
-        // Egrad, so every lane builds the one of its pass (lanes 9p .. 9p+8 apply pass p) at the same time;
-        // the passes are then applied in order.
-        const int npass = still ? 0 : (k == kStages ? 3 : 2);
-        if (npass) {
-            const int my = min(lane / 9, 2);
-            const m3 R = my == 0 ? rotation_matrix(wv - dwv, dt * dt_k / 2)
-                       : my == 1 ? rotation_matrix(wv + dwv, dt * dt_k / 2)
-                                 : rotation_matrix(eg, 1.0 / 72);
-            const double *Rr = &R.x.x;   // R column m at Rr[3m]
-            const int q = lane - 9 * my, col = q / 3, row = q % 3;
-            #pragma unroll 1
-            for (int pass = 0; pass < npass; ++pass) {
-                const bool mine = my == pass && q < 9;
-                double add = 0;
-                if (mine) {
-                    const v3 sc = fast3(o.s + 3 * col);
-                    add = (Rr[0 + row] * sc.x + Rr[3 + row] * sc.y) + Rr[6 + row] * sc.z;
-                }
-                __syncwarp();
-                if (mine) o.s[q] = dd_add(o.s[q], dd_make(add));
-                __syncwarp();
-            }
-        }
-        if (k == kStages) {
-            // mass::orthogonalize (mass.h:147-150): s += 0.5 fmis % (1 - fmis^T % fmis)
-            double add = 0;
-            if (lane < 9) {
-                const int col = lane / 3, row = lane % 3;
-                const m3 f = fast9(o.s);
-                // column `col` of (1 - f^T f): entries m = (1 if m == col) - dot(f[m], f[col])
-                const v3 fc = (col == 0) ? f.x : (col == 1) ? f.y : f.z;
-                const double o0 = (col == 0 ? 1.0 : 0.0) - dot(f.x, fc);
-                const double o1 = (col == 1 ? 1.0 : 0.0) - dot(f.y, fc);
-                const double o2 = (col == 2 ? 1.0 : 0.0) - dot(f.z, fc);
-                const double *fr = &f.x.x;
-                add = (0.5 * fr[0 + row] * o0 + 0.5 * fr[3 + row] * o1) + 0.5 * fr[6 + row] * o2;
-            }
-            __syncwarp();
-            if (lane < 9) o.s[lane] = dd_add(o.s[lane], dd_make(add));
-            __syncwarp();
-        }
+        rotate_frame(o, lane, s, dt);
         if (lane == 0) {
-            stv(o.w, wv);
+            stv(o.w, ldv(o.wnew));
             o.GM = o.GM0 + o.dGM * t;
             o.exJ2 = o.dJ2 * t;
         }
@@ -1436,7 +1449,32 @@ __global__ void __launch_bounds__(kThreads, 1) step_kernel(SysDev S, StepParams 
     for (int k = 0; k < min(S.n_gp, kGpSmem); ++k)
         gp_expand(S.gp_coef + (size_t)k * EPH_GP_TABLE_SIZE, S.gp_nz[k], S.gp_nt[k], sc.gp_x[k], threadIdx.x, blockDim.x);
     for (int q = threadIdx.x; q < EPH_GP_MAX_DEGREE + 2; q += blockDim.x) sc.gp_rcp[q] = GP_RCP[q];
+    for (int e = threadIdx.x; e < S.n_ext; e += blockDim.x) {   // the extended bodies and their models
+        HostInfo h;
+        h.E = S.ext_body[e];
+        const int gp = (int)S.cst[CST_GP * S.ld + h.E], rg = (int)S.cst[CST_RING * S.ld + h.E];
+        h.gp = (short)gp;
+        h.ring = (short)rg;
+        h.nz = gp >= 0 ? (unsigned char)S.gp_nz[gp] : 0;
+        h.nt = gp >= 0 ? (unsigned char)S.gp_nt[gp] : 0;
+        h.nd = rg >= 0 ? (unsigned char)S.ring_nd[rg] : 0;
+        h.pad = 0;
+        sc.host[e] = h;
+    }
     mbar_init(sc);
+    if (threadIdx.x == 0) {
+        int ng = 0, nr = 0, dmax = 0;
+        for (int e = 0; e < S.n_ext; ++e) {
+            if (sc.host[e].gp >= 0) sc.gp_list[ng++] = (unsigned char)e;
+            if (sc.host[e].ring >= 0) {
+                sc.ring_list[nr++] = (unsigned char)e;
+                dmax = max(dmax, (int)sc.host[e].nd);
+            }
+        }
+        sc.n_gp_e = ng;
+        sc.n_ring_e = nr;
+        sc.ring_dmax = dmax;
+    }
     int nb = 0;
     for (int b = 0; b < kOwnMax; ++b) {
         int id = S.own_list[blockIdx.x * kOwnMax + b];
@@ -1454,11 +1492,18 @@ __global__ void __launch_bounds__(kThreads, 1) step_kernel(SysDev S, StepParams 
     if (threadIdx.x < nb) publish_body(S, own[threadIdx.x], 0);
     if (threadIdx.x == 32) {
         // warp groups of the sweeps over all owned bodies: delayed-tide pass-A pairs cost ~8x a point pair,
-        // full-class pass-B pairs ~2x; the first pass-A sweep leaves kExtWarps warps to the extended bodies
+        // full-class pass-B pairs ~2x. During the pass-A sweeps the last warp evaluates the ring items, and
+        // in a CTA that iterates a delayed tide the kExtWarps - 1 warps before it the geopotential items.
         int wt[kOwnMax];
-        const bool ext_overlap = P.mode != MODE_DEFORM && S.n_ext > 0 && S.n <= S.tile;
+        bool delayed = false;
+        for (int b = 0; b < nb; ++b) delayed |= own[b].kind == 2;
+        sc.has_delayed = delayed;
+        const bool side = P.mode != MODE_DEFORM && S.n_ext > 0 && S.n <= S.tile;
+        sc.ext_overlap = side && (delayed || kOverlapAll);
+        sc.ring_side = side && sc.n_ring_e > 0;
+        sc.nw_a = sc.ext_overlap ? kWarps - kExtWarps : sc.ring_side ? kWarps - 1 : kWarps;
         for (int b = 0; b < nb; ++b) wt[b] = own[b].kind == 2 ? 8 : 1;
-        split_warps(wt, nb, ext_overlap ? kWarps - kExtWarps : kWarps, sc.split_a0);
+        split_warps(wt, nb, P.mode == MODE_DEFORM ? kWarps : sc.nw_a, sc.split_a0);
         for (int b = 0; b < nb; ++b) wt[b] = own[b].full ? 2 : 1;
         // a CTA that owns geopotential / ring hosts sums their reactions on its last warp during the
         // pass-B sweep (one tile only: streaming tiles needs every warp for the copies)
