@@ -107,6 +107,14 @@ struct Scratch {
     int flag, pad;
 };
 
+// Shared memory: the owned bodies, the scratch, then the staging tile of kTileRows rows. The tile's row stride
+// kTileW is fixed at compile time (the widest tile that fits), so that every tile access is a fixed offset
+// from the body's column; a system of n <= kTileW bodies is staged in one tile, a larger one in chunks.
+constexpr int kMaxSmem = 227 * 1024 - 4096;   // the 227 KB per-CTA maximum less room for static arrays
+constexpr size_t kFixedSmem = ((sizeof(Own) * kOwnMax + sizeof(Scratch) + 127) / 128) * 128;
+constexpr int kTileW = (int)((kMaxSmem - kFixedSmem) / (kTileRows * sizeof(double))) / kPad * kPad;
+static_assert(kTileW >= 512, "the staging tile must hold a 512-body system in one piece");
+
 // ------------------------------------------------------------------ small helpers
 __device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
     unsigned v;
@@ -186,16 +194,9 @@ __device__ __forceinline__ void mbar_init(Scratch &sc) {
 // Copy `rows` planes (row r from src[r] + j0, `count` bodies rounded up to kPad; rows from `tail_from` on
 // `count_tail` bodies; a null src[r] keeps tile row r as it is) into tile rows of `stride` doubles. Every
 // thread waits for completion (bounded). Returns false on timeout.
-struct NoSideWork {
-    __device__ void operator()() const {}
-};
-
-// `side()` runs on every thread after the copies are issued and before the wait: work whose own loads can
-// overlap the copies.
-template <typename Side = NoSideWork>
 __device__ bool load_tile(const SysDev &S, Scratch &sc, TileState &ts, double *tile, int stride,
-                          const double *const *src, int rows, int j0, int count, int count_tail, int tail_from,
-                          const Side &side = Side()) {
+                                       const double *const *src, int rows, int j0, int count, int count_tail,
+                                       int tail_from) {
     __syncthreads();   // the previous sweep's reads of the tile are done
     const int cpad = (count + kPad - 1) / kPad * kPad;
     const int tpad = (count_tail + kPad - 1) / kPad * kPad;
@@ -219,7 +220,6 @@ __device__ bool load_tile(const SysDev &S, Scratch &sc, TileState &ts, double *t
                 : "memory");
         }
     }
-    side();
     const unsigned parity = ts.parity;
     ts.parity ^= 1u;
     unsigned long long t0 = 0;
@@ -541,7 +541,8 @@ __device__ void publish_body_warp(const SysDev &S, const Own &o, int buf, int la
 // ------------------------------------------------------------------ pass A: deform_by + angular velocity
 // One ordered pair (i = owned body o, j from the tile) of DAMPED_TIDAL_DEFORMATION_MATRIX / _NDELAY /
 // _NK2 (mass.impl:1-46), accumulated into acc = {phi, naccel[3], C[9]}.
-__device__ __forceinline__ void pair_a(const Own &o, const double *T, int ts, int j, double acc[13]) {
+__device__ __forceinline__ void pair_a(const Own &o, const double *T, int j, double acc[13]) {
+    constexpr int ts = kTileW;
     v3 r = mk(sep_diff(T[(TA_R_HI + 0) * ts + j], T[(TA_R_LO + 0) * ts + j], o.r[0].hi, o.r[0].lo),
               sep_diff(T[(TA_R_HI + 1) * ts + j], T[(TA_R_LO + 1) * ts + j], o.r[1].hi, o.r[1].lo),
               sep_diff(T[(TA_R_HI + 2) * ts + j], T[(TA_R_LO + 2) * ts + j], o.r[2].hi, o.r[2].lo));
@@ -693,12 +694,12 @@ __device__ bool sweep_a(const SysDev &S, Own *own, int nb, unsigned mask, int bu
         if (!staged) {
             const double *src[TA_ROWS];
             tile_a_rows(S, pub, sc.has_delayed, src);
-            if (!load_tile(S, sc, ts, tile, T, src, TA_ROWS, j0, cnt, cnt, TA_ROWS)) return false;
+            if (!load_tile(S, sc, ts, tile, kTileW, src, TA_ROWS, j0, cnt, cnt, TA_ROWS)) return false;
         }
         const int self = o.idx - j0;
 #pragma unroll 1
         for (int jj = g.tid; jj < cnt; jj += g.size)
-            if (jj != self) pair_a(o, tile, T, jj, acc);
+            if (jj != self) pair_a(o, tile, jj, acc);
     }
     // sums over each body's warp group: a warp reduce-scatter, then the group's warps in ascending order
     {
@@ -947,7 +948,7 @@ __device__ bool pass_a(const SysDev &S, Own *own, int nb, int buf, bool deform_o
     if (one_tile) {
         const double *src[TA_ROWS];
         tile_a_rows(S, pub, sc.has_delayed, src);
-        if (!load_tile(S, sc, ts, tile, S.tile, src, TA_ROWS, 0, S.n, S.n, TA_ROWS)) return false;
+        if (!load_tile(S, sc, ts, tile, kTileW, src, TA_ROWS, 0, S.n, S.n, TA_ROWS)) return false;
     } else {
         __syncthreads();
     }
@@ -962,8 +963,8 @@ __device__ bool pass_a(const SysDev &S, Own *own, int nb, int buf, bool deform_o
     const bool gp_side = fields && sc.ext_overlap;
     const int max_iter = deform_only ? 1 : 4;   // MAX_ANGULAR_VELOCITY_ITER (mass.impl:74)
     const int nw = deform_only ? kWarps : sc.nw_a;
-    double *xa = tile + (size_t)TA_ROWS * S.tile;
-    const ReactStage st{kRingTerms + nb * S.n_ext * 12 <= (kTileRows - TA_ROWS) * S.tile ? xa + kRingTerms : nullptr, nb};
+    double *xa = tile + (size_t)TA_ROWS * kTileW;
+    const ReactStage st{kRingTerms + nb * S.n_ext * 12 <= (kTileRows - TA_ROWS) * kTileW ? xa + kRingTerms : nullptr, nb};
     const int warp = threadIdx.x >> 5;
     if (warp < nw) {
         #pragma unroll 1
@@ -984,19 +985,25 @@ __device__ bool pass_a(const SysDev &S, Own *own, int nb, int buf, bool deform_o
             for (int b = 0; b < nb; ++b) all &= own[b].converged;
             if (all) break;
         }
-    } else if (ring_side && warp == kWarps - 1) {
-        ext_ring(S, own, nb, buf, sc, st, xa);
-    } else {
-        ext_gp(S, own, nb, buf, sc, st, kWarps - kExtWarps, ring_side ? kWarps - 1 : kWarps);
     }
-    __syncthreads();
-    if (fields) {
-        const bool ring_after = !ring_side && sc.n_ring_e > 0;
-        if (!gp_side || ring_after) {
-            if (ring_after && warp == kWarps - 1) ext_ring(S, own, nb, buf, sc, st, xa);
-            else if (!gp_side) ext_gp(S, own, nb, buf, sc, st, 0, ring_after ? kWarps - 1 : kWarps);
+    // the field items: phase 0 beside the sweeps (warps >= nw), phase 1 after them on every warp; one call
+    // site per evaluator, so that each is compiled once
+    const bool ring_after = fields && !ring_side && sc.n_ring_e > 0;
+    #pragma unroll 1
+    for (int ph = 0; ph < 2; ++ph) {
+        if (ph == 1) {
             __syncthreads();
+            if (!fields || (gp_side && !ring_after)) break;
         }
+        const bool ring_here = warp == kWarps - 1 && (ph == 0 ? ring_side : ring_after);
+        const bool gp_here = ph == 0 ? (gp_side && warp >= nw) : !gp_side;
+        const int gp_lo = ph == 0 ? kWarps - kExtWarps : 0;
+        const int gp_hi = (ph == 0 ? ring_side : ring_after) ? kWarps - 1 : kWarps;
+        if (ring_here) ext_ring(S, own, nb, buf, sc, st, xa);
+        else if (gp_here && warp >= gp_lo && warp < gp_hi) ext_gp(S, own, nb, buf, sc, st, gp_lo, gp_hi);
+    }
+    if (fields) {
+        __syncthreads();
         ext_react(S, own, nb, sc, st, 0, blockDim.x);
         __syncthreads();
     }
@@ -1052,7 +1059,8 @@ __device__ __forceinline__ void track(Extremes &x, double m, double tp_dg, doubl
 // IF / JF: body i / body j of the full class. For a point-like body the deformation matrix, G*L,
 // luminosity and receptance are all zero, so the terms they multiply are exactly zero and skipped.
 template <bool IF, bool JF>
-__device__ __forceinline__ void pair_b(const Own &o, const double *T, int ts, int j, double acc[9], Extremes &x) {
+__device__ __forceinline__ void pair_b(const Own &o, const double *T, int j, double acc[9], Extremes &x) {
+    constexpr int ts = kTileW;
     v3 r = mk(sep_diff(T[(TB_R_HI + 0) * ts + j], T[(TB_R_LO + 0) * ts + j], o.r[0].hi, o.r[0].lo),
               sep_diff(T[(TB_R_HI + 1) * ts + j], T[(TB_R_LO + 1) * ts + j], o.r[1].hi, o.r[1].lo),
               sep_diff(T[(TB_R_HI + 2) * ts + j], T[(TB_R_LO + 2) * ts + j], o.r[2].hi, o.r[2].lo));
@@ -1107,11 +1115,11 @@ __device__ __forceinline__ void pair_b(const Own &o, const double *T, int ts, in
 }
 
 template <bool IF, bool JF>
-__device__ __forceinline__ void sweep_b_range(const Own &o, const double *tile, int T, int lo, int hi, int self,
+__device__ __forceinline__ void sweep_b_range(const Own &o, const double *tile, int lo, int hi, int self,
                                               const Group &g, double acc[9], Extremes &x) {
 #pragma unroll 1
     for (int jj = lo + g.tid; jj < hi; jj += g.size)
-        if (jj != self) pair_b<IF, JF>(o, tile, T, jj, acc, x);
+        if (jj != self) pair_b<IF, JF>(o, tile, jj, acc, x);
 }
 
 __device__ bool pass_b(const SysDev &S, Own *own, int nb, int buf, Scratch &sc, TileState &ts, double *tile) {
@@ -1146,15 +1154,15 @@ __device__ bool pass_b(const SysDev &S, Own *own, int nb, int buf, Scratch &sc, 
             aux + (AUX_CPOT + 3) * ld, aux + (AUX_CPOT + 4) * ld, aux + (AUX_CPOT + 5) * ld,
             aux + (AUX_CPOT + 6) * ld, aux + (AUX_CPOT + 7) * ld, aux + (AUX_CPOT + 8) * ld,
             cst + CST_R2 * ld, cst + CST_LUM * ld};
-        if (!load_tile(S, sc, ts, tile, T, src, TB_ROWS, j0, cnt, cnt_full, kTileBFullRows)) return false;
+        if (!load_tile(S, sc, ts, tile, kTileW, src, TB_ROWS, j0, cnt, cnt_full, kTileBFullRows)) return false;
         const int self = o.idx - j0;
         if (!sweeper) continue;
         if (o.full) {
-            sweep_b_range<true, true>(o, tile, T, 0, cnt_full, self, g, acc, x);
-            sweep_b_range<true, false>(o, tile, T, cnt_full, cnt, self, g, acc, x);
+            sweep_b_range<true, true>(o, tile, 0, cnt_full, self, g, acc, x);
+            sweep_b_range<true, false>(o, tile, cnt_full, cnt, self, g, acc, x);
         } else {
-            sweep_b_range<false, true>(o, tile, T, 0, cnt_full, self, g, acc, x);
-            sweep_b_range<false, false>(o, tile, T, cnt_full, cnt, self, g, acc, x);
+            sweep_b_range<false, true>(o, tile, 0, cnt_full, self, g, acc, x);
+            sweep_b_range<false, false>(o, tile, cnt_full, cnt, self, g, acc, x);
         }
     }
     __shared__ double red[kOwnMax][16];
@@ -1568,13 +1576,12 @@ __global__ void __launch_bounds__(kThreads, 1) step_kernel(SysDev S, StepParams 
 // ------------------------------------------------------------------ host launcher
 namespace eph {
 
-size_t step_fixed_smem_bytes() { return ((sizeof(Own) * kOwnMax + sizeof(Scratch) + 127) / 128) * 128; }
-size_t step_smem_bytes(int tile) { return step_fixed_smem_bytes() + (size_t)kTileRows * tile * sizeof(double); }
-// dynamic shared memory limit: the 227 KB per-CTA maximum less room for the kernel's static arrays
-constexpr int kMaxSmem = 227 * 1024 - 4096;
+size_t step_fixed_smem_bytes() { return kFixedSmem; }
+// the tile is always allocated at its full stride; `tile` (bodies staged per chunk) does not change the size
+size_t step_smem_bytes(int tile) { (void)tile; return kFixedSmem + (size_t)kTileRows * kTileW * sizeof(double); }
 
-// Largest tile (bodies, multiple of kPad) that fits next to the fixed shared-memory state.
-int max_tile() { return (int)((kMaxSmem - step_fixed_smem_bytes()) / (kTileRows * sizeof(double))) / kPad * kPad; }
+// Largest tile (bodies, multiple of kPad): the tile's stride.
+int max_tile() { return kTileW; }
 
 // Per-device "constants uploaded" flags. Contexts (each under its own lock) and the fixed-scratch entry
 // point (under its own) may set a device up at the same time: one mutex of its own orders the uploads.
