@@ -741,11 +741,6 @@ struct ReactStage {
     __device__ __forceinline__ double get(const double *p) const { return smem ? *p : __ldcg(p); }
 };
 constexpr int kRingTerms = kOwnMax * kRingPar * kRingDiskPar * 3;   // per-disk ring terms, [b][h][d][3]
-#ifndef EPH_OVERLAP_ALL
-constexpr bool kOverlapAll = false;   // fields beside the sweeps in every CTA, not only the delayed tides'
-#else
-constexpr bool kOverlapAll = true;
-#endif
 
 // Geopotential items (owned body b, geopotential host slot e) on `nthr` threads (t = this
 // thread's index), G lanes per item: every item's lanes evaluate it together (gp_field_lanes on the
@@ -953,11 +948,10 @@ __device__ bool pass_a(const SysDev &S, Own *own, int nb, int buf, bool deform_o
         __syncthreads();
     }
     // The extended bodies' fields do not depend on the angular velocity, so they run beside the pass-A sweeps
-    // where the CTA can spare the warps (one tile only: streaming tiles needs every warp): the ring items on
-    // the last warp in every CTA, and in a CTA that iterates a delayed tide (sc.ext_overlap) the geopotential
-    // items on the kExtWarps - 1 warps before it. The rest runs on every warp after the sweeps. The per-disk
-    // ring terms and, when they fit, the reactions are staged in the rows of the pass-A tile that pass A
-    // does not use.
+    // (one tile only: streaming tiles needs every warp): the ring items on the last warp, the geopotential
+    // items (sc.ext_overlap) on the kExtWarps - 1 warps before it. With streaming tiles they run on every warp
+    // after the sweeps. The per-disk ring terms and, when they fit, the reactions are staged in the rows of
+    // the pass-A tile that pass A does not use.
     const bool fields = !deform_only && S.n_ext > 0;
     const bool ring_side = fields && sc.ring_side;
     const bool gp_side = fields && sc.ext_overlap;
@@ -1500,14 +1494,14 @@ __global__ void __launch_bounds__(kThreads, 1) step_kernel(SysDev S, StepParams 
     if (threadIdx.x < nb) publish_body(S, own[threadIdx.x], 0);
     if (threadIdx.x == 32) {
         // warp groups of the sweeps over all owned bodies: delayed-tide pass-A pairs cost ~8x a point pair,
-        // full-class pass-B pairs ~2x. During the pass-A sweeps the last warp evaluates the ring items, and
-        // in a CTA that iterates a delayed tide the kExtWarps - 1 warps before it the geopotential items.
+        // full-class pass-B pairs ~2x. During the pass-A sweeps the last warp evaluates the ring items and
+        // the kExtWarps - 1 warps before it the geopotential items.
         int wt[kOwnMax];
         bool delayed = false;
         for (int b = 0; b < nb; ++b) delayed |= own[b].kind == 2;
         sc.has_delayed = delayed;
         const bool side = P.mode != MODE_DEFORM && S.n_ext > 0 && S.n <= S.tile;
-        sc.ext_overlap = side && (delayed || kOverlapAll);
+        sc.ext_overlap = side;
         sc.ring_side = side && sc.n_ring_e > 0;
         sc.nw_a = sc.ext_overlap ? kWarps - kExtWarps : sc.ring_side ? kWarps - 1 : kWarps;
         for (int b = 0; b < nb; ++b) wt[b] = own[b].kind == 2 ? 8 : 1;
