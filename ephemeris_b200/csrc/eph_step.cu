@@ -82,6 +82,16 @@ struct HostInfo {
     unsigned char nz, nt, nd, pad;    // geopotential zonal / tesseral degree, ring disks
 };
 
+// A body whose fields this CTA evaluates: one of its own, or one handed over by a CTA that owns a delayed
+// tide (`slot` < 0). Filled at the start of every pass A.
+constexpr int kForeignMax = 4;                   // bodies one CTA evaluates the fields of for other CTAs
+constexpr int kFieldMax = kOwnMax + kForeignMax;
+struct FieldBody {
+    int idx, slot;                    // body index; owned-body slot, or -1
+    dd r[3];                          // stage position
+    double GM;
+};
+
 struct Scratch {
     double part[kWarps][16];          // per-warp partial sums
     int split_a0[kOwnMax + 1];        // warp groups of the first pass-A sweep (all owned bodies, weighted)
@@ -96,6 +106,10 @@ struct Scratch {
     int ext_overlap;                  // geopotential items on warps [kWarps - kExtWarps, kWarps - 1) beside the pass-A sweeps
     int ring_side;                    // ring items on the last warp beside the pass-A sweeps
     int has_delayed;                  // the CTA owns a delayed tide
+    int fields_away;                  // this CTA's field items are evaluated by other CTAs (hand-off)
+    int n_foreign, foreign[kForeignMax];   // bodies of other CTAs whose field items this CTA evaluates
+    int nfb;                          // field bodies of the stage: nb owned ones, then the foreign ones
+    FieldBody fb[kFieldMax];
     int nw_a;                         // warps of the pass-A sweeps (fields computed)
     double gp_x[kGpSmem][kGpX];                     // expanded tables of the first kGpSmem geopotential models
     double gp_rcp[EPH_GP_MAX_DEGREE + 2];          // 1/k of the degree recursion
@@ -740,14 +754,14 @@ struct ReactStage {
     }
     __device__ __forceinline__ double get(const double *p) const { return smem ? *p : __ldcg(p); }
 };
-constexpr int kRingTerms = kOwnMax * kRingPar * kRingDiskPar * 3;   // per-disk ring terms, [b][h][d][3]
+constexpr int kRingTerms = kFieldMax * kRingPar * kRingDiskPar * 3;   // per-disk ring terms, [f][h][d][3]
 
-// Geopotential items (owned body b, geopotential host slot e) on `nthr` threads (t = this
+// Geopotential items (field body b, geopotential host slot e) on `nthr` threads (t = this
 // thread's index), G lanes per item: every item's lanes evaluate it together (gp_field_lanes on the
 // expanded table in shared memory, columns of the recursion split over the lanes) and the group's first
 // lane stores it; a model beyond the shared-memory copies runs gp_field on that lane alone.
 template <int G, typename Put>
-__device__ __forceinline__ void gp_items(const SysDev &S, const Own *own, int nb, const double *pub, const Scratch &sc,
+__device__ __forceinline__ void gp_items(const SysDev &S, const FieldBody *fb, int nb, const double *pub, const Scratch &sc,
                                          int t, int nthr, const Put &put) {
     const int ld = S.ld, ng = sc.n_gp_e;
     const int q = t & (G - 1), lane = threadIdx.x & 31;
@@ -755,7 +769,7 @@ __device__ __forceinline__ void gp_items(const SysDev &S, const Own *own, int nb
     #pragma unroll 1
     for (int item = t / G; item < nb * ng; item += nthr / G) {
         const int b = item / ng, e = sc.gp_list[item % ng];
-        const Own &o = own[b];
+        const FieldBody &o = fb[b];
         const HostInfo h = sc.host[e];
         const bool live = h.E != o.idx;
         v3 r = mk(0, 0, 0), an = mk(0, 0, 0);
@@ -777,30 +791,33 @@ __device__ __forceinline__ void gp_items(const SysDev &S, const Own *own, int nb
     }
 }
 
-// Fields of the geopotential / ring hosts at the owned bodies, once per (host, body) item: the force on
-// the owned body goes to sc.ext (geopotential) / sc.ext2 (ring), the host's reaction to the staging `st`
-// (APPLY_NONPOINT_FORCE, mass.impl:127-130; r = r_body - r_host as `mj.r - mi.r` with mi the host,
-// mass.cpp:358-371). Only the halves of a host's models are written: the readers skip the half a host does
-// not have.
+// Fields of the geopotential / ring hosts at the field bodies, once per (host, body) item: the force on an
+// owned body goes to sc.ext (geopotential) / sc.ext2 (ring), on a body of another CTA to the global
+// table S.react (its slots [host][body][half][0..2], read by the owner in pass B), the host's reaction to
+// the staging `st` (APPLY_NONPOINT_FORCE, mass.impl:127-130; r = r_body - r_host as `mj.r - mi.r` with mi
+// the host, mass.cpp:358-371). Only the halves of a host's models are written: the readers skip the half a
+// host does not have.
 struct FieldPut {
     const SysDev &S;
     Scratch &sc;
     const ReactStage &st;
-    __device__ void operator()(int half, int b, int e, const Own &o, v3 r, v3 an, double GME, bool live) const {
+    __device__ void operator()(int half, int b, int e, const FieldBody &o, v3 r, v3 an, double GME, bool live) const {
         v3 add3 = mk(0, 0, 0), da = mk(0, 0, 0), dt = mk(0, 0, 0);
         if (live) {
             add3 = GME * an;
             da = -(o.GM * an);
             dt = -(o.GM * cross(r, an));
         }
-        double (*dst)[kMaxExt][3] = half ? sc.ext2 : sc.ext;
-        dst[b][e][0] = add3.x; dst[b][e][1] = add3.y; dst[b][e][2] = add3.z;
+        double *f;
+        if (o.slot >= 0) f = (half ? sc.ext2 : sc.ext)[o.slot][e];
+        else f = S.react + (((size_t)e * S.ld + o.idx) * 2 + half) * 6;
+        f[0] = add3.x; f[1] = add3.y; f[2] = add3.z;
         double *rc = st.slot(S, e, b, o.idx, half);
         rc[0] = da.x; rc[1] = da.y; rc[2] = da.z; rc[3] = dt.x; rc[4] = dt.y; rc[5] = dt.z;
     }
 };
 
-__device__ __forceinline__ v3 body_sep(const Own &o, const double *pub, int ld, int E) {   // r_body - r_host (mass.cpp:184,198)
+__device__ __forceinline__ v3 body_sep(const FieldBody &o, const double *pub, int ld, int E) {   // r_body - r_host (mass.cpp:184,198)
     return mk(dd_diff(o.r[0].hi, o.r[0].lo, __ldcg(pub + PUB_R_HI * ld + E), __ldcg(pub + PUB_R_LO * ld + E)),
               dd_diff(o.r[1].hi, o.r[1].lo, __ldcg(pub + (PUB_R_HI + 1) * ld + E), __ldcg(pub + (PUB_R_LO + 1) * ld + E)),
               dd_diff(o.r[2].hi, o.r[2].lo, __ldcg(pub + (PUB_R_HI + 2) * ld + E), __ldcg(pub + (PUB_R_LO + 2) * ld + E)));
@@ -808,7 +825,7 @@ __device__ __forceinline__ v3 body_sep(const Own &o, const double *pub, int ld, 
 
 // Geopotential items on warps [w_lo, w_hi), as many lanes per item as one round over the items allows
 // (more lanes: shorter chains).
-__device__ void ext_gp(const SysDev &S, const Own *own, int nb, int buf, Scratch &sc, const ReactStage &st, int w_lo,
+__device__ void ext_gp(const SysDev &S, const FieldBody *own, int nb, int buf, Scratch &sc, const ReactStage &st, int w_lo,
                        int w_hi) {
     if (sc.n_gp_e == 0) return;
     const double *pub = S.pub + (size_t)buf * PUB_NPLANES * S.ld;
@@ -824,7 +841,7 @@ __device__ void ext_gp(const SysDev &S, const Own *own, int nb, int buf, Scratch
 // Ring items on the calling warp. With few hosts and disks each lane takes one (body, host, disk) term and
 // the terms are added in disk order afterwards (ring.impl:2122-2192, staged in `rterm`); otherwise one lane
 // per (body, host) runs ring::sum whole.
-__device__ void ext_ring(const SysDev &S, const Own *own, int nb, int buf, Scratch &sc, const ReactStage &st,
+__device__ void ext_ring(const SysDev &S, const FieldBody *own, int nb, int buf, Scratch &sc, const ReactStage &st,
                          double *rterm) {
     const int ld = S.ld, lane = threadIdx.x & 31;
     const double *pub = S.pub + (size_t)buf * PUB_NPLANES * ld;
@@ -835,7 +852,7 @@ __device__ void ext_ring(const SysDev &S, const Own *own, int nb, int buf, Scrat
         #pragma unroll 1
         for (int item = lane; item < nb * nr; item += 32) {
             const int b = item / nr, e = sc.ring_list[item % nr];
-            const Own &o = own[b];
+            const FieldBody &o = own[b];
             const HostInfo h = sc.host[e];
             const bool live = h.E != o.idx;
             v3 r = mk(0, 0, 0), an = mk(0, 0, 0);
@@ -854,7 +871,7 @@ __device__ void ext_ring(const SysDev &S, const Own *own, int nb, int buf, Scrat
     #pragma unroll 1
     for (int item = lane; item < nb * nr * dmax; item += 32) {
         const int b = item / (nr * dmax), hh = (item / dmax) % nr, d = item % dmax;
-        const Own &o = own[b];
+        const FieldBody &o = own[b];
         const HostInfo h = sc.host[sc.ring_list[hh]];
         v3 t = mk(0, 0, 0);
         if (h.E != o.idx && d < h.nd) {
@@ -869,7 +886,7 @@ __device__ void ext_ring(const SysDev &S, const Own *own, int nb, int buf, Scrat
     #pragma unroll 1
     for (int item = lane; item < nb * nr; item += 32) {
         const int b = item / nr, hh = item % nr, e = sc.ring_list[hh];
-        const Own &o = own[b];
+        const FieldBody &o = own[b];
         const HostInfo h = sc.host[e];
         const bool live = h.E != o.idx;
         v3 r = mk(0, 0, 0), an = mk(0, 0, 0);
@@ -892,7 +909,7 @@ __device__ void ext_ring(const SysDev &S, const Own *own, int nb, int buf, Scrat
 // This CTA's share of every host's reaction on threads [t0, t0 + nthr): the sum over its owned bodies (in
 // ownership order) of both model halves, S.react_cta[host][CTA][6], so that a host's owner adds one value per
 // CTA in pass B instead of one per body.
-__device__ void ext_react(const SysDev &S, const Own *own, int nb, const Scratch &sc, const ReactStage &st, int t0,
+__device__ void ext_react(const SysDev &S, const FieldBody *own, int nb, const Scratch &sc, const ReactStage &st, int t0,
                           int nthr) {
     const int ld = S.ld;
     #pragma unroll 1
@@ -939,6 +956,20 @@ __device__ bool pass_a(const SysDev &S, Own *own, int nb, int buf, bool deform_o
     const int ld = S.ld;
     const double *pub = S.pub + (size_t)buf * PUB_NPLANES * ld;
     if (threadIdx.x < nb) { own[threadIdx.x].converged = 0; own[threadIdx.x].gl_fixed = 0; }
+    // the bodies whose fields this CTA evaluates: its own, then those handed over to it (their stage
+    // position and GM from the published state); ordered before their use by load_tile's CTA barrier
+    if (threadIdx.x < sc.nfb) {
+        FieldBody &f = sc.fb[threadIdx.x];
+        if (threadIdx.x < nb) {
+            const Own &o = own[threadIdx.x];
+            f.idx = o.idx; f.slot = threadIdx.x; f.GM = o.GM;
+            for (int c = 0; c < 3; ++c) f.r[c] = o.r[c];
+        } else {
+            const int j = sc.foreign[threadIdx.x - nb];
+            f.idx = j; f.slot = -1; f.GM = __ldcg(pub + PUB_GM * ld + j);
+            for (int c = 0; c < 3; ++c) f.r[c] = dd{__ldcg(pub + (PUB_R_HI + c) * ld + j), __ldcg(pub + (PUB_R_LO + c) * ld + j)};
+        }
+    }
     const bool one_tile = S.n <= S.tile;
     if (one_tile) {
         const double *src[TA_ROWS];
@@ -952,13 +983,14 @@ __device__ bool pass_a(const SysDev &S, Own *own, int nb, int buf, bool deform_o
     // items (sc.ext_overlap) on the kExtWarps - 1 warps before it. With streaming tiles they run on every warp
     // after the sweeps. The per-disk ring terms and, when they fit, the reactions are staged in the rows of
     // the pass-A tile that pass A does not use.
-    const bool fields = !deform_only && S.n_ext > 0;
+    const bool fields = !deform_only && S.n_ext > 0 && !sc.fields_away;
     const bool ring_side = fields && sc.ring_side;
     const bool gp_side = fields && sc.ext_overlap;
     const int max_iter = deform_only ? 1 : 4;   // MAX_ANGULAR_VELOCITY_ITER (mass.impl:74)
     const int nw = deform_only ? kWarps : sc.nw_a;
     double *xa = tile + (size_t)TA_ROWS * kTileW;
-    const ReactStage st{kRingTerms + nb * S.n_ext * 12 <= (kTileRows - TA_ROWS) * kTileW ? xa + kRingTerms : nullptr, nb};
+    const int nf = sc.nfb;
+    const ReactStage st{kRingTerms + nf * S.n_ext * 12 <= (kTileRows - TA_ROWS) * kTileW ? xa + kRingTerms : nullptr, nf};
     const int warp = threadIdx.x >> 5;
     if (warp < nw) {
         #pragma unroll 1
@@ -993,12 +1025,12 @@ __device__ bool pass_a(const SysDev &S, Own *own, int nb, int buf, bool deform_o
         const bool gp_here = ph == 0 ? (gp_side && warp >= nw) : !gp_side;
         const int gp_lo = ph == 0 ? kWarps - kExtWarps : 0;
         const int gp_hi = (ph == 0 ? ring_side : ring_after) ? kWarps - 1 : kWarps;
-        if (ring_here) ext_ring(S, own, nb, buf, sc, st, xa);
-        else if (gp_here && warp >= gp_lo && warp < gp_hi) ext_gp(S, own, nb, buf, sc, st, gp_lo, gp_hi);
+        if (ring_here) ext_ring(S, sc.fb, nf, buf, sc, st, xa);
+        else if (gp_here && warp >= gp_lo && warp < gp_hi) ext_gp(S, sc.fb, nf, buf, sc, st, gp_lo, gp_hi);
     }
     if (fields) {
         __syncthreads();
-        ext_react(S, own, nb, sc, st, 0, blockDim.x);
+        ext_react(S, sc.fb, nf, sc, st, 0, blockDim.x);
         __syncthreads();
     }
     mark(S, sc, PH_B_EXT);   // the fields beyond the sweeps and updates
@@ -1236,10 +1268,22 @@ __device__ bool pass_b(const SysDev &S, Own *own, int nb, int buf, Scratch &sc, 
         Own &ob = own[b];
         v3 da = ldv(ob.dacc);
         v3 tq = ldv(ob.dtq);
-        for (int e = 0; e < n_ext; ++e) {   // the halves of the host's models (a missing half adds zero)
+        // the halves of the host's models (a missing half adds zero), from shared memory or, when other CTAs
+        // evaluated this CTA's fields, from their slots in the global table
+        const bool away = sc.fields_away;
+        for (int e = 0; e < n_ext; ++e) {
             const HostInfo h = sc.host[e];
-            da += h.gp >= 0 ? mk(sc.ext[b][e][0], sc.ext[b][e][1], sc.ext[b][e][2]) : mk(0, 0, 0);
-            da += h.ring >= 0 ? mk(sc.ext2[b][e][0], sc.ext2[b][e][1], sc.ext2[b][e][2]) : mk(0, 0, 0);
+            v3 a0, a1;
+            if (away) {
+                const double *g = S.react + ((size_t)e * S.ld + ob.idx) * 12;
+                a0 = mk(__ldcg(g), __ldcg(g + 1), __ldcg(g + 2));
+                a1 = mk(__ldcg(g + 6), __ldcg(g + 7), __ldcg(g + 8));
+            } else {
+                a0 = mk(sc.ext[b][e][0], sc.ext[b][e][1], sc.ext[b][e][2]);
+                a1 = mk(sc.ext2[b][e][0], sc.ext2[b][e][1], sc.ext2[b][e][2]);
+            }
+            da += h.gp >= 0 ? a0 : mk(0, 0, 0);
+            da += h.ring >= 0 ? a1 : mk(0, 0, 0);
         }
         if (ob.ext_slot >= 0) {
             da += mk(sc.react[b][0], sc.react[b][1], sc.react[b][2]);
@@ -1431,6 +1475,62 @@ __device__ void rk_stage(const SysDev &S, Own *own, int nb, int s, long long i_s
     __syncthreads();
 }
 
+// Field hand-off, decided once per launch by every CTA alike: a CTA that owns a delayed tide iterates
+// pass A up to four times, and every warp it can give the sweeps shortens each iteration (one pair per
+// thread for a whole system of up to 512 bodies instead of two), so the field items of its bodies are
+// evaluated by the CTAs that own no delayed tide, each taking at most kForeignMax of them, dealt in CTA
+// order round-robin. The forces on the handed-over bodies travel through the global table S.react (its
+// reaction-staging slots, free when every CTA stages its reactions in shared memory, which the hand-off
+// requires) and the CTAs that handed over their fields report zero reactions. Uses the staging tile, not
+// yet filled, as scratch; ends with a CTA barrier.
+constexpr int kPlanCtas = 1024;   // CTAs the hand-off plan handles (grids are at most the SM count)
+__device__ void field_handoff(const SysDev &S, const StepParams &P, const Own *own, int nb, Scratch &sc, double *tile) {
+    int *cta_del = reinterpret_cast<int *>(tile);   // [grid]: the CTA owns a delayed tide
+    int *cta_nb = cta_del + kPlanCtas;              // [grid]: bodies of the CTA
+    const bool possible = P.mode != MODE_DEFORM && S.n_ext > 0 && S.n <= S.tile && gridDim.x <= kPlanCtas &&
+                          kRingTerms + kFieldMax * S.n_ext * 12 <= (kTileRows - TA_ROWS) * kTileW;
+    const int n = S.n;
+    for (int c = threadIdx.x; c < (int)gridDim.x; c += blockDim.x) {
+        int d = 0, k = 0;
+        for (int b = 0; b < kOwnMax; ++b) {
+            const int id = S.own_list[c * kOwnMax + b];
+            if (id < 0) break;
+            ++k;
+            const int o = S.orig[id];   // kind 2 of load_own: k2 != 0 and a tide delay
+            d |= S.planes[(size_t)EPH_P_K2 * n + o] != 0 && S.planes[(size_t)EPH_P_TIDE_DELAY * n + o] != 0;
+        }
+        cta_del[c] = d;
+        cta_nb[c] = k;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int n_recv = 0, n_give = 0, my_rank = -1;
+        for (int c = 0; c < (int)gridDim.x; ++c) {
+            if (cta_del[c]) n_give += cta_nb[c];
+            else {
+                if (c == (int)blockIdx.x) my_rank = n_recv;
+                ++n_recv;
+            }
+        }
+        const bool on = possible && n_recv > 0 && n_give > 0 && (n_give + n_recv - 1) / n_recv <= kForeignMax;
+        sc.fields_away = on && cta_del[blockIdx.x];
+        sc.n_foreign = 0;
+        if (on && my_rank >= 0) {   // handed-over body k (CTA order) goes to receiver k % n_recv
+            int k = 0;
+            for (int c = 0; c < (int)gridDim.x; ++c) {
+                if (!cta_del[c]) continue;
+                for (int b = 0; b < cta_nb[c]; ++b, ++k)
+                    if (k % n_recv == my_rank) sc.foreign[sc.n_foreign++] = S.own_list[c * kOwnMax + b];
+            }
+        }
+        sc.nfb = sc.fields_away ? 0 : nb + sc.n_foreign;
+    }
+    __syncthreads();
+    if (sc.fields_away)   // this CTA's share of every host's reaction is evaluated elsewhere
+        for (int q = threadIdx.x; q < S.n_ext * 6; q += blockDim.x)
+            S.react_cta[((size_t)(q / 6) * S.ld + blockIdx.x) * 6 + q % 6] = 0.0;
+}
+
 // ------------------------------------------------------------------ the kernel
 __global__ void __launch_bounds__(kThreads, 1) step_kernel(SysDev S, StepParams P) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -1490,6 +1590,7 @@ __global__ void __launch_bounds__(kThreads, 1) step_kernel(SysDev S, StepParams 
     }
     __syncthreads();
     load_own(S, own, nb, P);
+    field_handoff(S, P, own, nb, sc, tile);
     __syncthreads();
     if (threadIdx.x < nb) publish_body(S, own[threadIdx.x], 0);
     if (threadIdx.x == 32) {
@@ -1500,7 +1601,7 @@ __global__ void __launch_bounds__(kThreads, 1) step_kernel(SysDev S, StepParams 
         bool delayed = false;
         for (int b = 0; b < nb; ++b) delayed |= own[b].kind == 2;
         sc.has_delayed = delayed;
-        const bool side = P.mode != MODE_DEFORM && S.n_ext > 0 && S.n <= S.tile;
+        const bool side = P.mode != MODE_DEFORM && S.n_ext > 0 && S.n <= S.tile && !sc.fields_away;
         sc.ext_overlap = side;
         sc.ring_side = side && sc.n_ring_e > 0;
         sc.nw_a = sc.ext_overlap ? kWarps - kExtWarps : sc.ring_side ? kWarps - 1 : kWarps;
