@@ -49,7 +49,7 @@ METRIC = "body-steps/s vs plain FP64 at <=1e-12 pos err; small-body p50/p99 late
 UNIT = "body-steps/s"
 # DRAM bytes (read + write) of one step_kernel launch, from an ncu capture of that launch
 # (dram__bytes_read.sum + dram__bytes_write.sum), keyed by (workload, RK12 steps per launch).
-DRAM_BYTES_PER_LAUNCH = {("config2", 100): 1499648 + 495104}
+DRAM_BYTES_PER_LAUNCH = {("config2", 100): 1530880 + 461056}
 # DRAM bytes (read + write) of one particle_kernel launch per particle, from the ncu capture summarised in
 # an ncu capture of one launch (1 M particles x 10 steps: 124.4 + 143.5 MB): the particle state is read
 # and written once per launch and the stage store stays in L2, so the traffic scales with the particles and
