@@ -956,19 +956,13 @@ __device__ bool pass_a(const SysDev &S, Own *own, int nb, int buf, bool deform_o
     const int ld = S.ld;
     const double *pub = S.pub + (size_t)buf * PUB_NPLANES * ld;
     if (threadIdx.x < nb) { own[threadIdx.x].converged = 0; own[threadIdx.x].gl_fixed = 0; }
-    // the bodies whose fields this CTA evaluates: its own, then those handed over to it (their stage
-    // position and GM from the published state); ordered before their use by load_tile's CTA barrier
-    if (threadIdx.x < sc.nfb) {
+    // the bodies whose fields this CTA evaluates: its own (ordered before their use by load_tile's CTA
+    // barrier), then those handed over to it (filled by the field warps below)
+    if (threadIdx.x < nb) {
         FieldBody &f = sc.fb[threadIdx.x];
-        if (threadIdx.x < nb) {
-            const Own &o = own[threadIdx.x];
-            f.idx = o.idx; f.slot = threadIdx.x; f.GM = o.GM;
-            for (int c = 0; c < 3; ++c) f.r[c] = o.r[c];
-        } else {
-            const int j = sc.foreign[threadIdx.x - nb];
-            f.idx = j; f.slot = -1; f.GM = __ldcg(pub + PUB_GM * ld + j);
-            for (int c = 0; c < 3; ++c) f.r[c] = dd{__ldcg(pub + (PUB_R_HI + c) * ld + j), __ldcg(pub + (PUB_R_LO + c) * ld + j)};
-        }
+        const Own &o = own[threadIdx.x];
+        f.idx = o.idx; f.slot = threadIdx.x; f.GM = o.GM;
+        for (int c = 0; c < 3; ++c) f.r[c] = o.r[c];
     }
     const bool one_tile = S.n <= S.tile;
     if (one_tile) {
@@ -1015,6 +1009,18 @@ __device__ bool pass_a(const SysDev &S, Own *own, int nb, int buf, bool deform_o
     // the field items: phase 0 beside the sweeps (warps >= nw), phase 1 after them on every warp; one call
     // site per evaluator, so that each is compiled once
     const bool ring_after = fields && !ring_side && sc.n_ring_e > 0;
+    // handed-over bodies (only with the fields beside the sweeps): their stage position and GM from the
+    // published state, loaded by the field warps once the tile copies are under way
+    if (warp >= nw && sc.n_foreign > 0) {
+        const int k = threadIdx.x - nw * 32;
+        if (k < sc.n_foreign) {
+            FieldBody &f = sc.fb[nb + k];
+            const int j = sc.foreign[k];
+            f.idx = j; f.slot = -1; f.GM = __ldcg(pub + PUB_GM * ld + j);
+            for (int c = 0; c < 3; ++c) f.r[c] = dd{__ldcg(pub + (PUB_R_HI + c) * ld + j), __ldcg(pub + (PUB_R_LO + c) * ld + j)};
+        }
+        asm volatile("bar.sync 2, %0;" ::"r"((kWarps - nw) * 32) : "memory");
+    }
     #pragma unroll 1
     for (int ph = 0; ph < 2; ++ph) {
         if (ph == 1) {
