@@ -191,6 +191,58 @@ __device__ __forceinline__ v3 gp_field_lanes(const double *X, const double *rcp,
     return mk(ax * s, ay * s, az * s);
 }
 
+// The field from an expanded table on one lane, column by column (a loop over the order m), the degree
+// steps of a column unrolled up to K: for every model with Nz + 1 <= K and Nt + 1 <= M (the table's zeros
+// cover the terms beyond it). The recursion and gradient terms of gp_field_lanes, but a column starts at
+// its diagonal value (no steps below degree m) and the terms of zero weight are skipped; every branch is
+// the same on all lanes, so the lanes (one model evaluation each) never diverge.
+template <int K, int M>
+__device__ __forceinline__ v3 gp_field_columns(const double *X, const double *rcp, double R, v3 r) {
+    double xs, ys, zs, rho2, v00;
+    gp_setup(R, r.x, r.y, r.z, xs, ys, zs, rho2, v00);
+    double ax = 0, ay = 0, az = 0;
+    double dv = v00, dw = 0;   // diagonal V_mm, W_mm
+    #pragma unroll 1
+    for (int m = 0; m <= M; ++m) {
+        if (m >= 1) {
+            const double f = 2 * m - 1;
+            const double ndv = f * (xs * dv - ys * dw), ndw = f * (xs * dw + ys * dv);
+            dv = ndv;
+            dw = ndw;
+        }
+        const double md = (double)m, wB = m == 1 ? 1.0 : 0.5;
+        const double *XA = X + 2 * m, *XB = X + 2 * (m >= 1 ? m - 1 : 0), *XC = X + 2 * (m + 1);
+        double v = dv, w = dw, vp = 0, wp = 0;   // column m at degrees k and k - 1
+#pragma unroll
+        for (int k = 1; k <= K; ++k) {
+            if (k < m) continue;
+            if (k > m) {
+                const double a = (2 * k - 1) * zs, b = ((k - 1) + md) * rho2, c = rcp[k - m];
+                const double nv = (a * v - b * vp) * c, nw = (a * w - b * wp) * c;
+                vp = v; wp = w; v = nv; w = nw;
+                const double wA = k - md;
+                az -= wA * (XA[(k - 1) * kGpXM * 2] * v + XA[(k - 1) * kGpXM * 2 + 1] * w);
+            }
+            const int row = (k - 1) * kGpXM * 2;
+            if (m >= 1) {
+                const double CB = XB[row], SB = XB[row + 1];
+                ax -= wB * (CB * v + SB * w);
+                ay += wB * (SB * v - CB * w);
+            }
+            if (k >= m + 2) {
+                const double km = k - md, wC = 0.5 * km * (km - 1);
+                const double CC = XC[row], SC = XC[row + 1];
+                ax += wC * (CC * v + SC * w);
+                ay += wC * (SC * v - CC * w);
+            }
+        }
+    }
+    const double s = 1.0 / (R * R);
+    return mk(ax * s, ay * s, az * s);
+}
+constexpr int kGpColK = 7, kGpColM = 5;   // models up to degree 6 and tesseral order 4
+__device__ __forceinline__ bool gp_fits_columns(int Nz, int Nt) { return Nz >= 2 && Nz + 1 <= kGpColK && Nt + 1 <= kGpColM; }
+
 // FP64 field of a geopotential model (any Nz, Nt), out of line: it sits on a cold path of the step kernel.
 static __device__ __noinline__ v3 gp_field(const double *__restrict__ tab, int Nz, int Nt, double R, v3 r) {
     v3 a = mk(0, 0, 0);

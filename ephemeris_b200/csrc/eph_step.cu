@@ -783,7 +783,9 @@ __device__ __forceinline__ void gp_items(const SysDev &S, const FieldBody *fb, i
             const m3 f = ld9(pub + PUB_FRAME * ld, ld, E);
             const double R = __ldg(S.cst + CST_R * ld + E);
             v3 al = mk(0, 0, 0);
-            if (h.gp < kGpSmem) al = gp_field_lanes<G>(sc.gp_x[h.gp], sc.gp_rcp, h.nz, h.nt, R, tolocal(f, r), q, mask);
+            if (G == 1 && h.gp < kGpSmem && gp_fits_columns(h.nz, h.nt))
+                al = gp_field_columns<kGpColK, kGpColM>(sc.gp_x[h.gp], sc.gp_rcp, R, tolocal(f, r));
+            else if (h.gp < kGpSmem) al = gp_field_lanes<G>(sc.gp_x[h.gp], sc.gp_rcp, h.nz, h.nt, R, tolocal(f, r), q, mask);
             else if (q == 0) al = gp_field(S.gp_coef + (size_t)h.gp * EPH_GP_TABLE_SIZE, h.nz, h.nt, R, tolocal(f, r));
             an = toworld(f, al);
         }
