@@ -1,5 +1,6 @@
 // eph_fields.cu - direct evaluation of an extended body's geopotential field on the device, with the same
-// device functions the step kernel (gp_field_lanes) and the particle kernels (gp_field) use. It is what
+// device functions the step kernel (gp_field_lanes, gp_field_columns) and the particle kernels (gp_field)
+// use. It is what
 // geopotential::sum (src/physics/geopotential.h:36) offers the reference's own known-answer test
 // (src/tests/test_geopotential.cpp), so the device evaluation can be held to that test's bound.
 #include <cuda_runtime.h>
@@ -39,12 +40,29 @@ __global__ void gp_field_lanes_kernel(const double *__restrict__ coef, int nz, i
     }
 }
 
+// one point per thread, as the step kernel's one-lane items (the column evaluation for models it covers,
+// else gp_field_lanes on one lane)
+__global__ void gp_field_item_kernel(const double *__restrict__ coef, int nz, int nt, double R, long long count,
+                                     const double *__restrict__ r, double *__restrict__ out) {
+    __shared__ double X[kGpX];
+    gp_expand(coef, nz, nt, X, threadIdx.x, blockDim.x);
+    __syncthreads();
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const v3 p = mk(r[3 * i], r[3 * i + 1], r[3 * i + 2]);
+    const v3 a = gp_fits_columns(nz, nt) ? gp_field_columns<kGpColK, kGpColM>(X, GP_RCP, R, p)
+                                         : gp_field_lanes<1>(X, GP_RCP, nz, nt, R, p, 0, 1u << (threadIdx.x & 31));
+    out[3 * i] = a.x;
+    out[3 * i + 1] = a.y;
+    out[3 * i + 2] = a.z;
+}
+
 }  // namespace eph
 
 extern "C" int eph_geopotential_field(int device, const double *coef, int nz, int nt, double R, int lanes,
                                       int64_t count, const double *r, double *out) {
     if (!coef || !r || !out || count < 0 || nz < 0 || nz > EPH_GP_MAX_DEGREE || nt < 0 || nt > nz ||
-        (lanes != 1 && lanes != 8))
+        (lanes != 0 && lanes != 1 && lanes != 8))
         return EPH_ERR_ARG;
     if (count == 0) return EPH_OK;
     int prev = -1;
@@ -64,8 +82,9 @@ extern "C" int eph_geopotential_field(int device, const double *coef, int nz, in
     }
     if (rc == EPH_OK) {
         const int threads = 128;
-        const long long blocks = (count * lanes + threads - 1) / threads;
+        const long long blocks = (count * (lanes == 8 ? 8 : 1) + threads - 1) / threads;
         if (lanes == 1) eph::gp_field_kernel<<<(unsigned)blocks, threads>>>(d_coef, nz, nt, R, count, d_r, d_out);
+        else if (lanes == 0) eph::gp_field_item_kernel<<<(unsigned)blocks, threads>>>(d_coef, nz, nt, R, count, d_r, d_out);
         else eph::gp_field_lanes_kernel<<<(unsigned)blocks, threads>>>(d_coef, nz, nt, R, count, d_r, d_out);
         if (cudaGetLastError() != cudaSuccess || cudaMemcpy(out, d_out, vb, cudaMemcpyDeviceToHost) != cudaSuccess)
             rc = EPH_ERR_CUDA;

@@ -260,7 +260,9 @@ int eph_serve_info(const eph_serve *s, int64_t *launches, int64_t *queued, int64
  * of a geopotential model coef[EPH_GP_TABLE_SIZE] (degrees 2..nz zonal, tesseral up to nt <= nz) of a body
  * of radius R at `count` body-frame positions r[count][3] (host arrays): out[count][3] = acceleration per
  * unit GM of the body, computed on `device` by the device functions the integration kernels use: lanes = 1
- * one point per thread (massless-particle kernels), lanes = 8 one point per 8 lanes (step kernel). */
+ * one point per thread (massless-particle kernels), lanes = 8 one point per 8 lanes (step kernel), lanes = 0
+ * one point per thread as the step kernel's one-lane items (column by column for models up to degree 6
+ * and order 4, else the lane evaluation on one lane). */
 int eph_geopotential_field(int device, const double *coef, int nz, int nt, double R, int lanes, int64_t count,
                            const double *r, double *out);
 

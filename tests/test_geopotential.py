@@ -9,8 +9,8 @@ the value on it. The same grid and bound are used here against an independent ex
 
 * the oracle's restatement of the reference's evaluation (CPU), and
 * the device functions of the integration kernels (`eph_geopotential_field`, GPU: one point per thread as
-  the particle kernels evaluate it, and one point per 8 lanes as the step kernel does), which use
-  Cunningham's Cartesian recursion, plus a comparison with the oracle on random full models.
+  the particle kernels evaluate it, one point per 8 lanes and one point per lane as the step kernel does),
+  which use Cunningham's Cartesian recursion, plus a comparison with the oracle on random full models.
 """
 import ctypes
 
@@ -65,11 +65,11 @@ def test_geopotential_field_rejects_bad_arguments():
     assert lib.eph_geopotential_field(0, args[0], 9, 0, *args[1:]) == 1       # degree above 8
     assert lib.eph_geopotential_field(0, args[0], 4, 5, *args[1:]) == 1       # tesseral above zonal
     assert lib.eph_geopotential_field(0, None, 4, 4, *args[1:]) == 1
-    assert lib.eph_geopotential_field(0, args[0], 4, 4, 1.0, 4, 1, args[4], args[5]) == 1   # lanes not 1 or 8
+    assert lib.eph_geopotential_field(0, args[0], 4, 4, 1.0, 4, 1, args[4], args[5]) == 1   # lanes not 0, 1 or 8
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("lanes", [1, 8])
+@pytest.mark.parametrize("lanes", [0, 1, 8])
 def test_device_geopotential_known_answer(lanes):
     worst, worst_axis = 0.0, 0.0
     for n, m, sine, tab, nz, nt in H.kat_cases():
@@ -89,7 +89,7 @@ def test_device_geopotential_known_answer(lanes):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("lanes", [1, 8])
+@pytest.mark.parametrize("lanes", [0, 1, 8])
 def test_device_geopotential_matches_oracle(oracle, lanes):
     rng = np.random.default_rng(77)
     worst = 0.0
