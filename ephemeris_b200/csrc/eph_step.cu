@@ -158,8 +158,10 @@ __device__ __forceinline__ void mark(const SysDev &S, Scratch &sc, int ph) {
 // 64-bit word zeroed before the launch that only grows: barrier number k of the launch is complete when it
 // reaches k * gridDim.x, so every CTA announces its arrival with one acquire-release add (which carries the
 // CTA's writes, ordered before it by the CTA barrier) and polls the counter only if its add was not the
-// last one; no CTA has to reset or flip anything. Returns false when the wait timed out here or elsewhere
-// (status word set); the caller then leaves the kernel.
+// last one; no CTA has to reset or flip anything. Returns false when the wait timed out here, or when the
+// status word, read in flight with every poll (no dependent load once the barrier completes), shows that
+// another CTA failed; the caller then leaves the kernel. A CTA that failed arrives at no later barrier, so
+// the others see its status while they wait there.
 __device__ bool grid_sync(const SysDev &S, Scratch &sc) {
     __syncthreads();
     if (gridDim.x == 1) return true;
@@ -172,9 +174,15 @@ __device__ bool grid_sync(const SysDev &S, Scratch &sc) {
         int fail = 0;
         unsigned long long t0 = 0;
         for (unsigned it = 0; old + 1 < target; ++it) {   // the last arrival does not wait
+            // the status word is read before the counter, so that both loads are in flight together
+            const int st = *(volatile const int *)S.status;
             unsigned long long v;
             asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(count) : "memory");
             if (v >= target) break;
+            if (st != ST_OK) {   // another CTA failed: leave at once
+                fail = 1;
+                break;
+            }
             if ((it & 15) == 15) {
                 const unsigned long long t = global_ns();
                 if (t0 == 0) t0 = t;
@@ -185,7 +193,6 @@ __device__ bool grid_sync(const SysDev &S, Scratch &sc) {
                 }
             }
         }
-        if (*(volatile int *)S.status != ST_OK) fail = 1;
         sc.flag = fail;
     }
     __syncthreads();
@@ -1271,28 +1278,41 @@ __device__ bool pass_b(const SysDev &S, Own *own, int nb, int buf, Scratch &sc, 
     // finalisation (mass.cpp:389-396): FINALIZE_RELATIVITY and RING_CORRECTION
     const double c2 = kC * kC;
     const int n_ext = S.n_ext;
+    // the extended bodies' fields on the owned bodies, added to the deformation sum in host order, one thread
+    // per (body, component): the halves of each host's models (a missing half adds zero), from shared memory
+    // or, when other CTAs evaluated this CTA's fields, from their slots in the global table
+    if (n_ext > 0) {
+        if (threadIdx.x < nb * 3) {
+            const int b = threadIdx.x / 3, c = threadIdx.x - 3 * b;
+            Own &ob = own[b];
+            double da = ob.dacc[c];
+            if (sc.fields_away) {
+                const double *g = S.react + (size_t)ob.idx * 12 + c;
+                #pragma unroll 4
+                for (int e = 0; e < n_ext; ++e) {
+                    const HostInfo h = sc.host[e];
+                    const double a0 = __ldcg(g + (size_t)e * S.ld * 12), a1 = __ldcg(g + (size_t)e * S.ld * 12 + 6);
+                    da += h.gp >= 0 ? a0 : 0.0;
+                    da += h.ring >= 0 ? a1 : 0.0;
+                }
+            } else {
+                #pragma unroll 4
+                for (int e = 0; e < n_ext; ++e) {
+                    const HostInfo h = sc.host[e];
+                    const double a0 = sc.ext[b][e][c], a1 = sc.ext2[b][e][c];
+                    da += h.gp >= 0 ? a0 : 0.0;
+                    da += h.ring >= 0 ? a1 : 0.0;
+                }
+            }
+            ob.dacc[c] = da;
+        }
+        __syncthreads();
+    }
     #pragma unroll 1
     for (int b = threadIdx.x; b < nb; b += blockDim.x) {
         Own &ob = own[b];
         v3 da = ldv(ob.dacc);
         v3 tq = ldv(ob.dtq);
-        // the halves of the host's models (a missing half adds zero), from shared memory or, when other CTAs
-        // evaluated this CTA's fields, from their slots in the global table
-        const bool away = sc.fields_away;
-        for (int e = 0; e < n_ext; ++e) {
-            const HostInfo h = sc.host[e];
-            v3 a0, a1;
-            if (away) {
-                const double *g = S.react + ((size_t)e * S.ld + ob.idx) * 12;
-                a0 = mk(__ldcg(g), __ldcg(g + 1), __ldcg(g + 2));
-                a1 = mk(__ldcg(g + 6), __ldcg(g + 7), __ldcg(g + 8));
-            } else {
-                a0 = mk(sc.ext[b][e][0], sc.ext[b][e][1], sc.ext[b][e][2]);
-                a1 = mk(sc.ext2[b][e][0], sc.ext2[b][e][1], sc.ext2[b][e][2]);
-            }
-            da += h.gp >= 0 ? a0 : mk(0, 0, 0);
-            da += h.ring >= 0 ? a1 : mk(0, 0, 0);
-        }
         if (ob.ext_slot >= 0) {
             da += mk(sc.react[b][0], sc.react[b][1], sc.react[b][2]);
             tq += mk(sc.react[b][3], sc.react[b][4], sc.react[b][5]);
