@@ -17,7 +17,8 @@
 //                 other warps evaluate every geopotential / ring host's field at the owned bodies, once
 //                 per (host, body) pair: the force on the body stays in shared memory, the reaction on
 //                 the host goes to a global table its owner sums in pass B (APPLY_NONPOINT_FORCE,
-//                 mass.impl:127-130);
+//                 mass.impl:127-130). A CTA that owns a delayed tide hands its bodies' field items to
+//                 CTAs that own none (field_handoff), so that its fixed-point sweeps run on every warp;
 //       pass B  - 1PN, deformation, Lense-Thirring and radiation (mass.impl:82-125), the hosts' reaction
 //                 sums, finalisation (mass.cpp:389-396), then the RK12 stage combination and the state
 //                 update of the owned bodies;
@@ -677,8 +678,8 @@ __device__ __forceinline__ void tile_a_rows(const SysDev &S, const double *pub, 
 
 // Pair sums of pass A for the owned bodies in `mask` over all bodies j, by the first `nw` warps (tile
 // already staged when the whole system fits in one tile; otherwise tiles are streamed, which needs the
-// whole CTA, nw == kWarps). Results land in own[b].sumA. Two bodies j per iteration keep two
-// independent pair chains in flight per thread.
+// whole CTA, nw == kWarps). Results land in own[b].sumA. One pair per iteration: a second pair chain in
+// flight per thread spills registers at the kernel's 128 per thread.
 __device__ bool sweep_a(const SysDev &S, Own *own, int nb, unsigned mask, int buf, Scratch &sc, TileState &ts,
                         double *tile, bool staged, int nw, const int *first_all) {
     const int na = __popc(mask);
