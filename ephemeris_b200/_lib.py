@@ -97,6 +97,12 @@ SIGNATURES = [
     ("eph_bspline_cheb_coef", ctypes.c_double, [ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     ("eph_bspline_fit_batch", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int64, ctypes.c_int64, ctypes.c_int,
                                               ctypes.c_int64, _D, _D]),
+    ("eph_ephem_open", ctypes.c_int, [_VP, ctypes.c_int64, ctypes.c_double, ctypes.POINTER(_VP)]),
+    ("eph_ephem_close", ctypes.c_int, [_VP]),
+    ("eph_ephem_info", ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                       ctypes.POINTER(ctypes.c_int64), _D, _D]),
+    ("eph_ephem_state", ctypes.c_int, [_VP, ctypes.c_double, _D, _D, _D]),
+    ("eph_ephem_to_bspline", ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int64, ctypes.c_int64, _D]),
     ("eph_geopotential_field", ctypes.c_int, [ctypes.c_int, _D, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                                ctypes.c_int, ctypes.c_int64, _D, _D]),
     ("eph_fp64_fma_rate", ctypes.c_int, [ctypes.c_int, _D]),

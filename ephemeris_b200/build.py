@@ -22,7 +22,7 @@ BUILD = os.path.join(HERE, "_build")
 
 CUDA_UNITS = ["eph_step.cu", "eph_capi.cu", "eph_noalloc.cu", "eph_batch.cu", "eph_particles.cu", "eph_serve.cu",
               "eph_fields.cu"]
-CXX_UNITS = ["eph_msystem.cpp", "eph_bspline.cpp"]
+CXX_UNITS = ["eph_msystem.cpp", "eph_bspline.cpp", "eph_ephemeris.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr", *ARCH]
 

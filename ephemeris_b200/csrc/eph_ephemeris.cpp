@@ -1,0 +1,351 @@
+// eph_ephemeris.cpp - reading the reference's compressed orbital ephemeris records on the host, and
+// resampling them into the B-spline tables of the device ephemeris (eph_bspline_fit, eph_serve_*).
+//
+// Record format (src/modules/ephemeris_compressor.h:50-72 and ephemeris_compressor.cpp:9-66): a 24-byte
+// common header {float relative_error; int16 degree; uint16 ~format; int64 n; float smooth_range[2]},
+// the format's end corrections fix[4][channels] (left value, left derivative, right value, right
+// derivative), the format's extra constants, then (n + degree) B-spline coefficients of `channels` values
+// over n uniform segments spanning the record's time range. The orbital formats read here:
+//
+//   1 STATE_VECTORS       channel: position vector                        (fix: 4 vectors)
+//   2 KEPLERIAN_VECTORS   channel: position vector, then GM               (fix: 4 vectors)
+//   3 KEPLERIAN_CIRCULAR  6 channels j[3], ex, ey, mean longitude; GM      (fix: 4 x 6)
+//   4 KEPLERIAN_RAW       6 channels j[3], q, el, modified mean anomaly; GM (fix: 4 x 6)
+//
+// Evaluation at time t in [0, range] (ephemeris_compressor.cpp:1017-1053): the spline's value and time
+// derivative at x = t n / range, a cubic blend of the end corrections inside the first / last
+// smooth_range segments (ephemeris_compressor.cpp:719-735), then the format's conversion to position and
+// velocity: the vector formats take value and derivative as they are; the element formats turn the
+// interpolated elements into a state (state_parameters.cpp:69-86,137-168 for the element sets,
+// keplerian.cpp:138-224 for the state), with velocities scaled by sqrt(GM). The rotational formats (5-7)
+// are not read (EPH_ERR_UNSUPPORTED).
+//
+// Own implementation: the B-spline pieces come from the degree recursion evaluated at the point (not the
+// reference's Chebyshev tables), and the element-to-state conversion is the textbook perifocal form with
+// Kepler's equation solved by safeguarded Newton steps; agreement with the reference interpolator is to
+// rounding, not bit for bit.
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "../../include/eph_b200.h"
+
+namespace {
+
+constexpr int kMaxRecordDegree = 11;   // the compressor's largest (odd) degree
+constexpr size_t kCommonHeader = 24;
+
+struct Header {
+    float relative_error;
+    int16_t degree;
+    uint16_t uformat;
+    int64_t n;
+    float smooth[2];
+};
+static_assert(sizeof(Header) == kCommonHeader, "the record's common header is 24 bytes");
+
+// per-format layout: channels, bytes of the header before the coefficients, whether GM follows the fix
+struct Layout {
+    int channels;
+    size_t header_bytes;
+    bool has_gm;
+};
+bool layout_of(int format, Layout &L) {
+    switch (format) {
+        case 1: L = {3, kCommonHeader + 4 * 3 * 8, false}; return true;
+        case 2: L = {3, kCommonHeader + 4 * 3 * 8 + 8, true}; return true;
+        case 3:
+        case 4: L = {6, kCommonHeader + 4 * 6 * 8 + 8, true}; return true;
+        default: return false;
+    }
+}
+
+}  // namespace
+
+struct eph_ephem {
+    int format = 0, degree = 0, channels = 0;
+    int64_t n = 0;
+    double range = 0, relative_error = 0, gm = 0;
+    double smooth[2] = {0, 0};
+    double fix[4][6] = {};
+    std::vector<double> coef;   // [n + degree][channels]
+};
+
+namespace {
+
+// Values and x-derivatives of the degree-d pieces at u in [0, 1]: piece k is the basis function of
+// coefficient (segment + k), B[d, u - k] with B[0, x] = 1 on [0, 1) and
+// B[d, x] = ((x + d) B[d-1, x+1] + (1 - x) B[d-1, x]) / d (src/math/interp.h:10-22); the derivative is
+// B[d-1, x+1] - B[d-1, x].
+void pieces(int d, double u, double *b, double *db) {
+    double prev[kMaxRecordDegree + 1] = {1.0};
+    for (int e = 1; e <= d; ++e) {
+        double cur[kMaxRecordDegree + 1];
+        for (int k = 0; k <= e; ++k) {
+            const double left = k >= 1 ? prev[k - 1] : 0.0;   // B[e-1, u-k+1]: piece k-1 of degree e-1
+            const double right = k <= e - 1 ? prev[k] : 0.0;  // B[e-1, u-k]: piece k of degree e-1
+            if (e == d) db[k] = left - right;
+            cur[k] = ((u - k + e) * left + (1 - u + k) * right) / e;
+        }
+        for (int k = 0; k <= e; ++k) prev[k] = cur[k];
+    }
+    if (d == 0) db[0] = 0;
+    for (int k = 0; k <= d; ++k) b[k] = prev[k];
+}
+
+// Spline value and time derivative of every channel at t; false outside [0, range].
+bool spline_at(const eph_ephem &E, double t, double *val, double *der) {
+    const double x = t / E.range * (double)E.n;
+    if (!(x >= 0 && x <= (double)E.n)) return false;
+    int64_t seg = (int64_t)std::floor(x);
+    if (seg == E.n) seg -= 1;
+    const double u = x - (double)seg;
+    double b[kMaxRecordDegree + 1], db[kMaxRecordDegree + 1];
+    pieces(E.degree, u, b, db);
+    const double dxdt = (double)E.n / E.range;
+    const int C = E.channels;
+    for (int c = 0; c < C; ++c) { val[c] = 0; der[c] = 0; }
+    for (int k = 0; k <= E.degree; ++k) {
+        const double *a = E.coef.data() + (size_t)(seg + k) * C;
+        for (int c = 0; c < C; ++c) {
+            val[c] += b[k] * a[c];
+            der[c] += db[k] * a[c];
+        }
+    }
+    for (int c = 0; c < C; ++c) der[c] *= dxdt;
+    return true;
+}
+
+// The end corrections: inside the first (last) smooth[0] (smooth[1]) segments the spline is pulled toward
+// the recorded end state by value + derivative * distance, weighted by the cubic (1 - s)^2 (1 + 2 s) of the
+// fraction s of the blending range (ephemeris_compressor.cpp:719-735, 1017-1030).
+void blend_ends(const eph_ephem &E, double t, double *val, double *der) {
+    const double x = t / E.range * (double)E.n, nn = (double)E.n;
+    const double vscale = nn / E.range;
+    auto pull = [&](const double *fv, const double *fd, double dist, double width) {
+        const double s = dist / width, w1 = 1 - s;
+        const double w = w1 * w1 * (1 + 2 * s), dw = -6 * s * w1 / width;
+        for (int c = 0; c < E.channels; ++c) {
+            const double dr = fv[c] + fd[c] * dist;
+            val[c] += w * dr;
+            der[c] += (dw * dr + w * fd[c]) * vscale;
+        }
+    };
+    if (std::floor(x) == 0 && x < E.smooth[0]) pull(E.fix[0], E.fix[1], x, E.smooth[0]);
+    if (std::ceil(x) == nn && nn - x < E.smooth[1]) pull(E.fix[2], E.fix[3], nn - x, E.smooth[1]);
+}
+
+// ------------------------------------------------------------------ orbital elements to state
+struct V3 {
+    double x, y, z;
+};
+V3 operator+(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+V3 operator*(double s, V3 a) { return {s * a.x, s * a.y, s * a.z}; }
+double dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+V3 cross(V3 a, V3 b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+
+// Unit vector toward the ascending node of the plane normal to j: (-j.y, j.x, 0) normalised, or the x axis
+// when j is along z (src/math/vec_t.h:226-230).
+V3 ascending_node(V3 j) {
+    const double h = std::hypot(j.x, j.y);
+    if (h == 0) return {1, 0, 0};
+    return {-j.y / h, j.x / h, 0};
+}
+
+// The reference's element set (src/math/keplerian.h:6-22), with time scaled by sqrt(GM):
+//   j  angular momentum per mass / sqrt(GM)      q  e - 1
+//   w  argument of the eccentricity vector from the ascending node, in the orbit plane
+//   m  mean anomaly / |1 - e^2|^(3/2)            (dm/dt = 1 / |j|^3)
+struct Elements {
+    V3 j;
+    double q, w, m;
+};
+
+// The interpolated channels of a record as elements (state_parameters.cpp:69-86 with 137-168): circular
+// sets hold j, e (cos, sin) of the longitude of periapsis and the mean longitude; raw sets hold j, q, the
+// longitude of periapsis and m. Longitudes count from the x axis: w = longitude - phi(ascending node).
+Elements elements_from(const double *p, bool circular) {
+    Elements k;
+    k.j = {p[0], p[1], p[2]};
+    const V3 an = ascending_node(k.j);
+    const double node = std::atan2(an.y, an.x);
+    if (circular) {
+        const double e = std::sqrt(p[3] * p[3] + p[4] * p[4]);
+        const double lp = std::atan2(p[4], p[3]);
+        k.q = e - 1;
+        const double s = -k.q * (k.q + 2);   // 1 - e^2
+        k.m = (p[5] - lp) / (s * std::sqrt(s));
+        k.w = lp - node;
+    } else {
+        k.q = p[3];
+        k.m = p[5];
+        k.w = p[4] - node;
+    }
+    return k;
+}
+
+// Mean anomaly reduced into [-pi, pi].
+double wrap_pi(double a) {
+    constexpr double two_pi = 6.283185307179586476925286766559;
+    if (a > -M_PI && a <= M_PI) return a;
+    return a - two_pi * std::nearbyint(a / two_pi);
+}
+
+// Position and velocity / sqrt(GM) of elements k at their epoch (keplerian.cpp:138-224 for the quantity;
+// the conics in perifocal coordinates scaled by the semi-latus rectum p = |j|^2: x = X / p, y = Y / p,
+// velocity (-y, e - Q x) |j| / r with Q = e^2 - 1).
+void elements_to_state(const Elements &k, V3 &r, V3 &v) {
+    const double jj = dot(k.j, k.j), jn = std::sqrt(jj);
+    const double e = k.q + 1;
+    const double Q = k.q * (k.q + 2);   // e^2 - 1 without cancellation
+    const double aQ = std::fabs(Q), sQ = std::sqrt(aQ);
+    double x, y;
+    if (Q < 0) {
+        // ellipse: E - e sin E = M; x = (cos E - e) / (1 - e^2), y = sin E / sqrt(1 - e^2), with
+        // cos E - e = -2 sin^2(E/2) - q kept free of cancellation near periapsis of a near-parabolic orbit
+        const double M = wrap_pi(k.m * aQ * sQ);
+        double E = M + 0.85 * e * (M >= 0 ? 1 : -1);   // Danby's start: Newton converges for every e < 1
+        for (int it = 0; it < 60; ++it) {
+            const double f = E - e * std::sin(E) - M, fp = 1 - e * std::cos(E);
+            const double dE = f / fp;
+            E -= dE;
+            if (std::fabs(dE) <= 1e-16 * (1 + std::fabs(E))) break;
+        }
+        const double sh = std::sin(0.5 * E);
+        x = (-2 * sh * sh - k.q) / aQ;
+        y = std::sin(E) / sQ;
+    } else if (Q > 0) {
+        // hyperbola: e sinh H - H = M; x = (e - cosh H) / (e^2 - 1), y = sinh H / sqrt(e^2 - 1)
+        const double M = k.m * aQ * sQ;
+        double H = std::asinh(M / e);
+        for (int it = 0; it < 200; ++it) {
+            const double f = e * std::sinh(H) - H - M, fp = e * std::cosh(H) - 1;
+            const double dH = f / fp;
+            H -= dH;
+            if (std::fabs(dH) <= 1e-16 * (1 + std::fabs(H))) break;
+        }
+        const double sh = std::sinh(0.5 * H);
+        x = (k.q - 2 * sh * sh) / aQ;   // e - cosh H = q - 2 sinh^2(H/2)
+        y = std::sinh(H) / sQ;
+    } else {
+        // parabola: Barker's equation for D = tan(nu/2): D / 2 + D^3 / 6 = m (the limit of the modified
+        // mean anomaly); x = (1 - D^2) / 2, y = D
+        const double m3 = 3 * k.m, s = std::cbrt(m3 + std::sqrt(1 + m3 * m3));
+        const double D = s - 1 / s;
+        x = (1 - D * D) / 2;
+        y = D;
+    }
+    const double rn = jj * std::sqrt(x * x + y * y);   // |r|
+    const double vv = jn / rn;
+    const double vx = -y * vv, vy = (e - Q * x) * vv;
+    const V3 jx = ascending_node(k.j), jy = (1 / jn) * cross(k.j, jx);
+    const double cw = std::cos(k.w), sw = std::sin(k.w);
+    const double X = jj * x, Y = jj * y;
+    r = (X * cw - Y * sw) * jx + (X * sw + Y * cw) * jy;
+    v = (vx * cw - vy * sw) * jx + (vx * sw + vy * cw) * jy;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ C ABI
+extern "C" {
+
+int eph_ephem_open(const void *record, int64_t size, double range, eph_ephem **out) {
+    if (!out) return EPH_ERR_ARG;
+    *out = nullptr;
+    if (!record || size < (int64_t)kCommonHeader || !(range != 0 && range * 0 == 0)) return EPH_ERR_ARG;
+    const uint8_t *p = static_cast<const uint8_t *>(record);
+    Header h;
+    std::memcpy(&h, p, sizeof(h));
+    const double rel = h.relative_error;
+    if (!(rel >= 0 && rel < 1)) return EPH_ERR_LOAD;   // an uncompressed or failed record
+    const int format = (uint16_t)~h.uformat;
+    if (format >= 5 && format <= 7) return EPH_ERR_UNSUPPORTED;   // rotational records
+    Layout L;
+    if (!layout_of(format, L)) return EPH_ERR_LOAD;
+    if (h.degree < 1 || h.degree > kMaxRecordDegree || h.n < 1) return EPH_ERR_LOAD;
+    const int64_t per = (int64_t)L.channels * 8;
+    if (size < (int64_t)L.header_bytes || (size - (int64_t)L.header_bytes) % per != 0 ||
+        (size - (int64_t)L.header_bytes) / per != h.n + h.degree)
+        return EPH_ERR_LOAD;
+    eph_ephem *E = new (std::nothrow) eph_ephem;
+    if (!E) return EPH_ERR_LIMIT;
+    E->format = format;
+    E->degree = h.degree;
+    E->channels = L.channels;
+    E->n = h.n;
+    E->range = range;
+    E->relative_error = rel;
+    E->smooth[0] = h.smooth[0];
+    E->smooth[1] = h.smooth[1];
+    const uint8_t *q = p + kCommonHeader;
+    for (int a = 0; a < 4; ++a, q += per) std::memcpy(E->fix[a], q, (size_t)per);
+    if (L.has_gm) std::memcpy(&E->gm, q, 8);
+    try {
+        E->coef.resize((size_t)(h.n + h.degree) * L.channels);
+    } catch (...) {
+        delete E;
+        return EPH_ERR_LIMIT;
+    }
+    std::memcpy(E->coef.data(), p + L.header_bytes, E->coef.size() * 8);
+    *out = E;
+    return EPH_OK;
+}
+
+int eph_ephem_close(eph_ephem *E) {
+    delete E;
+    return EPH_OK;
+}
+
+int eph_ephem_info(const eph_ephem *E, int *format, int *degree, int64_t *segments, double *relative_error,
+                   double *gm) {
+    if (!E) return EPH_ERR_ARG;
+    if (format) *format = E->format;
+    if (degree) *degree = E->degree;
+    if (segments) *segments = E->n;
+    if (relative_error) *relative_error = E->relative_error;
+    if (gm) *gm = E->format == 1 ? 0.0 : E->gm;
+    return EPH_OK;
+}
+
+int eph_ephem_state(const eph_ephem *E, double t, double *r, double *v, double *gm) {
+    if (!E || !r || !v) return EPH_ERR_ARG;
+    double val[6], der[6];
+    if (!spline_at(*E, t, val, der)) {
+        for (int c = 0; c < 3; ++c) r[c] = v[c] = NAN;
+        return EPH_ERR_ARG;
+    }
+    blend_ends(*E, t, val, der);
+    if (E->format <= 2) {
+        for (int c = 0; c < 3; ++c) { r[c] = val[c]; v[c] = der[c]; }
+    } else {
+        V3 rr, vv;
+        elements_to_state(elements_from(val, E->format == 3), rr, vv);
+        const double sg = std::sqrt(E->gm);
+        r[0] = rr.x; r[1] = rr.y; r[2] = rr.z;
+        v[0] = sg * vv.x; v[1] = sg * vv.y; v[2] = sg * vv.z;
+    }
+    if (gm) *gm = E->format == 1 ? 0.0 : E->gm;
+    return EPH_OK;
+}
+
+int eph_ephem_to_bspline(const eph_ephem *E, int d, int64_t n, int64_t mn, double *coefs) {
+    if (!E || !coefs || mn < 1 || n < 1 || mn + 1 < n + d) return EPH_ERR_ARG;
+    std::vector<double> samples;
+    try {
+        samples.resize((size_t)(mn + 1) * 3);
+    } catch (...) {
+        return EPH_ERR_LIMIT;
+    }
+    for (int64_t k = 0; k <= mn; ++k) {
+        const double t = k == mn ? E->range : E->range * ((double)k / (double)mn);
+        double v[3];
+        const int rc = eph_ephem_state(E, t, samples.data() + 3 * k, v, nullptr);
+        if (rc) return rc;
+    }
+    return eph_bspline_fit(d, n, mn, 3, samples.data(), coefs);
+}
+
+}  // extern "C"

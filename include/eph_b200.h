@@ -210,6 +210,25 @@ int eph_bspline_fit_batch(int device, int d, int64_t n, int64_t mn, int channels
 /* c(d, k, j): B[d, x - k] = sum_j c(d,k,j) T_j(2x - 1) on x in [0, 1) (src/math/interp.h:24-30). */
 double eph_bspline_cheb_coef(int d, int k, int j);
 
+/* ---- Compressed orbital ephemeris records (host). One record as the reference's compressor writes it
+ * (ephemeris_compressor::compress_orbital_data, src/modules/ephemeris_compressor.cpp:164-399; the reader
+ * hands each one to ephemeris_compressor::interpolator, ephemeris_compressor.h:74-148 and
+ * ephemeris_compressor.cpp:852-910) covering `range` seconds. Formats 1-4 (state vectors, Keplerian
+ * vectors, circular and raw Keplerian elements) are read; rotational records (formats 5-7) return
+ * EPH_ERR_UNSUPPORTED, a record that is not a valid compressed orbital record EPH_ERR_LOAD. */
+typedef struct eph_ephem eph_ephem;
+int eph_ephem_open(const void *record, int64_t size, double range, eph_ephem **out);
+int eph_ephem_close(eph_ephem *e);
+/* Format (1-4), B-spline degree, segments, the recorded relative error and GM (0 for state vectors). */
+int eph_ephem_info(const eph_ephem *e, int *format, int *degree, int64_t *segments, double *relative_error,
+                   double *gm);
+/* Position r[3] and velocity v[3] at time t in [0, range] (interpolator::operator(), ephemeris_compressor.cpp:
+ * 1036-1053); gm may be NULL. Outside [0, range]: NaN and EPH_ERR_ARG. */
+int eph_ephem_state(const eph_ephem *e, double t, double *r, double *v, double *gm);
+/* The record's positions at mn + 1 uniform times over [0, range], fitted by eph_bspline_fit with degree d
+ * and n segments: coefs[n + d][3], the form of the device ephemeris (eph_serve_*, eph_bspline_fit_batch). */
+int eph_ephem_to_bspline(const eph_ephem *e, int d, int64_t n, int64_t mn, double *coefs);
+
 /* ---- Ephemeris samples for a B-spline ephemeris (no counterpart in the reference's GPU path; its
  * generator records states on the host per cadence, src/modules/ephemeris_generator.cpp:128-169).
  * Integrates n_step steps of dt from t_eph (advanced, msystem::integrate's RK12) and writes the state at

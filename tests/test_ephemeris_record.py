@@ -1,0 +1,128 @@
+"""Compressed orbital ephemeris records: the library's decoder against the reference's own interpolator.
+
+The fixtures (tests/golden/ephemeris/*.npz, recorded by tests/golden/make_ephemeris_golden.py) hold
+records written by the reference's compressor (`ephemeris_compressor::compress_orbital_data`,
+src/modules/ephemeris_compressor.cpp:164-399) and the reference interpolator's states at 59 times per
+record (ephemeris_compressor.cpp:1036-1053), both on the B-spline form as loaded and after expand(). They
+cover the four orbital formats: state vectors, Keplerian vectors, circular and raw Keplerian elements.
+
+The decoder evaluates the spline and the element-to-state conversion its own way, so the bound is the
+reference's own rounding spread: the larger of 1e-14 and 1.5x the difference between the reference's two
+evaluation forms, relative to the record's largest |r| (|v|). GM is compared exactly.
+CPU-only: the decoder is host code of libeph_b200.so.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from ephemeris_b200.ephemeris_record import EphemerisInterpolator
+from ephemeris_b200 import EphError, bspline_fit
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+FIXTURES = sorted(glob.glob(os.path.join(HERE, "golden", "ephemeris", "*.npz")))
+EPH_ERR_ARG, EPH_ERR_LOAD, EPH_ERR_UNSUPPORTED = 1, 6, 7
+
+
+def _load(path):
+    z = np.load(path)
+    return z, EphemerisInterpolator(z["blob"].tobytes(), float(z["span"]))
+
+
+def test_fixtures_cover_every_orbital_format():
+    formats = {int(np.load(f)["format"]) for f in FIXTURES}
+    assert formats == {1, 2, 3, 4}, formats
+
+
+@pytest.mark.parametrize("path", FIXTURES, ids=[os.path.basename(f)[:-4] for f in FIXTURES])
+def test_record_matches_reference_interpolator(path):
+    z, ip = _load(path)
+    assert ip.format == int(z["format"])
+    assert 0 <= ip.relative_error < 1
+    got = ip.states(z["times"])
+    ref_a, ref_b = z["loaded"], z["expanded"]
+    rs = np.linalg.norm(ref_a[:, :3], axis=1).max()
+    vs = np.linalg.norm(ref_a[:, 3:6], axis=1).max()
+    spread_r = np.abs(ref_a[:, :3] - ref_b[:, :3]).max() / rs
+    spread_v = np.abs(ref_a[:, 3:6] - ref_b[:, 3:6]).max() / vs
+    tol_r, tol_v = max(1e-14, 1.5 * spread_r), max(1e-14, 1.5 * spread_v)
+    for ref in (ref_a, ref_b):
+        assert np.abs(got[:, :3] - ref[:, :3]).max() / rs <= tol_r
+        assert np.abs(got[:, 3:] - ref[:, 3:6]).max() / vs <= tol_v
+    gm_ref = ref_a[:, 6]
+    for k, t in enumerate(z["times"][:5]):
+        _, _, gm = ip(t)
+        assert gm == gm_ref[k] or (ip.format == 1 and gm == 0 and gm_ref[k] == 0)
+    ip.close()
+
+
+def test_times_outside_the_record_are_rejected():
+    z, ip = _load(FIXTURES[0])
+    with pytest.raises(EphError) as e:
+        ip(float(z["span"]) * 1.001)
+    assert e.value.code == EPH_ERR_ARG
+    with pytest.raises(EphError):
+        ip(-1.0)
+
+
+def _patched(blob, offset, dtype, value):
+    b = bytearray(blob)
+    b[offset:offset + np.dtype(dtype).itemsize] = np.array([value], dtype).tobytes()
+    return bytes(b)
+
+
+def test_invalid_records_are_rejected():
+    z = np.load(FIXTURES[0])
+    blob, span = z["blob"].tobytes(), float(z["span"])
+    cases = [
+        (blob[:-8], EPH_ERR_LOAD),                               # size does not match n + degree coefficients
+        (_patched(blob, 0, np.float32, 1.0), EPH_ERR_LOAD),       # relative error not below 1
+        (_patched(blob, 0, np.float32, np.nan), EPH_ERR_LOAD),
+        (_patched(blob, 6, np.uint16, 0xFFFF), EPH_ERR_LOAD),     # format 0 (uncompressed)
+        (_patched(blob, 6, np.uint16, 0xFFFF ^ 6), EPH_ERR_UNSUPPORTED),   # a rotational (quaternion) record
+        (_patched(blob, 4, np.int16, 0), EPH_ERR_LOAD),           # degree 0
+        (_patched(blob, 8, np.int64, 0), EPH_ERR_LOAD),           # no segments
+        (blob[:16], EPH_ERR_ARG),                                 # shorter than the common header
+    ]
+    for rec, want in cases:
+        with pytest.raises(EphError) as e:
+            EphemerisInterpolator(rec, span)
+        assert e.value.code == want, (want, e.value.code)
+    with pytest.raises(EphError) as e:
+        EphemerisInterpolator(blob, 0.0)
+    assert e.value.code == EPH_ERR_ARG
+
+
+def _bspline_eval(coefs, d, n, x):
+    """Value of sum_i coefs[i] B[d, x - i] at positions x in [0, n] (the basis recursion)."""
+    out = np.zeros((len(x), coefs.shape[1]))
+    for q, xv in enumerate(x):
+        seg = min(int(np.floor(xv)), n - 1)
+        u = xv - seg
+        prev = [1.0]
+        for e in range(1, d + 1):
+            cur = []
+            for k in range(e + 1):
+                left = prev[k - 1] if k >= 1 else 0.0
+                right = prev[k] if k <= e - 1 else 0.0
+                cur.append(((u - k + e) * left + (1 - u + k) * right) / e)
+            prev = cur
+        out[q] = sum(prev[k] * coefs[seg + k] for k in range(d + 1))
+    return out
+
+
+def test_record_resampled_into_device_bspline_table():
+    path = [f for f in FIXTURES if os.path.basename(f).startswith("moon_circular")][0]
+    z, ip = _load(path)
+    span = float(z["span"])
+    d, n, mn = 3, 216, 864
+    coefs = ip.to_bspline(d, n, mn)
+    samples = ip.states(span * np.arange(mn + 1) / mn)[:, :3]
+    samples[-1] = ip(span)[0]
+    assert np.array_equal(coefs, bspline_fit(samples, n, d))   # the same fit of the same samples
+    x = np.sort(np.random.default_rng(5).uniform(0, n, 40))
+    fit = _bspline_eval(coefs, d, n, x)
+    exact = ip.states(x / n * span)[:, :3]
+    err = np.linalg.norm(fit - exact, axis=1).max() / np.linalg.norm(exact, axis=1).max()
+    assert err < 1e-7, err
