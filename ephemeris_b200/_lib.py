@@ -103,6 +103,8 @@ SIGNATURES = [
                                        ctypes.POINTER(ctypes.c_int64), _D, _D]),
     ("eph_ephem_state", ctypes.c_int, [_VP, ctypes.c_double, _D, _D, _D]),
     ("eph_ephem_to_bspline", ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int64, ctypes.c_int64, _D]),
+    ("eph_ephem_rotation", ctypes.c_int, [_VP, ctypes.c_double, _D, _D, _D]),
+    ("eph_ephem_set_orbital_state", ctypes.c_int, [_VP, _D, _D]),
     ("eph_geopotential_field", ctypes.c_int, [ctypes.c_int, _D, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                                ctypes.c_int, ctypes.c_int64, _D, _D]),
     ("eph_fp64_fma_rate", ctypes.c_int, [ctypes.c_int, _D]),

@@ -1,11 +1,11 @@
-// eph_ephemeris.cpp - reading the reference's compressed orbital ephemeris records on the host, and
+// eph_ephemeris.cpp - reading the reference's compressed ephemeris records on the host, and
 // resampling them into the B-spline tables of the device ephemeris (eph_bspline_fit, eph_serve_*).
 //
 // Record format (src/modules/ephemeris_compressor.h:50-72 and ephemeris_compressor.cpp:9-66): a 24-byte
 // common header {float relative_error; int16 degree; uint16 ~format; int64 n; float smooth_range[2]},
 // the format's end corrections fix[4][channels] (left value, left derivative, right value, right
 // derivative), the format's extra constants, then (n + degree) B-spline coefficients of `channels` values
-// over n uniform segments spanning the record's time range. The orbital formats read here:
+// over n uniform segments spanning the record's time range. The orbital formats:
 //
 //   1 STATE_VECTORS       channel: position vector                        (fix: 4 vectors)
 //   2 KEPLERIAN_VECTORS   channel: position vector, then GM               (fix: 4 vectors)
@@ -17,13 +17,20 @@
 // smooth_range segments (ephemeris_compressor.cpp:719-735), then the format's conversion to position and
 // velocity: the vector formats take value and derivative as they are; the element formats turn the
 // interpolated elements into a state (state_parameters.cpp:69-86,137-168 for the element sets,
-// keplerian.cpp:138-224 for the state), with velocities scaled by sqrt(GM). The rotational formats (5-7)
-// are not read (EPH_ERR_UNSUPPORTED).
+// keplerian.cpp:138-224 for the state), with velocities scaled by sqrt(GM).
+//
+// The rotational formats give a body's angular velocity and surface-frame axes x, z:
+//
+//   5 AXIAL_OFFSET        6 channels w[3], spin-axis offsets py, pz, rotation angle; local-axis angles
+//   6 QUATERNION          4 channels (x, y, z, w) of the frame's quaternion
+//   7 TIDAL_LOCK          the same, relative to the orbit frame; needs the orbital state at the same time
+//
+// (ephemeris_compressor.cpp:761-790, state_parameters.cpp:29-57).
 //
 // Own implementation: the B-spline pieces come from the degree recursion evaluated at the point (not the
-// reference's Chebyshev tables), and the element-to-state conversion is the textbook perifocal form with
-// Kepler's equation solved by safeguarded Newton steps; agreement with the reference interpolator is to
-// rounding, not bit for bit.
+// reference's Chebyshev tables), the element-to-state conversion is the textbook perifocal form with
+// Kepler's equation solved by Newton steps from Danby's start, and the frames are built as rotations of
+// explicit axis triples; agreement with the reference interpolator is to rounding, not bit for bit.
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -46,18 +53,22 @@ struct Header {
 };
 static_assert(sizeof(Header) == kCommonHeader, "the record's common header is 24 bytes");
 
-// per-format layout: channels, bytes of the header before the coefficients, whether GM follows the fix
+// per-format layout: channels (doubles per coefficient), bytes of the header before the coefficients, the
+// doubles that follow the end corrections (GM; or the local axis's polar and azimuthal angles)
 struct Layout {
     int channels;
     size_t header_bytes;
-    bool has_gm;
+    int extras;
 };
 bool layout_of(int format, Layout &L) {
     switch (format) {
-        case 1: L = {3, kCommonHeader + 4 * 3 * 8, false}; return true;
-        case 2: L = {3, kCommonHeader + 4 * 3 * 8 + 8, true}; return true;
+        case 1: L = {3, kCommonHeader + 4 * 3 * 8, 0}; return true;
+        case 2: L = {3, kCommonHeader + 4 * 3 * 8 + 8, 1}; return true;
         case 3:
-        case 4: L = {6, kCommonHeader + 4 * 6 * 8 + 8, true}; return true;
+        case 4: L = {6, kCommonHeader + 4 * 6 * 8 + 8, 1}; return true;
+        case 5: L = {6, kCommonHeader + 4 * 6 * 8 + 16, 2}; return true;   // AXIAL_OFFSET
+        case 6:
+        case 7: L = {4, kCommonHeader + 4 * 4 * 8, 0}; return true;        // QUATERNION, TIDAL_LOCK
         default: return false;
     }
 }
@@ -70,6 +81,8 @@ struct eph_ephem {
     double range = 0, relative_error = 0, gm = 0;
     double smooth[2] = {0, 0};
     double fix[4][6] = {};
+    double axis_theta = 0, axis_phi = 0;   // AXIAL_OFFSET: the local spin axis's polar / azimuthal angle
+    double orb_r[3] = {0, 0, 0}, orb_v[3] = {0, 0, 0};   // TIDAL_LOCK: the orbital state at the same time
     std::vector<double> coef;   // [n + degree][channels]
 };
 
@@ -247,6 +260,93 @@ void elements_to_state(const Elements &k, V3 &r, V3 &v) {
     v = (vx * cw - vy * sw) * jx + (vx * sw + vy * cw) * jy;
 }
 
+// ------------------------------------------------------------------ rotational records to frame and spin
+// A body's rotation state is its angular velocity w and two axes of its surface frame, x and z (y = z x x).
+V3 unit_or_z(V3 a) {   // a / |a|, or the z axis for a zero vector (src/math/vec_t.h:166-175)
+    const double n = std::sqrt(dot(a, a));
+    if (n == 0) return {0, 0, 1};
+    return (1 / n) * a;
+}
+// the world image of local coordinates a in the frame (ex, ey, ez)
+V3 to_world(V3 ex, V3 ey, V3 ez, V3 a) { return a.x * ex + a.y * ey + a.z * ez; }
+
+// AXIAL_OFFSET channels {w[3], py, pz, angle} (ephemeris_compressor.cpp:420-466, state_parameters.cpp:29-57):
+// the spin axis's polar angle theta (cos theta = pz) and azimuth phi (sin theta sin phi = py) in the frame
+// built on w (x toward w's ascending node, z along w), the rotation angle about w; the surface frame is
+// that frame turned by -theta about its y axis and -phi about its z axis, then by the angle about w, then
+// taken to the record's local axis (polar angle, azimuth stored in the header).
+void axial_to_rotation(const eph_ephem &E, const double *a, V3 &w, V3 &x, V3 &z) {
+    w = {a[0], a[1], a[2]};
+    const V3 wz = unit_or_z(w);
+    const double th = std::acos(a[4]), ph = std::asin(a[3] / std::sqrt(1 - a[4] * a[4]));
+    V3 X = ascending_node(w), Z = wz, Y = cross(Z, X);
+    {   // -theta about the frame's y axis
+        const double c = std::cos(th), s = std::sin(th);
+        const V3 nz = c * Z + (-s) * X;
+        X = c * X + s * Z;
+        Z = nz;
+    }
+    {   // -phi about the frame's z axis
+        const double c = std::cos(ph), s = std::sin(ph);
+        const V3 nx = c * X + (-s) * Y;
+        Y = c * Y + s * X;
+        X = nx;
+    }
+    const double c = std::cos(a[5]), s = std::sin(a[5]);
+    auto spin = [&](V3 v) {   // v turned by the angle about wz: v + (c - 1) v_perp + s wz x v
+        const V3 perp = v + (-dot(wz, v)) * wz;
+        return v + (c - 1) * perp + s * cross(wz, v);
+    };
+    X = spin(X);
+    Y = spin(Y);
+    Z = spin(Z);
+    // local axis frame (u, v, u x v) from the header's angles; the surface axes are the rows of its
+    // transpose taken through (X, Y, Z)
+    const double t0 = E.axis_theta, p0 = E.axis_phi, t1 = t0 + M_PI / 2;
+    const V3 u = {std::sin(t0) * std::cos(p0), std::sin(t0) * std::sin(p0), std::cos(t0)};
+    const V3 v = {std::sin(t1) * std::cos(p0), std::sin(t1) * std::sin(p0), std::cos(t1)};
+    const V3 n = cross(u, v);
+    x = to_world(X, Y, Z, {u.x, v.x, n.x});
+    z = to_world(X, Y, Z, {u.z, v.z, n.z});
+}
+
+// Unit quaternion (x, y, z, w) to the frame's x and z axes (src/math/vec_t.h:612-623).
+void quat_axes(const double *q, V3 &x, V3 &z) {
+    double n = std::sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+    double a = q[0], b = q[1], c = q[2], d = q[3];
+    if (n == 0) { a = b = c = 0; d = 1; n = 1; }
+    a /= n; b /= n; c /= n; d /= n;
+    x = {d * d + a * a - (b * b + c * c), 2 * (a * b + d * c), 2 * (c * a - d * b)};
+    z = {2 * (c * a + d * b), 2 * (b * c - d * a), d * d + c * c - (a * a + b * b)};
+}
+
+// Angular velocity of a rotating quaternion q with derivative qd: the vector part of 2 qd q^-1.
+V3 quat_spin(const double *q, const double *qd) {
+    const double nn = q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3];
+    // qd (x) conj(q), Hamilton product, vector part
+    const double px = -qd[3] * q[0] + qd[0] * q[3] - qd[1] * q[2] + qd[2] * q[1];
+    const double py = -qd[3] * q[1] + qd[1] * q[3] - qd[2] * q[0] + qd[0] * q[2];
+    const double pz = -qd[3] * q[2] + qd[2] * q[3] - qd[0] * q[1] + qd[1] * q[0];
+    return (2 / nn) * V3{px, py, pz};
+}
+
+// QUATERNION / TIDAL_LOCK channels (ephemeris_compressor.cpp:769-790): the frame of the quaternion and the
+// spin 2 q' q^-1; a tidally locked record holds them relative to the orbit frame (x toward the orbital
+// centre, z along r x v), which the orbital state at the same time takes back to the world, adding the
+// orbit's own angular velocity r x v / r^2.
+void quat_to_rotation(const eph_ephem &E, const double *q, const double *qd, V3 &w, V3 &x, V3 &z) {
+    quat_axes(q, x, z);
+    w = quat_spin(q, qd);
+    if (E.format != 7) return;
+    const V3 r = {E.orb_r[0], E.orb_r[1], E.orb_r[2]}, v = {E.orb_v[0], E.orb_v[1], E.orb_v[2]};
+    const double r2 = dot(r, r);
+    const V3 wo = (1 / r2) * cross(r, v);
+    const V3 jx = (-1 / std::sqrt(r2)) * r, jz = unit_or_z(wo), jy = cross(jz, jx);
+    x = to_world(jx, jy, jz, x);
+    z = to_world(jx, jy, jz, z);
+    w = to_world(jx, jy, jz, w) + wo;
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------ C ABI
@@ -262,7 +362,6 @@ int eph_ephem_open(const void *record, int64_t size, double range, eph_ephem **o
     const double rel = h.relative_error;
     if (!(rel >= 0 && rel < 1)) return EPH_ERR_LOAD;   // an uncompressed or failed record
     const int format = (uint16_t)~h.uformat;
-    if (format >= 5 && format <= 7) return EPH_ERR_UNSUPPORTED;   // rotational records
     Layout L;
     if (!layout_of(format, L)) return EPH_ERR_LOAD;
     if (h.degree < 1 || h.degree > kMaxRecordDegree || h.n < 1) return EPH_ERR_LOAD;
@@ -282,7 +381,12 @@ int eph_ephem_open(const void *record, int64_t size, double range, eph_ephem **o
     E->smooth[1] = h.smooth[1];
     const uint8_t *q = p + kCommonHeader;
     for (int a = 0; a < 4; ++a, q += per) std::memcpy(E->fix[a], q, (size_t)per);
-    if (L.has_gm) std::memcpy(&E->gm, q, 8);
+    if (format == 5) {
+        std::memcpy(&E->axis_theta, q, 8);
+        std::memcpy(&E->axis_phi, q + 8, 8);
+    } else if (L.extras == 1) {
+        std::memcpy(&E->gm, q, 8);
+    }
     try {
         E->coef.resize((size_t)(h.n + h.degree) * L.channels);
     } catch (...) {
@@ -310,8 +414,33 @@ int eph_ephem_info(const eph_ephem *E, int *format, int *degree, int64_t *segmen
     return EPH_OK;
 }
 
+int eph_ephem_set_orbital_state(eph_ephem *E, const double *r, const double *v) {
+    if (!E || !r || !v) return EPH_ERR_ARG;
+    for (int c = 0; c < 3; ++c) { E->orb_r[c] = r[c]; E->orb_v[c] = v[c]; }
+    return EPH_OK;
+}
+
+int eph_ephem_rotation(const eph_ephem *E, double t, double *w, double *x, double *z) {
+    if (!E || !w || !x || !z) return EPH_ERR_ARG;
+    if (E->format < 5) return EPH_ERR_UNSUPPORTED;
+    double val[6], der[6];
+    if (!spline_at(*E, t, val, der)) {
+        for (int c = 0; c < 3; ++c) w[c] = x[c] = z[c] = NAN;
+        return EPH_ERR_ARG;
+    }
+    blend_ends(*E, t, val, der);
+    V3 ww, xx, zz;
+    if (E->format == 5) axial_to_rotation(*E, val, ww, xx, zz);
+    else quat_to_rotation(*E, val, der, ww, xx, zz);
+    w[0] = ww.x; w[1] = ww.y; w[2] = ww.z;
+    x[0] = xx.x; x[1] = xx.y; x[2] = xx.z;
+    z[0] = zz.x; z[1] = zz.y; z[2] = zz.z;
+    return EPH_OK;
+}
+
 int eph_ephem_state(const eph_ephem *E, double t, double *r, double *v, double *gm) {
     if (!E || !r || !v) return EPH_ERR_ARG;
+    if (E->format > 4) return EPH_ERR_UNSUPPORTED;   // a rotational record: eph_ephem_rotation
     double val[6], der[6];
     if (!spline_at(*E, t, val, der)) {
         for (int c = 0; c < 3; ++c) r[c] = v[c] = NAN;
@@ -333,6 +462,7 @@ int eph_ephem_state(const eph_ephem *E, double t, double *r, double *v, double *
 
 int eph_ephem_to_bspline(const eph_ephem *E, int d, int64_t n, int64_t mn, double *coefs) {
     if (!E || !coefs || mn < 1 || n < 1 || mn + 1 < n + d) return EPH_ERR_ARG;
+    if (E->format > 4) return EPH_ERR_UNSUPPORTED;
     std::vector<double> samples;
     try {
         samples.resize((size_t)(mn + 1) * 3);

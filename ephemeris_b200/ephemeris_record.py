@@ -1,11 +1,14 @@
-"""Compressed orbital ephemeris records of the reference, read through the library's host decoder.
+"""Compressed ephemeris records of the reference, read through the library's host decoder.
 
 `EphemerisInterpolator` mirrors the reference's `ephemeris_compressor::interpolator`
 (src/modules/ephemeris_compressor.h:74-148): it takes one compressed record (the bytes that
-`ephemeris_compressor::compress_orbital_data` leaves in its MFILE) and the time span it covers, and returns
-position, velocity and the record's GM at a time in [0, span] (`operator()(t, orbital_state_t*, keplerian&)`,
-ephemeris_compressor.cpp:1036-1053). `to_bspline` resamples the record into the B-spline table form of the
-device ephemeris used by `Server` (eph_serve_*) and `bspline_fit_batch`.
+`ephemeris_compressor::compress_orbital_data` / `compress_rotational_data` leave in their MFILE) and the
+time span it covers. An orbital record returns position, velocity and the record's GM at a time in
+[0, span] (`operator()(t, orbital_state_t*, keplerian&)`, ephemeris_compressor.cpp:1036-1053); a rotational
+record returns the angular velocity and the surface frame's x and z axes (`operator()(t, rotational_state_t*)`,
+ephemeris_compressor.cpp:1017-1034), a tidally locked one after `set_orbital_state` with the orbital state at
+that time (ephemeris_compressor.cpp:1010-1015). `to_bspline` resamples an orbital record into the B-spline
+table form of the device ephemeris used by `Server` (eph_serve_*) and `bspline_fit_batch`.
 """
 import ctypes
 
@@ -18,7 +21,7 @@ FORMAT_NAMES = {1: "STATE_VECTORS", 2: "KEPLERIAN_VECTORS", 3: "KEPLERIAN_CIRCUL
 
 
 class EphemerisInterpolator:
-    """One compressed orbital record over `span` seconds (formats 1-4)."""
+    """One compressed record over `span` seconds: orbital (formats 1-4) or rotational (formats 5-7)."""
 
     def __init__(self, record: bytes, span: float):
         self.lib = load_library()
@@ -59,6 +62,25 @@ class EphemerisInterpolator:
             r, v, _ = self(t)
             out[k, :3], out[k, 3:] = r, v
         return out
+
+    def is_rotational(self) -> bool:
+        return 5 <= self.format <= 7
+
+    def set_orbital_state(self, r, v):
+        """The orbital state at the next evaluation's time (needed by a tidally locked record)."""
+        r = np.ascontiguousarray(r, np.float64)
+        v = np.ascontiguousarray(v, np.float64)
+        D = ctypes.POINTER(ctypes.c_double)
+        check(self.lib.eph_ephem_set_orbital_state(self.h, r.ctypes.data_as(D), v.ctypes.data_as(D)), None,
+              "eph_ephem_set_orbital_state")
+
+    def rotation(self, t: float):
+        """(w[3], x[3], z[3]) of a rotational record at time t in [0, span]."""
+        w, x, z = np.zeros(3), np.zeros(3), np.zeros(3)
+        D = ctypes.POINTER(ctypes.c_double)
+        check(self.lib.eph_ephem_rotation(self.h, float(t), w.ctypes.data_as(D), x.ctypes.data_as(D),
+                                          z.ctypes.data_as(D)), None, "eph_ephem_rotation")
+        return w, x, z
 
     def to_bspline(self, d: int, n: int, mn: int) -> np.ndarray:
         """Positions at mn + 1 uniform times over [0, span] fitted with n + d degree-d B-splines: [n + d][3]."""

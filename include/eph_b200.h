@@ -210,12 +210,13 @@ int eph_bspline_fit_batch(int device, int d, int64_t n, int64_t mn, int channels
 /* c(d, k, j): B[d, x - k] = sum_j c(d,k,j) T_j(2x - 1) on x in [0, 1) (src/math/interp.h:24-30). */
 double eph_bspline_cheb_coef(int d, int k, int j);
 
-/* ---- Compressed orbital ephemeris records (host). One record as the reference's compressor writes it
- * (ephemeris_compressor::compress_orbital_data, src/modules/ephemeris_compressor.cpp:164-399; the reader
- * hands each one to ephemeris_compressor::interpolator, ephemeris_compressor.h:74-148 and
- * ephemeris_compressor.cpp:852-910) covering `range` seconds. Formats 1-4 (state vectors, Keplerian
- * vectors, circular and raw Keplerian elements) are read; rotational records (formats 5-7) return
- * EPH_ERR_UNSUPPORTED, a record that is not a valid compressed orbital record EPH_ERR_LOAD. */
+/* ---- Compressed ephemeris records (host). One record as the reference's compressor writes it
+ * (ephemeris_compressor::compress_orbital_data / compress_rotational_data, src/modules/
+ * ephemeris_compressor.cpp:164-530; the reader hands each one to ephemeris_compressor::interpolator,
+ * ephemeris_compressor.h:74-148 and ephemeris_compressor.cpp:852-910) covering `range` seconds. Orbital
+ * formats 1-4 (state vectors, Keplerian vectors, circular and raw Keplerian elements) and rotational
+ * formats 5-7 (axial offset, quaternion, tidal lock); a record that is not a valid compressed record
+ * returns EPH_ERR_LOAD. */
 typedef struct eph_ephem eph_ephem;
 int eph_ephem_open(const void *record, int64_t size, double range, eph_ephem **out);
 int eph_ephem_close(eph_ephem *e);
@@ -223,8 +224,16 @@ int eph_ephem_close(eph_ephem *e);
 int eph_ephem_info(const eph_ephem *e, int *format, int *degree, int64_t *segments, double *relative_error,
                    double *gm);
 /* Position r[3] and velocity v[3] at time t in [0, range] (interpolator::operator(), ephemeris_compressor.cpp:
- * 1036-1053); gm may be NULL. Outside [0, range]: NaN and EPH_ERR_ARG. */
+ * 1036-1053); gm may be NULL. Outside [0, range]: NaN and EPH_ERR_ARG; a rotational record:
+ * EPH_ERR_UNSUPPORTED. */
 int eph_ephem_state(const eph_ephem *e, double t, double *r, double *v, double *gm);
+/* Angular velocity w[3] and surface-frame axes x[3], z[3] at time t of a rotational record
+ * (interpolator::operator()(t, rotational_state_t*), ephemeris_compressor.cpp:1017-1034); an orbital record:
+ * EPH_ERR_UNSUPPORTED. A tidally locked record (format 7) needs the orbital state at the same time first. */
+int eph_ephem_rotation(const eph_ephem *e, double t, double *w, double *x, double *z);
+/* The orbital state (position and velocity relative to the orbital centre) a tidally locked record is
+ * evaluated against (interpolator::set_orbital_state, ephemeris_compressor.cpp:1010-1015). */
+int eph_ephem_set_orbital_state(eph_ephem *e, const double *r, const double *v);
 /* The record's positions at mn + 1 uniform times over [0, range], fitted by eph_bspline_fit with degree d
  * and n segments: coefs[n + d][3], the form of the device ephemeris (eph_serve_*, eph_bspline_fit_batch). */
 int eph_ephem_to_bspline(const eph_ephem *e, int d, int64_t n, int64_t mn, double *coefs);

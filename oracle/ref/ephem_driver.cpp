@@ -3,6 +3,7 @@
 // used only to record golden fixtures for the compressed-ephemeris decoder's tests.
 //
 //   ephc orbital IN BLOB EVAL
+//   ephc rotational IN BLOB EVAL [ORB]   (see rotational() below)
 //
 // IN   : int64 N, double time_span, N x {r[3], v[3]} raw samples (orbital_state_t), int64 M, M times
 // BLOB : the compressed record that ephemeris_compressor::compress_orbital_data leaves in the MFILE
@@ -37,10 +38,83 @@ static bool write_all(const char *path, const void *p, size_t n) {
     return ok;
 }
 
+// ephc rotational IN BLOB EVAL [ORB]
+// IN   : int64 N, double time_span, N x {w[3], x[3], z[3]} raw samples (rotational_state_t), int64 M, M times
+// ORB  : optional orbital samples on the same grid (int64 N, double span, N x {r, v}): compressed first,
+//        passed to compress_rotational_data (which then also tries the tidally locked form), and its
+//        interpolator's state at each evaluation time is handed to set_orbital_state before the rotation
+//        is evaluated, as the reader does
+// EVAL : int64 level, int64 format, then for each time {w[3], x[3], z[3], r[3], v[3]} (the rotation of the
+//        B-spline form as loaded, with the orbital state it was given), then the same after expand()
+static int rotational(int argc, char **argv) {
+    static_assert(sizeof(rotational_state_t) == 9 * sizeof(double), "rotational_state_t is nine doubles");
+    std::vector<uint8_t> in, orb;
+    if (!read_all(argv[2], in) || in.size() < 16) return 3;
+    const bool has_orb = argc == 6;
+    if (has_orb && (!read_all(argv[5], orb) || orb.size() < 16)) return 3;
+    int64_t N, M;
+    double span;
+    std::memcpy(&N, in.data(), 8);
+    std::memcpy(&span, in.data() + 8, 8);
+    if (N < 2 || in.size() < 16 + (size_t)N * 72 + 8) return 3;
+    MFILE mf;
+    fwrite(in.data() + 16, sizeof(rotational_state_t), (size_t)N, &mf);
+    std::memcpy(&M, in.data() + 16 + (size_t)N * 72, 8);
+    if (M < 0 || in.size() < 16 + (size_t)N * 72 + 8 + (size_t)M * 8) return 3;
+    std::vector<double> ts((size_t)M);
+    std::memcpy(ts.data(), in.data() + 16 + (size_t)N * 72 + 8, (size_t)M * 8);
+
+    MFILE morb;
+    std::vector<uint8_t> orb_blob;
+    if (has_orb) {
+        int64_t No;
+        std::memcpy(&No, orb.data(), 8);
+        if (No < 2 || orb.size() < 16 + (size_t)No * 48) return 3;
+        fwrite(orb.data() + 16, sizeof(orbital_state_t), (size_t)No, &morb);
+        if (ephemeris_compressor::compress_orbital_data(morb, span) <= 0) return 5;
+        morb.publish();
+        orb_blob.assign(morb.data(), morb.data() + morb.size());
+    }
+    const int64_t level = ephemeris_compressor::compress_rotational_data(mf, span, has_orb ? &morb : nullptr);
+    mf.publish();
+    std::vector<uint8_t> blob;
+    if (level > 0) blob.assign(mf.data(), mf.data() + mf.size());
+    if (!write_all(argv[3], blob.data(), blob.size())) return 4;
+
+    std::vector<double> out;
+    int64_t fmt = -1;
+    if (level > 0) {
+        MFILE rd(blob.data(), blob.size());
+        ephemeris_interpolator ip(&rd, span);
+        fmt = (int64_t)ip.data_format();
+        MFILE ro(orb_blob.data(), orb_blob.size());
+        ephemeris_interpolator io(has_orb ? &ro : nullptr, span);
+        for (int pass = 0; pass < 2; ++pass) {
+            if (pass == 1) ip.expand();
+            for (double t : ts) {
+                orbital_state_t os{};
+                if (has_orb) io(t, &os);
+                ip.set_orbital_state(os.r, os.v);
+                rotational_state_t s;
+                ip(t, &s);
+                const double rec[15] = {s.w.x, s.w.y, s.w.z, s.x.x, s.x.y, s.x.z, s.z.x, s.z.y, s.z.z,
+                                        os.r.x, os.r.y, os.r.z, os.v.x, os.v.y, os.v.z};
+                out.insert(out.end(), rec, rec + 15);
+            }
+        }
+    }
+    std::vector<uint8_t> ev(16 + out.size() * 8);
+    std::memcpy(ev.data(), &level, 8);
+    std::memcpy(ev.data() + 8, &fmt, 8);
+    if (!out.empty()) std::memcpy(ev.data() + 16, out.data(), out.size() * 8);
+    return write_all(argv[4], ev.data(), ev.size()) ? 0 : 4;
+}
+
 int main(int argc, char **argv) {
     static_assert(sizeof(orbital_state_t) == 6 * sizeof(double), "orbital_state_t is six doubles");
+    if ((argc == 5 || argc == 6) && std::strcmp(argv[1], "rotational") == 0) return rotational(argc, argv);
     if (argc != 5 || std::strcmp(argv[1], "orbital") != 0) {
-        std::fprintf(stderr, "usage: ephc orbital IN BLOB EVAL\n");
+        std::fprintf(stderr, "usage: ephc orbital IN BLOB EVAL | ephc rotational IN BLOB EVAL [ORB]\n");
         return 2;
     }
     std::vector<uint8_t> in;

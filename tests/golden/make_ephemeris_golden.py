@@ -1,8 +1,10 @@
 """Record the compressed-ephemeris golden fixtures (tests/golden/ephemeris/*.npz).
 
-Synthetic orbital sample series (two-body orbits of several shapes, a perturbed orbit and a non-Keplerian
-track) go through the reference's own compressor, `ephemeris_compressor::compress_orbital_data`
-(src/modules/ephemeris_compressor.cpp:164-399), via oracle/_ref/ephc (built by `make -C oracle ephc` from
+Synthetic orbital sample series (two-body orbits of several shapes, a perturbed orbit and non-Keplerian
+tracks) go through the reference's own compressor, `ephemeris_compressor::compress_orbital_data`
+(src/modules/ephemeris_compressor.cpp:164-399), and rotational series (a fast principal spin, a slow tumble,
+a tidally locked moon with its orbit) through `compress_rotational_data` (ephemeris_compressor.cpp:401-530),
+via oracle/_ref/ephc (built by `make -C oracle ephc` from
 the reference sources). Each fixture keeps the compressed record exactly as the reference writes it, the
 time span, evaluation times, and the reference interpolator's {r, v, GM} at those times
 (ephemeris_compressor.cpp:1036-1053), on the B-spline form as loaded and after expand().
@@ -86,6 +88,45 @@ def cases():
     return out
 
 
+def rot(axis, ang):
+    """Rotation matrices [len(ang)][3][3] about a unit axis by angles ang (Rodrigues)."""
+    a = np.asarray(axis, float) / np.linalg.norm(axis)
+    K = np.array([[0, -a[2], a[1]], [a[2], 0, -a[0]], [-a[1], a[0], 0]])
+    ang = np.atleast_1d(ang)
+    return np.eye(3) + np.sin(ang)[:, None, None] * K + (1 - np.cos(ang))[:, None, None] * (K @ K)
+
+
+def rotational_cases():
+    """(name, times, w, x, z, orbital (r, v) or None): body-frame axes x, z and angular velocity w."""
+    out = []
+    R0 = rot([0.3, -0.5, 0.8], [0.7])[0]
+    # fast principal spin (about 0.6 turn per sample): only the axial form applies
+    ts = np.linspace(0, 10 * DAY, 41)
+    n, om = np.array([0.1, 0.2, 0.97]) / np.linalg.norm([0.1, 0.2, 0.97]), 2 * np.pi / (10 * 3600.0)
+    R = rot(n, om * ts) @ R0
+    out.append(("spin_fast", ts, np.tile(om * n, (len(ts), 1)), R[:, :, 0], R[:, :, 2], None))
+    # slow tumbling (precession about a perpendicular axis): the body-frame spin axis wanders
+    ts = np.linspace(0, 2 * DAY, 97)
+    n1, n2, Om, om = np.array([0.0, 0.0, 1.0]), np.array([1.0, 0.0, 0.0]), 2 * np.pi / (1.1 * DAY), 2 * np.pi / (0.9 * DAY)
+    A, B = rot(n1, Om * ts), rot(n2, om * ts)
+    R = A @ B @ R0
+    w = Om * n1 + om * (A @ n2)
+    out.append(("tumble_slow", ts, w, R[:, :, 0], R[:, :, 2], None))
+    # tidally locked moon with a small libration about the orbit normal
+    ts = np.linspace(0, 27 * DAY, 325)
+    r, v = kepler_states(3.986004418e14, 3.844e8, 0.0549, 0.09, 2.1, 0.6, 0.3, ts)
+    h = np.cross(r, v)
+    zh = h / np.linalg.norm(h, axis=1)[:, None]
+    xh = -r / np.linalg.norm(r, axis=1)[:, None]
+    yh = np.cross(zh, xh)
+    lib_n = 2 * np.pi / (27.5 * DAY)
+    lam, dlam = 0.02 * np.sin(lib_n * ts), 0.02 * lib_n * np.cos(lib_n * ts)
+    x = np.cos(lam)[:, None] * xh + np.sin(lam)[:, None] * yh
+    w = h / np.einsum("ij,ij->i", r, r)[:, None] + dlam[:, None] * zh
+    out.append(("moon_locked", ts, w, x, zh, (r, v)))
+    return out
+
+
 def eval_times(span, rng):
     t = np.concatenate([[0.0, span], span * np.array([1e-6, 0.003, 0.01, 0.02, 0.5, 0.98, 0.99, 0.997, 1 - 1e-6]),
                         np.sort(rng.uniform(0, span, 48))])
@@ -111,6 +152,28 @@ def main():
             ev = np.fromfile(fev, np.uint8)
             level, fmt = np.frombuffer(ev[:16].tobytes(), np.int64)
             vals = np.frombuffer(ev[16:].tobytes(), np.float64).reshape(2, len(tev), 7) if level > 0 else np.zeros((2, 0, 7))
+            np.savez_compressed(os.path.join(OUT, name + ".npz"), blob=blob, span=span, times=tev, level=level,
+                                format=fmt, loaded=vals[0], expanded=vals[1])
+            print(f"{name:18s} level {level} format {fmt} blob {len(blob)} bytes")
+        for name, ts, w, x, z, orbit in rotational_cases():
+            span = float(ts[-1] - ts[0])
+            tev = eval_times(span, rng)
+            raw = np.concatenate([w, x, z], 1).astype(np.float64)
+            fin, fblob, fev, forb = (os.path.join(td, s) for s in ("in", "blob", "ev", "orb"))
+            with open(fin, "wb") as f:
+                f.write(np.int64(len(ts)).tobytes() + np.float64(span).tobytes() + raw.tobytes()
+                        + np.int64(len(tev)).tobytes() + tev.tobytes())
+            cmd = [EPHC, "rotational", fin, fblob, fev]
+            if orbit is not None:
+                with open(forb, "wb") as f:
+                    f.write(np.int64(len(ts)).tobytes() + np.float64(span).tobytes()
+                            + np.concatenate(orbit, 1).astype(np.float64).tobytes())
+                cmd.append(forb)
+            subprocess.run(cmd, check=True)
+            blob = np.fromfile(fblob, np.uint8)
+            ev = np.fromfile(fev, np.uint8)
+            level, fmt = np.frombuffer(ev[:16].tobytes(), np.int64)
+            vals = np.frombuffer(ev[16:].tobytes(), np.float64).reshape(2, len(tev), 15) if level > 0 else np.zeros((2, 0, 15))
             np.savez_compressed(os.path.join(OUT, name + ".npz"), blob=blob, span=span, times=tev, level=level,
                                 format=fmt, loaded=vals[0], expanded=vals[1])
             print(f"{name:18s} level {level} format {fmt} blob {len(blob)} bytes")

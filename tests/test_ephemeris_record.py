@@ -1,14 +1,17 @@
-"""Compressed orbital ephemeris records: the library's decoder against the reference's own interpolator.
+"""Compressed ephemeris records: the library's decoder against the reference's own interpolator.
 
 The fixtures (tests/golden/ephemeris/*.npz, recorded by tests/golden/make_ephemeris_golden.py) hold
-records written by the reference's compressor (`ephemeris_compressor::compress_orbital_data`,
-src/modules/ephemeris_compressor.cpp:164-399) and the reference interpolator's states at 59 times per
-record (ephemeris_compressor.cpp:1036-1053), both on the B-spline form as loaded and after expand(). They
-cover the four orbital formats: state vectors, Keplerian vectors, circular and raw Keplerian elements.
+records written by the reference's compressor (`ephemeris_compressor::compress_orbital_data` and
+`compress_rotational_data`, src/modules/ephemeris_compressor.cpp:164-530) and the reference interpolator's states at 59 times per
+record (ephemeris_compressor.cpp:1017-1053), both on the B-spline form as loaded and after expand(). They
+cover the four orbital formats (state vectors, Keplerian vectors, circular and raw Keplerian elements) and
+the three rotational ones (axial offset, quaternion, tidal lock; the tidally locked record is evaluated
+against the orbital state the reference interpolator was given, kept in the fixture).
 
 The decoder evaluates the spline and the element-to-state conversion its own way, so the bound is the
 reference's own rounding spread: the larger of 1e-14 and 1.5x the difference between the reference's two
-evaluation forms, relative to the record's largest |r| (|v|). GM is compared exactly.
+evaluation forms, relative to the record's largest |r| (|v|, |w|; the frame axes are unit vectors).
+GM is compared exactly.
 CPU-only: the decoder is host code of libeph_b200.so.
 """
 import glob
@@ -21,7 +24,9 @@ from ephemeris_b200.ephemeris_record import EphemerisInterpolator
 from ephemeris_b200 import EphError, bspline_fit
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-FIXTURES = sorted(glob.glob(os.path.join(HERE, "golden", "ephemeris", "*.npz")))
+ALL = sorted(glob.glob(os.path.join(HERE, "golden", "ephemeris", "*.npz")))
+FIXTURES = [f for f in ALL if int(np.load(f)["format"]) <= 4]
+ROTATIONAL = [f for f in ALL if int(np.load(f)["format"]) >= 5]
 EPH_ERR_ARG, EPH_ERR_LOAD, EPH_ERR_UNSUPPORTED = 1, 6, 7
 
 
@@ -30,9 +35,9 @@ def _load(path):
     return z, EphemerisInterpolator(z["blob"].tobytes(), float(z["span"]))
 
 
-def test_fixtures_cover_every_orbital_format():
-    formats = {int(np.load(f)["format"]) for f in FIXTURES}
-    assert formats == {1, 2, 3, 4}, formats
+def test_fixtures_cover_every_format():
+    formats = {int(np.load(f)["format"]) for f in ALL}
+    assert formats == {1, 2, 3, 4, 5, 6, 7}, formats
 
 
 @pytest.mark.parametrize("path", FIXTURES, ids=[os.path.basename(f)[:-4] for f in FIXTURES])
@@ -80,7 +85,8 @@ def test_invalid_records_are_rejected():
         (_patched(blob, 0, np.float32, 1.0), EPH_ERR_LOAD),       # relative error not below 1
         (_patched(blob, 0, np.float32, np.nan), EPH_ERR_LOAD),
         (_patched(blob, 6, np.uint16, 0xFFFF), EPH_ERR_LOAD),     # format 0 (uncompressed)
-        (_patched(blob, 6, np.uint16, 0xFFFF ^ 6), EPH_ERR_UNSUPPORTED),   # a rotational (quaternion) record
+        (_patched(blob, 6, np.uint16, 0xFFFF ^ 6), EPH_ERR_LOAD),   # quaternion format, wrong size for it
+        (_patched(blob, 6, np.uint16, 0xFFFF ^ 8), EPH_ERR_LOAD),   # beyond the last format
         (_patched(blob, 4, np.int16, 0), EPH_ERR_LOAD),           # degree 0
         (_patched(blob, 8, np.int64, 0), EPH_ERR_LOAD),           # no segments
         (blob[:16], EPH_ERR_ARG),                                 # shorter than the common header
@@ -92,6 +98,34 @@ def test_invalid_records_are_rejected():
     with pytest.raises(EphError) as e:
         EphemerisInterpolator(blob, 0.0)
     assert e.value.code == EPH_ERR_ARG
+
+
+@pytest.mark.parametrize("path", ROTATIONAL, ids=[os.path.basename(f)[:-4] for f in ROTATIONAL])
+def test_rotational_record_matches_reference_interpolator(path):
+    z, ip = _load(path)
+    assert ip.format == int(z["format"]) and ip.is_rotational()
+    ref_a, ref_b = z["loaded"], z["expanded"]
+    got = np.zeros((len(z["times"]), 9))
+    for k, t in enumerate(z["times"]):
+        ip.set_orbital_state(ref_a[k, 9:12], ref_a[k, 12:15])   # the reference's orbital state at t
+        got[k] = np.concatenate(ip.rotation(t))
+    ws = np.linalg.norm(ref_a[:, :3], axis=1).max()
+    spread_w = np.abs(ref_a[:, :3] - ref_b[:, :3]).max() / ws
+    spread_f = np.abs(ref_a[:, 3:9] - ref_b[:, 3:9]).max()
+    for ref in (ref_a, ref_b):
+        assert np.abs(got[:, :3] - ref[:, :3]).max() / ws <= max(1e-14, 1.5 * spread_w)
+        assert np.abs(got[:, 3:9] - ref[:, 3:9]).max() <= max(1e-14, 1.5 * spread_f)
+    with pytest.raises(EphError) as e:
+        ip(0.0)                                   # a rotational record has no orbital state
+    assert e.value.code == EPH_ERR_UNSUPPORTED
+    ip.close()
+
+
+def test_orbital_record_has_no_rotation():
+    _, ip = _load(FIXTURES[0])
+    with pytest.raises(EphError) as e:
+        ip.rotation(0.0)
+    assert e.value.code == EPH_ERR_UNSUPPORTED
 
 
 def _bspline_eval(coefs, d, n, x):
