@@ -46,6 +46,28 @@ def kepler_states(gm, a, e, inc, node, argp, m0, ts):
     return r, v
 
 
+def hyperbolic_states(gm, q, e, inc, node, argp, t_peri, ts):
+    """Two-body states of a hyperbolic orbit (periapsis distance q, eccentricity e > 1, periapsis at t_peri)."""
+    a = q / (e - 1)
+    n = np.sqrt(gm / a ** 3)
+    M = n * (ts - t_peri)
+    H = np.arcsinh(M / e)
+    for _ in range(80):
+        H -= (e * np.sinh(H) - H - M) / (e * np.cosh(H) - 1)
+    ch, sh = np.cosh(H), np.sinh(H)
+    b = a * np.sqrt(e * e - 1)
+    xp, yp = a * (e - ch), b * sh
+    hdot = n / (e * ch - 1)
+    vxp, vyp = -a * sh * hdot, b * ch * hdot
+    co, so, ci, si, cw, sw = np.cos(node), np.sin(node), np.cos(inc), np.sin(inc), np.cos(argp), np.sin(argp)
+    R = np.array([[co * cw - so * sw * ci, -co * sw - so * cw * ci, so * si],
+                  [so * cw + co * sw * ci, -so * sw + co * cw * ci, -co * si],
+                  [sw * si, cw * si, ci]])
+    r = np.stack([xp, yp, np.zeros_like(xp)], 1) @ R.T
+    v = np.stack([vxp, vyp, np.zeros_like(xp)], 1) @ R.T
+    return r, v
+
+
 def cases():
     rng = np.random.default_rng(2024)
     gm_earth, gm_sun = 3.986004418e14, 1.32712440018e20
@@ -81,6 +103,11 @@ def cases():
     v = v0 + np.outer(ts, acc) + 1.0e5 * np.stack(
         [np.cos(ts / DAY) / DAY, -np.sin(ts / (2 * DAY)) / (2 * DAY), np.cos(ts / (3 * DAY)) / (3 * DAY)], 1)
     out.append(("outward_track", ts, r, v))
+    # hyperbolic flyby through periapsis, and a mildly hyperbolic interstellar-like comet
+    ts = np.linspace(0, 8 * DAY, 321)
+    out.append(("flyby_hyperbolic", ts, *hyperbolic_states(gm_earth, 7.0e6, 1.8, 0.7, 0.4, 1.1, 4 * DAY, ts)))
+    ts = np.linspace(0, 200 * DAY, 401)
+    out.append(("comet_hyperbolic", ts, *hyperbolic_states(gm_sun, 0.25 * 1.496e11, 1.2, 2.2, 0.3, 2.0, 90 * DAY, ts)))
     # short series: few samples (low B-spline degree)
     ts = np.linspace(0, 2 * DAY, 5)
     out.append(("moon_short", ts, *kepler_states(gm_earth, 3.844e8, 0.0549, 0.09, 2.1, 0.6, 1.0, ts)))
