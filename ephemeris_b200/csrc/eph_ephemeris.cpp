@@ -29,8 +29,9 @@
 //
 // Own implementation: the B-spline pieces come from the degree recursion evaluated at the point (not the
 // reference's Chebyshev tables), the element-to-state conversion is the textbook perifocal form with
-// Kepler's equation solved by Newton steps from Danby's start, and the frames are built as rotations of
-// explicit axis triples; agreement with the reference interpolator is to rounding, not bit for bit.
+// Kepler's equation solved by Newton steps (in a form that keeps near-parabolic orbits accurate), and the
+// frames are built as rotations of explicit axis triples; agreement with the reference interpolator is to
+// rounding, not bit for bit.
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -199,6 +200,30 @@ Elements elements_from(const double *p, bool circular) {
     return k;
 }
 
+// x - sin x and sinh x - x, by their series below |x| = 1 (where the difference cancels), else directly.
+double x_minus_sin(double x) {
+    if (std::fabs(x) >= 1) return x - std::sin(x);
+    const double x2 = x * x;
+    double term = x * x2 / 6, sum = 0;
+    for (int k = 2; k < 40 && term != 0; ++k) {   // x^3/3! - x^5/5! + ...
+        sum += term;
+        term *= -x2 / ((2 * k) * (2 * k + 1));
+        if (std::fabs(term) < 1e-18 * std::fabs(sum)) break;
+    }
+    return sum;
+}
+double sinh_minus_x(double x) {
+    if (std::fabs(x) >= 1) return std::sinh(x) - x;
+    const double x2 = x * x;
+    double term = x * x2 / 6, sum = 0;
+    for (int k = 2; k < 40 && term != 0; ++k) {   // x^3/3! + x^5/5! + ...
+        sum += term;
+        term *= x2 / ((2 * k) * (2 * k + 1));
+        if (std::fabs(term) < 1e-18 * std::fabs(sum)) break;
+    }
+    return sum;
+}
+
 // Mean anomaly reduced into [-pi, pi].
 double wrap_pi(double a) {
     constexpr double two_pi = 6.283185307179586476925286766559;
@@ -214,34 +239,44 @@ void elements_to_state(const Elements &k, V3 &r, V3 &v) {
     const double e = k.q + 1;
     const double Q = k.q * (k.q + 2);   // e^2 - 1 without cancellation
     const double aQ = std::fabs(Q), sQ = std::sqrt(aQ);
-    double x, y;
+    double x, y, vyn;   // perifocal position / p; vyn = e - Q x (cos E, cosh H or 1) without cancellation
     if (Q < 0) {
         // ellipse: E - e sin E = M; x = (cos E - e) / (1 - e^2), y = sin E / sqrt(1 - e^2), with
         // cos E - e = -2 sin^2(E/2) - q kept free of cancellation near periapsis of a near-parabolic orbit
+        // written as (1 - e) E + e (E - sin E) = M, with 1 - e = -q and E - sin E from its series at small E,
+        // so that near-parabolic orbits (M and 1 - e both small) keep full relative precision
         const double M = wrap_pi(k.m * aQ * sQ);
         double E = M + 0.85 * e * (M >= 0 ? 1 : -1);   // Danby's start: Newton converges for every e < 1
-        for (int it = 0; it < 60; ++it) {
-            const double f = E - e * std::sin(E) - M, fp = 1 - e * std::cos(E);
+        for (int it = 0; it < 100; ++it) {
+            const double sh = std::sin(0.5 * E);
+            const double f = -k.q * E + e * x_minus_sin(E) - M, fp = -k.q + 2 * e * sh * sh;
             const double dE = f / fp;
             E -= dE;
-            if (std::fabs(dE) <= 1e-16 * (1 + std::fabs(E))) break;
+            if (std::fabs(dE) <= 1e-16 * std::fabs(E) || f == 0) break;
         }
         const double sh = std::sin(0.5 * E);
         x = (-2 * sh * sh - k.q) / aQ;
         y = std::sin(E) / sQ;
+        vyn = std::cos(E);
     } else if (Q > 0) {
         // hyperbola: e sinh H - H = M; x = (e - cosh H) / (e^2 - 1), y = sinh H / sqrt(e^2 - 1)
+        // written as (e - 1) H + e (sinh H - H) = M, the same way as the ellipse
         const double M = k.m * aQ * sQ;
-        double H = std::asinh(M / e);
+        // start: the cubic root cbrt(6 |M| / e) lies beyond the solution (sinh H - H >= H^3 / 6); for large |M|
+        // asinh(|M| / e) + 1 is closer. f is odd and convex for H > 0, so Newton converges from either side.
+        const double aM = std::fabs(M);
+        double H = std::fmin(std::cbrt(6 * aM / e), std::asinh(aM / e) + 1) * (M >= 0 ? 1 : -1);
         for (int it = 0; it < 200; ++it) {
-            const double f = e * std::sinh(H) - H - M, fp = e * std::cosh(H) - 1;
+            const double sh = std::sinh(0.5 * H);
+            const double f = k.q * H + e * sinh_minus_x(H) - M, fp = k.q + 2 * e * sh * sh;
             const double dH = f / fp;
             H -= dH;
-            if (std::fabs(dH) <= 1e-16 * (1 + std::fabs(H))) break;
+            if (std::fabs(dH) <= 1e-16 * std::fabs(H) || f == 0) break;
         }
         const double sh = std::sinh(0.5 * H);
         x = (k.q - 2 * sh * sh) / aQ;   // e - cosh H = q - 2 sinh^2(H/2)
         y = std::sinh(H) / sQ;
+        vyn = std::cosh(H);
     } else {
         // parabola: Barker's equation for D = tan(nu/2): D / 2 + D^3 / 6 = m (the limit of the modified
         // mean anomaly); x = (1 - D^2) / 2, y = D
@@ -249,10 +284,11 @@ void elements_to_state(const Elements &k, V3 &r, V3 &v) {
         const double D = s - 1 / s;
         x = (1 - D * D) / 2;
         y = D;
+        vyn = 1;
     }
     const double rn = jj * std::sqrt(x * x + y * y);   // |r|
     const double vv = jn / rn;
-    const double vx = -y * vv, vy = (e - Q * x) * vv;
+    const double vx = -y * vv, vy = vyn * vv;
     const V3 jx = ascending_node(k.j), jy = (1 / jn) * cross(k.j, jx);
     const double cw = std::cos(k.w), sw = std::sin(k.w);
     const double X = jj * x, Y = jj * y;

@@ -108,6 +108,12 @@ def cases():
     out.append(("flyby_hyperbolic", ts, *hyperbolic_states(gm_earth, 7.0e6, 1.8, 0.7, 0.4, 1.1, 4 * DAY, ts)))
     ts = np.linspace(0, 200 * DAY, 401)
     out.append(("comet_hyperbolic", ts, *hyperbolic_states(gm_sun, 0.25 * 1.496e11, 1.2, 2.2, 0.3, 2.0, 90 * DAY, ts)))
+    # near-parabolic comets through perihelion (e = 0.9995 and 1.0005)
+    ts = np.linspace(0, 60 * DAY, 241)
+    q = 0.4 * 1.496e11
+    out.append(("comet_near_parabolic_e", ts, *kepler_states(gm_sun, q / (1 - 0.9995), 0.9995, 1.9, 0.5, 2.4,
+                                                             -np.sqrt(gm_sun / (q / 0.0005) ** 3) * 30 * DAY, ts)))
+    out.append(("comet_near_parabolic_h", ts, *hyperbolic_states(gm_sun, q, 1.0005, 1.9, 0.5, 2.4, 30 * DAY, ts)))
     # short series: few samples (low B-spline degree)
     ts = np.linspace(0, 2 * DAY, 5)
     out.append(("moon_short", ts, *kepler_states(gm_earth, 3.844e8, 0.0549, 0.09, 2.1, 0.6, 1.0, ts)))
