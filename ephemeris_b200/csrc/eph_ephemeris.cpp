@@ -400,7 +400,8 @@ int eph_ephem_open(const void *record, int64_t size, double range, eph_ephem **o
     const int format = (uint16_t)~h.uformat;
     Layout L;
     if (!layout_of(format, L)) return EPH_ERR_LOAD;
-    if (h.degree < 1 || h.degree > kMaxRecordDegree || h.n < 1) return EPH_ERR_LOAD;
+    // (n above the record's size cannot fit its coefficients; checked first so that n + degree cannot overflow)
+    if (h.degree < 1 || h.degree > kMaxRecordDegree || h.n < 1 || h.n > size) return EPH_ERR_LOAD;
     const int64_t per = (int64_t)L.channels * 8;
     if (size < (int64_t)L.header_bytes || (size - (int64_t)L.header_bytes) % per != 0 ||
         (size - (int64_t)L.header_bytes) / per != h.n + h.degree)

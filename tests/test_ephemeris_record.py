@@ -89,6 +89,7 @@ def test_invalid_records_are_rejected():
         (_patched(blob, 6, np.uint16, 0xFFFF ^ 8), EPH_ERR_LOAD),   # beyond the last format
         (_patched(blob, 4, np.int16, 0), EPH_ERR_LOAD),           # degree 0
         (_patched(blob, 8, np.int64, 0), EPH_ERR_LOAD),           # no segments
+        (_patched(blob, 8, np.int64, 2 ** 63 - 1), EPH_ERR_LOAD),  # a segment count beyond any record size
         (blob[:16], EPH_ERR_ARG),                                 # shorter than the common header
     ]
     for rec, want in cases:
