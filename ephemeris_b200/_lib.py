@@ -102,6 +102,7 @@ SIGNATURES = [
     ("eph_ephem_info", ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                        ctypes.POINTER(ctypes.c_int64), _D, _D]),
     ("eph_ephem_state", ctypes.c_int, [_VP, ctypes.c_double, _D, _D, _D]),
+    ("eph_ephem_states", ctypes.c_int, [_VP, ctypes.c_int64, _D, _D]),
     ("eph_ephem_to_bspline", ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int64, ctypes.c_int64, _D]),
     ("eph_ephem_rotation", ctypes.c_int, [_VP, ctypes.c_double, _D, _D, _D]),
     ("eph_ephem_set_orbital_state", ctypes.c_int, [_VP, _D, _D]),

@@ -497,6 +497,18 @@ int eph_ephem_state(const eph_ephem *E, double t, double *r, double *v, double *
     return EPH_OK;
 }
 
+int eph_ephem_states(const eph_ephem *E, int64_t count, const double *t, double *out) {
+    if (!E || count < 0 || (count > 0 && (!t || !out))) return EPH_ERR_ARG;
+    if (E->format > 4) return EPH_ERR_UNSUPPORTED;
+    int status = EPH_OK;
+    for (int64_t k = 0; k < count; ++k) {
+        double *o = out + 6 * k;
+        const int rc = eph_ephem_state(E, t[k], o, o + 3, nullptr);
+        if (rc && !status) status = rc;   // the state is NaN there; the rest are still evaluated
+    }
+    return status;
+}
+
 int eph_ephem_to_bspline(const eph_ephem *E, int d, int64_t n, int64_t mn, double *coefs) {
     if (!E || !coefs || mn < 1 || n < 1 || mn + 1 < n + d) return EPH_ERR_ARG;
     if (E->format > 4) return EPH_ERR_UNSUPPORTED;

@@ -57,10 +57,11 @@ class EphemerisInterpolator:
 
     def states(self, times):
         """Positions and velocities [len(times)][6] at the given times."""
-        out = np.empty((len(times), 6))
-        for k, t in enumerate(times):
-            r, v, _ = self(t)
-            out[k, :3], out[k, 3:] = r, v
+        t = np.ascontiguousarray(times, np.float64)
+        out = np.empty((len(t), 6))
+        D = ctypes.POINTER(ctypes.c_double)
+        check(self.lib.eph_ephem_states(self.h, len(t), t.ctypes.data_as(D), out.ctypes.data_as(D)), None,
+              "eph_ephem_states")
         return out
 
     def is_rotational(self) -> bool:

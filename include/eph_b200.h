@@ -227,6 +227,9 @@ int eph_ephem_info(const eph_ephem *e, int *format, int *degree, int64_t *segmen
  * 1036-1053); gm may be NULL. Outside [0, range]: NaN and EPH_ERR_ARG; a rotational record:
  * EPH_ERR_UNSUPPORTED. */
 int eph_ephem_state(const eph_ephem *e, double t, double *r, double *v, double *gm);
+/* The same at `count` times: out[count][6] = {r, v}. Times outside [0, range] give NaN rows and EPH_ERR_ARG
+ * after every other row is filled. */
+int eph_ephem_states(const eph_ephem *e, int64_t count, const double *t, double *out);
 /* Angular velocity w[3] and surface-frame axes x[3], z[3] at time t of a rotational record
  * (interpolator::operator()(t, rotational_state_t*), ephemeris_compressor.cpp:1017-1034); an orbital record:
  * EPH_ERR_UNSUPPORTED. A tidally locked record (format 7) needs the orbital state at the same time first. */
@@ -234,6 +237,8 @@ int eph_ephem_rotation(const eph_ephem *e, double t, double *w, double *x, doubl
 /* The orbital state (position and velocity relative to the orbital centre) a tidally locked record is
  * evaluated against (interpolator::set_orbital_state, ephemeris_compressor.cpp:1010-1015). */
 int eph_ephem_set_orbital_state(eph_ephem *e, const double *r, const double *v);
+/* A record handle is read-only after eph_ephem_open except for eph_ephem_set_orbital_state: handles may be
+ * used from several threads, one handle's orbital state from one thread at a time. */
 /* The record's positions at mn + 1 uniform times over [0, range], fitted by eph_bspline_fit with degree d
  * and n segments: coefs[n + d][3], the form of the device ephemeris (eph_serve_*, eph_bspline_fit_batch). */
 int eph_ephem_to_bspline(const eph_ephem *e, int d, int64_t n, int64_t mn, double *coefs);

@@ -69,6 +69,13 @@ def test_times_outside_the_record_are_rejected():
     assert e.value.code == EPH_ERR_ARG
     with pytest.raises(EphError):
         ip(-1.0)
+    t = np.array([0.0, -1.0, float(z["span"])])
+    out = np.empty((3, 6))
+    import ctypes
+    D = ctypes.POINTER(ctypes.c_double)
+    assert ip.lib.eph_ephem_states(ip.h, 3, t.ctypes.data_as(D), out.ctypes.data_as(D)) == EPH_ERR_ARG
+    assert np.isnan(out[1]).all() and np.isfinite(out[[0, 2]]).all()   # the other times are still evaluated
+    assert np.array_equal(out[0], np.concatenate(ip(0.0)[:2]))
 
 
 def _patched(blob, offset, dtype, value):
