@@ -84,6 +84,7 @@ struct eph_ephem {
     double fix[4][6] = {};
     double axis_theta = 0, axis_phi = 0;   // AXIAL_OFFSET: the local spin axis's polar / azimuthal angle
     double orb_r[3] = {0, 0, 0}, orb_v[3] = {0, 0, 0};   // TIDAL_LOCK: the orbital state at the same time
+    bool orb_set = false;
     std::vector<double> coef;   // [n + degree][channels]
 };
 
@@ -454,12 +455,14 @@ int eph_ephem_info(const eph_ephem *E, int *format, int *degree, int64_t *segmen
 int eph_ephem_set_orbital_state(eph_ephem *E, const double *r, const double *v) {
     if (!E || !r || !v) return EPH_ERR_ARG;
     for (int c = 0; c < 3; ++c) { E->orb_r[c] = r[c]; E->orb_v[c] = v[c]; }
+    E->orb_set = true;
     return EPH_OK;
 }
 
 int eph_ephem_rotation(const eph_ephem *E, double t, double *w, double *x, double *z) {
     if (!E || !w || !x || !z) return EPH_ERR_ARG;
     if (E->format < 5) return EPH_ERR_UNSUPPORTED;
+    if (E->format == 7 && !E->orb_set) return EPH_ERR_STATE;   // no orbital state to take the frame back
     double val[6], der[6];
     if (!spline_at(*E, t, val, der)) {
         for (int c = 0; c < 3; ++c) w[c] = x[c] = z[c] = NAN;

@@ -232,7 +232,8 @@ int eph_ephem_state(const eph_ephem *e, double t, double *r, double *v, double *
 int eph_ephem_states(const eph_ephem *e, int64_t count, const double *t, double *out);
 /* Angular velocity w[3] and surface-frame axes x[3], z[3] at time t of a rotational record
  * (interpolator::operator()(t, rotational_state_t*), ephemeris_compressor.cpp:1017-1034); an orbital record:
- * EPH_ERR_UNSUPPORTED. A tidally locked record (format 7) needs the orbital state at the same time first. */
+ * EPH_ERR_UNSUPPORTED. A tidally locked record (format 7) needs the orbital state at the same time first
+ * (EPH_ERR_STATE until one is set). */
 int eph_ephem_rotation(const eph_ephem *e, double t, double *w, double *x, double *z);
 /* The orbital state (position and velocity relative to the orbital centre) a tidally locked record is
  * evaluated against (interpolator::set_orbital_state, ephemeris_compressor.cpp:1010-1015). */

@@ -114,6 +114,10 @@ def test_rotational_record_matches_reference_interpolator(path):
     assert ip.format == int(z["format"]) and ip.is_rotational()
     ref_a, ref_b = z["loaded"], z["expanded"]
     got = np.zeros((len(z["times"]), 9))
+    if ip.format == 7:
+        with pytest.raises(EphError) as e:
+            ip.rotation(0.0)                      # no orbital state given yet
+        assert e.value.code == 5                  # EPH_ERR_STATE
     for k, t in enumerate(z["times"]):
         ip.set_orbital_state(ref_a[k, 9:12], ref_a[k, 12:15])   # the reference's orbital state at t
         got[k] = np.concatenate(ip.rotation(t))
