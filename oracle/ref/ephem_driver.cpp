@@ -92,7 +92,8 @@ static int rotational(int argc, char **argv) {
         for (int pass = 0; pass < 2; ++pass) {
             if (pass == 1) ip.expand();
             for (double t : ts) {
-                orbital_state_t os{};
+                orbital_state_t os;
+                std::memset(&os, 0, sizeof(os));   // (its vectors have no initialising constructor)
                 if (has_orb) io(t, &os);
                 ip.set_orbital_state(os.r, os.v);
                 rotational_state_t s;

@@ -10,6 +10,7 @@ time span, evaluation times, and the reference interpolator's {r, v, GM} at thos
 (ephemeris_compressor.cpp:1036-1053), on the B-spline form as loaded and after expand().
 
 Run from the repository root: python tests/golden/make_ephemeris_golden.py
+(EPH_GOLDEN_EPHEMERIS_DIR writes the fixtures elsewhere, for the reproducibility test.)
 """
 import os
 import subprocess
@@ -21,7 +22,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 EPHC = os.path.join(ROOT, "oracle", "_ref", "ephc")
-OUT = os.path.join(HERE, "ephemeris")
+OUT = os.environ.get("EPH_GOLDEN_EPHEMERIS_DIR", os.path.join(HERE, "ephemeris"))
 DAY = 86400.0
 
 

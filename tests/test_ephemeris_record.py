@@ -172,3 +172,22 @@ def test_record_resampled_into_device_bspline_table():
     exact = ip.states(x / n * span)[:, :3]
     err = np.linalg.norm(fit - exact, axis=1).max() / np.linalg.norm(exact, axis=1).max()
     assert err < 1e-7, err
+
+
+def test_fixtures_are_what_the_reference_compressor_writes(tmp_path):
+    """Re-record the fixtures through the reference's own compressor (oracle/_ref/ephc, built from the
+    reference sources where they are present) and compare the records byte for byte and the reference
+    interpolator's values exactly."""
+    import subprocess
+    import sys
+    ephc = os.path.join(os.path.dirname(HERE), "oracle", "_ref", "ephc")
+    if not os.path.exists(ephc):
+        pytest.skip("oracle/_ref/ephc is not built (the reference sources are not present)")
+    env = dict(os.environ, EPH_GOLDEN_EPHEMERIS_DIR=str(tmp_path))
+    subprocess.run([sys.executable, os.path.join(HERE, "golden", "make_ephemeris_golden.py")], check=True, env=env,
+                   capture_output=True)
+    for f in ALL:
+        a, b = np.load(f), np.load(os.path.join(str(tmp_path), os.path.basename(f)))
+        assert np.array_equal(a["blob"], b["blob"]), f
+        for key in ("times", "loaded", "expanded"):
+            assert np.array_equal(a[key], b[key]), (f, key)
